@@ -1,0 +1,153 @@
+/*
+ * oracle.h -- CPU restatement of the closures-2d Mn/PPn entropy-closure path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle: a plain-C, FP64 restatement
+ * of the reference algorithm, used as the checker by tests/, by
+ * __graft_entry__.smoke() and by bench.py's cpu_baseline / reference arm.
+ * The product (closures-2d_b200/) never links, loads or calls anything here.
+ *
+ * Parity pin: the restatement reproduces the reference's eight momopt
+ * regression goldens (tests/regression/momopt/{delta,gaussian,lattice,smooth}
+ * /{mn,ppn}.pn, copied to tests/golden/) -- see tests/test_oracle_golden.py.
+ *
+ * Each function cites the reference file:line it follows (paths inside the
+ * closures-2d project).  Third-party arithmetic the reference pulls from GSL
+ * (Gauss-Legendre table, normalised associated Legendre functions, Householder
+ * QR least squares) and LAPACK (dpotrf, dpocon, dpotrs) is restated from the
+ * published algorithms; neither library is present here and neither version is
+ * pinned by the reference (install.md lists no versions).
+ */
+#ifndef CLOSURES_ORACLE_H
+#define CLOSURES_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* opt/opt.h:34-37 */
+enum { ORC_MN = 0, ORC_PPN = 1 };
+
+/* opt/opt.h:39-40 */
+#define ORC_NUM_REG 5
+extern const double ORC_REGULARIZATIONS[ORC_NUM_REG];
+
+/* Status codes.  The reference aborts the process in these cases
+ * (opt.cpp:97-101 "u[0] < 0", opt.cpp:256-261 "Max regularization achieved");
+ * the oracle returns them so tests can observe the failure. */
+enum { ORC_OK = 0, ORC_ERR_U0 = -1, ORC_ERR_MAXREG = -2, ORC_ERR_INPUT = -3 };
+
+/* opt/opt.h:11-23 (BFGS-only fields dropped; tolAbs is unused by opt.cpp). */
+typedef struct {
+    int momentType;
+    int maxIter;
+    double tolRel;
+    double condHMax;
+    double deltaPPn;
+    int useGaunt;
+    /* Supplementary stopping test gamma = modcfl(d) <= tolGamma, present in
+     * the reference as commented-out code (opt.cpp:99-126, :339, :343;
+     * tolGamma = 1.1 at momopt_update.cpp:226).  0 disables it, which is the
+     * reference's current behaviour; 1.1 reproduces the revision that wrote
+     * the delta and lattice regression goldens. */
+    double tolGamma;
+} orc_options;
+
+/* opt/opt.h:25-32 */
+typedef struct {
+    double r;
+    int iter;
+    double normG;
+} orc_outs;
+
+/* Gaunt table (fobj.h:12-22 HStruct), stored CSR over the n*n (i,j) pairs. */
+typedef struct {
+    int n;          /* moments */
+    int *off;       /* n*n+1 offsets */
+    int *idx;       /* extended-moment index k */
+    double *val;    /* coefficient */
+} orc_gaunt;
+
+/* Angular set-up: momopt_init.cpp:88-259 */
+typedef struct {
+    int order, Q, useGaunt;
+    int n, n2, nq;
+    double *w, *xi, *eta;   /* [nq] */
+    double *p;              /* [nq*n2] row-major, p[q*n2+k] */
+    orc_gaunt gaunt;        /* only when useGaunt */
+} orc_setup;
+
+int  orc_setup_create(int order, int Q, int useGaunt, orc_setup *s);
+void orc_setup_free(orc_setup *s);
+
+/* Gauss-Legendre nodes (ascending) and weights on [-1,1]; utils.cpp:55-60. */
+void orc_gauss_legendre(int n, double *x, double *w);
+/* Normalised associated Legendre with Condon-Shortley phase
+ * (the quantity gsl_sf_legendre_sphPlm returns). */
+double orc_sphPlm(int l, int m, double x);
+
+/* Per-cell operator: opt.cpp:82-148 (in-place on u, alpha). */
+int orc_opt(int n, int n2, int nq, double *u, double *alpha, orc_options opts,
+            const double *w, const double *p, const orc_gaunt *g, orc_outs *outs);
+
+/* Batched opt over count vectors of n (OpenMP, schedule(dynamic,1)), as the
+ * reference's solveOptimization loop (momopt_update.cpp:208-277).
+ * status[c] receives the orc_opt return code; iters/regs may be NULL. */
+int orc_opt_batch(const orc_setup *s, orc_options opts, int count,
+                  double *u, double *alpha, int *iters, double *regs, int *status);
+
+/* f,g,H evaluation (fobj.cpp); g and h may be NULL as in the reference. */
+double orc_fobj(int momentType, int n, int n2, int nq, const double *alpha,
+                const double *u, const double *w, const double *p, double delta,
+                double *g, double *h, int useGaunt, const orc_gaunt *gt, double *gExt);
+
+/* ---------------------------------------------------------------------- */
+/* Whole solver: main.cpp + momopt_*.cpp                                  */
+
+typedef struct {
+    /* input.deck (main.cpp:67-83) */
+    int numCellsX, numCellsY;
+    double ax, ay, bx, by, tFinal, outDeltaT, gaussianSigma, floor_, sigma;
+    int initCond;
+    /* momopt deck (momopt_init.cpp:56-68) */
+    int momentOrder, quadOrder, useGaunt, momentType, optType, maxIter;
+    double cflFactor, tol, condHMax, theta, deltaPPn;
+    double tolGamma;        /* optional key MOMOPT_TOL_GAMMA, default 0 (off) */
+} orc_deck;
+
+typedef struct {
+    int maxIter;
+    int histReg[ORC_NUM_REG];
+    double iterMean;
+    int64_t numDualSolves;
+} orc_stats;
+
+typedef struct {
+    orc_deck deck;
+    orc_setup set;
+    int gX[4], gY[4];
+    int NX, NY;             /* with ghosts */
+    double dx, dy, maxDt;
+    double *initialGrid, *sigmaT, *sigmaS;   /* [NX*NY] */
+    double *moments, *alpha, *flux, *momentsOld, *ansatzGrid;
+    orc_stats stats;
+    int status;             /* first error code seen */
+    int64_t errCell;
+} orc_solver;
+
+/* Deck parsing with the reference's semantics (input_deck_reader.cpp). */
+int orc_deck_read(const char *path, orc_deck *d);
+int orc_solver_create(const orc_deck *d, orc_solver *s);
+void orc_solver_free(orc_solver *s);
+/* One RK2 step, momopt_update.cpp:283-382.  Returns the status. */
+int orc_solver_update(orc_solver *s, double dt);
+/* momopt_output.cpp:21-77, files out_<t>_0.{pn,opt} in dir. */
+int orc_solver_output(orc_solver *s, double time, const char *dir);
+/* main.cpp:204-230 time loop including outputs; nsteps_max<0 = no limit. */
+int orc_solver_run(orc_solver *s, const char *dir, int nsteps_max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,70 @@
+"""input.deck writers for the tests and the bench.
+
+The deck format is the reference's flat key/value file
+(input_deck_reader.cpp:17-78).  The regression deck reproduces the values the
+reference's harness writes for its momopt goldens (site_scons/testing.py:143-146
+and util/decks.py:26-56, 58-104): 36x74 cells on [-1.55,1.45]x[-1.62,1.38],
+t_final 1.03, sigma 1.111, Gaussian sigma 1.7 (0 for "delta"), floor 1e-4,
+order 3, Q 30, tol 1e-4, cond 1e10, max_iter 100, Gaunt 1, theta 2.
+"""
+
+INIT_CONDS = {"delta": 0, "gaussian": 0, "lattice": 1, "smooth": 2}
+MOMENT_TYPES = {"mn": 0, "ppn": 1}
+
+
+def deck_text(solver="momopt", num_cells_x=50, num_cells_y=50, a_x=-1.5, b_x=1.5,
+              a_y=-1.5, b_y=1.5, t_final=1.0, out_delta_t=1000.1, gaussian_sigma=0.4,
+              floor=1e-4, init_cond="gaussian", sigma=1.0, moment_order=3, quad_order=30,
+              cfl_factor=0.9, tol=1e-4, cond_h_max=1e10, cond_h_max_bfgs=20, max_iter=100,
+              max_bfgs_iter=5, use_gaunt=1, theta=2.0, delta_ppn=1e-10, moment_type="mn",
+              opt_type=0, extra=None):
+    ic = INIT_CONDS[init_cond] if isinstance(init_cond, str) else int(init_cond)
+    mt = MOMENT_TYPES[moment_type] if isinstance(moment_type, str) else int(moment_type)
+    lines = [
+        "SOLVER %s" % solver,
+        "NUM_CELLS_X %d" % num_cells_x,
+        "NUM_CELLS_Y %d" % num_cells_y,
+        "NUM_MPI_PARTITIONS_X 1",
+        "NUM_MPI_PARTITIONS_Y 1",
+        "A_X %.17f" % a_x,
+        "B_X %.17f" % b_x,
+        "A_Y %.17f" % a_y,
+        "B_Y %.17f" % b_y,
+        "T_FINAL %.17f" % t_final,
+        "OUT_DELTA_T %.17f" % out_delta_t,
+        "GAUSSIAN_SIGMA %.17f" % gaussian_sigma,
+        "FLOOR %.17f" % floor,
+        "INIT_COND %d" % ic,
+        "SIGMA %.17f" % sigma,
+        "MOMOPT_MOMENT_ORDER %d" % moment_order,
+        "MOMOPT_QUAD_ORDER %d" % quad_order,
+        "MOMOPT_CFL_FACTOR %.17f" % cfl_factor,
+        "MOMOPT_TOL %.17f" % tol,
+        "MOMOPT_COND_H_MAX %.17f" % cond_h_max,
+        "MOMOPT_COND_H_MAX_BFGS %d" % cond_h_max_bfgs,
+        "MOMOPT_MAX_ITER %d" % max_iter,
+        "MOMOPT_MAX_BFGS_ITER %d" % max_bfgs_iter,
+        "MOMOPT_USE_GAUNT %d" % use_gaunt,
+        "MOMOPT_THETA %.17f" % theta,
+        "MOMOPT_DELTA_PPN %.17f" % delta_ppn,
+        "MOMOPT_MOMENT_TYPE %d" % mt,
+        "MOMOPT_OPTIMIZATION_TYPE %d" % opt_type,
+    ]
+    for k, v in (extra or {}).items():
+        lines.append("%s %s" % (k, v))
+    return "\n".join(lines) + "\n"
+
+
+def regression_deck(init_cond, moment_type, **kw):
+    """The deck the reference's regression harness runs for one momopt golden."""
+    args = dict(num_cells_x=36, num_cells_y=74, a_x=-1.55, b_x=1.45, a_y=-1.62, b_y=1.38,
+                t_final=1.03, sigma=1.111, init_cond=init_cond,
+                gaussian_sigma=0.0 if init_cond == "delta" else 1.7,
+                moment_type=moment_type)
+    args.update(kw)
+    return deck_text(**args)
+
+
+def write_deck(path, text):
+    with open(path, "w") as f:
+        f.write(text)
