@@ -1,0 +1,383 @@
+"""Python binding of libclosures_gpu.so (include/closures_gpu.h) via ctypes.
+
+Mirrors the reference's interfaces for the Mn/PPn path:
+  * ``Solver`` -- MomOptSolver behind the Solver interface (src/solver.h:15-61):
+    built from an input.deck, ``update(dt)`` (momopt_update.cpp:283-382),
+    ``output_data(time)`` (momopt_output.cpp:21-77);
+  * ``Context.solve_batch`` -- the per-vector operator
+    ``opt(n, n2, nq, u, alpha, options, w, p, &outs)`` (opt/opt.cpp:82-148),
+    batched, in place on u and alpha;
+  * ``angular`` -- MomOptSolver::init's quadrature / basis / Gaunt set-up
+    (momopt_init.cpp:88-259).
+Every call goes to the CUDA library; there is no Python or CPU fallback and
+a missing library or device raises ``ClosuresError``.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libclosures_gpu.so")
+
+CL_OK, CL_ERR_ARG, CL_ERR_CUDA, CL_ERR_U0, CL_ERR_MAXREG, CL_ERR_TIMEOUT, CL_ERR_STATE = (
+    0, -1, -2, -3, -4, -5, -6)
+CL_MN, CL_PPN = 0, 1
+CL_FP64, CL_MIXED = 0, 1
+REGULARIZATIONS = (0.0, 1e-3, 1e-2, 1e-1, 5e-1)
+
+
+class ClosuresError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("closures_gpu error %d: %s" % (code, msg))
+        self.code = code
+
+
+class cl_angular(C.Structure):
+    _fields_ = [("order", C.c_int), ("quad_order", C.c_int), ("use_gaunt", C.c_int),
+                ("n", C.c_int), ("n2", C.c_int), ("nq", C.c_int),
+                ("w", C.POINTER(C.c_double)), ("xi", C.POINTER(C.c_double)),
+                ("eta", C.POINTER(C.c_double)), ("p", C.POINTER(C.c_double)),
+                ("gaunt_nnz", C.c_int), ("gaunt_off", C.POINTER(C.c_int)),
+                ("gaunt_idx", C.POINTER(C.c_int)), ("gaunt_val", C.POINTER(C.c_double))]
+
+
+class cl_options(C.Structure):
+    _fields_ = [("moment_type", C.c_int), ("opt_type", C.c_int), ("max_iter", C.c_int),
+                ("tol", C.c_double), ("cond_h_max", C.c_double), ("delta_ppn", C.c_double),
+                ("tol_gamma", C.c_double), ("precision", C.c_int)]
+
+
+class cl_grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("ghost", C.c_int), ("init_cond", C.c_int),
+                ("init_x", C.c_double), ("init_y", C.c_double), ("theta", C.c_double)]
+
+
+class cl_stats(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
+                ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ClosuresError(CL_ERR_STATE, "%s is missing: build it with make -C %s"
+                                % (LIB_PATH, HERE))
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+        sig = {
+            "cl_angular_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(cl_angular)]),
+            "cl_angular_free": (None, [C.POINTER(cl_angular)]),
+            "cl_create": (C.c_int, [C.POINTER(cl_grid), C.POINTER(cl_options),
+                                    C.POINTER(cl_angular), dp, dp, dp, dp, C.POINTER(vp)]),
+            "cl_destroy": (None, [vp]),
+            "cl_last_error": (C.c_char_p, [vp]),
+            "cl_global_error": (C.c_char_p, []),
+            "cl_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+            "cl_step_async": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+            "cl_sync": (C.c_int, [vp]),
+            "cl_get_state": (C.c_int, [vp, dp, dp]),
+            "cl_set_state": (C.c_int, [vp, dp, dp]),
+            "cl_get_stats": (C.c_int, [vp, C.POINTER(cl_stats)]),
+            "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
+            "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
+            "cl_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
+            "cl_multi_create": (C.c_int, [C.c_int, ip, C.c_int, C.c_int, C.POINTER(cl_options),
+                                          C.POINTER(vp)]),
+            "cl_multi_destroy": (None, [vp]),
+            "cl_multi_last_error": (C.c_char_p, [vp]),
+            "cl_multi_solve_device": (C.c_int, [vp, ip, C.POINTER(vp), C.POINTER(vp),
+                                                C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+            "cl_launch_count": (C.c_int64, []),
+            "cl_selftest": (C.c_int, []),
+            "cl_solver_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(vp), dp]),
+            "cl_solver_geometry": (C.c_int, [vp, ip, ip, ip, dp, dp, dp, dp]),
+            "cl_solver_update": (C.c_int, [vp, C.c_double]),
+            "cl_solver_output": (C.c_int, [vp, C.c_double]),
+            "cl_solver_context": (vp, [vp]),
+            "cl_solver_last_error": (C.c_char_p, [vp]),
+            "cl_solver_destroy": (None, [vp]),
+            "cl_run_deck": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _check(rc, msg_fn):
+    if rc != CL_OK:
+        m = msg_fn()
+        raise ClosuresError(rc, m.decode() if isinstance(m, bytes) else str(m))
+
+
+def global_error():
+    return lib().cl_global_error().decode()
+
+
+def launch_count():
+    return int(lib().cl_launch_count())
+
+
+def selftest():
+    _check(lib().cl_selftest(), lib().cl_global_error)
+
+
+class Angular:
+    """Quadrature, basis and Gaunt table (momopt_init.cpp:88-259) as numpy arrays."""
+
+    def __init__(self, order, quad_order, use_gaunt):
+        self._a = cl_angular()
+        _check(lib().cl_angular_create(order, quad_order, int(use_gaunt), C.byref(self._a)),
+               lib().cl_global_error)
+        a = self._a
+        self.order, self.quad_order, self.use_gaunt = a.order, a.quad_order, a.use_gaunt
+        self.n, self.n2, self.nq = a.n, a.n2, a.nq
+        cp = lambda ptr, k: np.ctypeslib.as_array(ptr, shape=(k,)).copy()
+        self.w = cp(a.w, a.nq)
+        self.xi = cp(a.xi, a.nq)
+        self.eta = cp(a.eta, a.nq)
+        self.p = cp(a.p, a.nq * a.n2).reshape(a.nq, a.n2)
+        if a.use_gaunt:
+            self.gaunt_off = cp(a.gaunt_off, a.n * a.n + 1)
+            self.gaunt_idx = cp(a.gaunt_idx, a.gaunt_nnz) if a.gaunt_nnz else np.zeros(0, np.int32)
+            self.gaunt_val = cp(a.gaunt_val, a.gaunt_nnz) if a.gaunt_nnz else np.zeros(0)
+        else:
+            self.gaunt_off = self.gaunt_idx = self.gaunt_val = None
+
+    def __del__(self):
+        if _lib is not None and hasattr(self, "_a"):
+            _lib.cl_angular_free(C.byref(self._a))
+
+
+def make_options(moment_type=CL_MN, max_iter=100, tol=1e-8, cond_h_max=1e10, delta_ppn=1e-10,
+                 tol_gamma=0.0, precision=CL_FP64, opt_type=0):
+    return cl_options(moment_type, opt_type, max_iter, tol, cond_h_max, delta_ppn, tol_gamma,
+                      precision)
+
+
+class Context:
+    """A grid state on the device (cl_create); also serves batched solves."""
+
+    def __init__(self, grid, options, angular, sigma_t, sigma_s, moments, alpha):
+        self._ctx = C.c_void_p()
+        self.n = angular.n
+        self.NX, self.NY = grid.nx + 4, grid.ny + 4
+        st = np.ascontiguousarray(sigma_t, dtype=np.float64)
+        ss = np.ascontiguousarray(sigma_s, dtype=np.float64)
+        m = np.ascontiguousarray(moments, dtype=np.float64)
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        _check(lib().cl_create(C.byref(grid), C.byref(options), C.byref(angular._a), _dp(st),
+                               _dp(ss), _dp(m), _dp(a), C.byref(self._ctx)),
+               lib().cl_global_error)
+
+    @classmethod
+    def for_batches(cls, angular, options):
+        """A minimal 1x1 grid context used only for batched opt() solves."""
+        g = cl_grid(1, 1, 2, 0, 0.0, 0.0, 2.0)
+        C_ = 25
+        n = angular.n
+        m = np.zeros((C_, n))
+        m[:, 0] = 1.0
+        a = np.zeros((C_, n))
+        return cls(g, options, angular, np.ones(C_), np.ones(C_), m, a)
+
+    def close(self):
+        if self._ctx:
+            lib().cl_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_ctx", None):
+            self.close()
+
+    def _err(self):
+        return lib().cl_last_error(self._ctx)
+
+    def step(self, dt, dx, dy):
+        _check(lib().cl_step(self._ctx, dt, dx, dy), self._err)
+
+    def step_async(self, dt, dx, dy):
+        _check(lib().cl_step_async(self._ctx, dt, dx, dy), self._err)
+
+    def sync(self):
+        _check(lib().cl_sync(self._ctx), self._err)
+
+    def get_state(self):
+        m = np.empty((self.NX * self.NY, self.n))
+        a = np.empty((self.NX * self.NY, self.n))
+        _check(lib().cl_get_state(self._ctx, _dp(m), _dp(a)), self._err)
+        return m.reshape(self.NX, self.NY, self.n), a.reshape(self.NX, self.NY, self.n)
+
+    def set_state(self, moments, alpha):
+        m = np.ascontiguousarray(moments, dtype=np.float64)
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        _check(lib().cl_set_state(self._ctx, _dp(m), _dp(a)), self._err)
+
+    def stats(self):
+        s = cl_stats()
+        _check(lib().cl_get_stats(self._ctx, C.byref(s)), self._err)
+        return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
+                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter}
+
+    def solve_batch(self, u, alpha, check=True):
+        """opt() on every row of u/alpha (in place).  Returns iters, reg, status."""
+        count = u.shape[0]
+        assert u.dtype == np.float64 and alpha.dtype == np.float64
+        assert u.flags.c_contiguous and alpha.flags.c_contiguous
+        iters = np.zeros(count, np.int32)
+        reg = np.zeros(count)
+        status = np.zeros(count, np.int32)
+        rc = lib().cl_solve_batch(self._ctx, count, _dp(u), _dp(alpha), _ip(iters), _dp(reg),
+                                  _ip(status))
+        if check:
+            _check(rc, self._err)
+        return iters, reg, status
+
+    def solve_batch_device(self, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None, count=None):
+        """Device-pointer form (torch tensors or raw addresses)."""
+        ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+        _check(lib().cl_solve_batch_device(self._ctx, count, ptr(d_u), ptr(d_alpha), ptr(d_iters),
+                                           ptr(d_reg), ptr(d_status)), self._err)
+
+    def device_state(self):
+        m, a = C.c_void_p(), C.c_void_p()
+        _check(lib().cl_device_state(self._ctx, C.byref(m), C.byref(a)), self._err)
+        return m.value, a.value
+
+
+class MultiSolver:
+    """Several moment orders at one quadrature order, one persistent launch."""
+
+    def __init__(self, orders, quad_order, use_gaunt, options):
+        self._m = C.c_void_p()
+        self.orders = list(orders)
+        arr = (C.c_int * len(orders))(*orders)
+        _check(lib().cl_multi_create(len(orders), arr, quad_order, int(use_gaunt),
+                                     C.byref(options), C.byref(self._m)), lib().cl_global_error)
+
+    def solve_device(self, counts, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None):
+        k = len(self.orders)
+        ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+        arr = lambda ts: None if ts is None else (C.c_void_p * k)(*[ptr(t) for t in ts])
+        cnt = (C.c_int * k)(*counts)
+        _check(lib().cl_multi_solve_device(self._m, cnt, arr(d_u), arr(d_alpha), arr(d_iters),
+                                           arr(d_reg), arr(d_status)),
+               lambda: lib().cl_multi_last_error(self._m))
+
+    def close(self):
+        if self._m:
+            lib().cl_multi_destroy(self._m)
+            self._m = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_m", None):
+            self.close()
+
+
+class Solver:
+    """MomOptSolver on the B200, driven like the reference's Solver."""
+
+    def __init__(self, deck_path, out_dir="."):
+        self._s = C.c_void_p()
+        md = C.c_double()
+        _check(lib().cl_solver_create(deck_path.encode(), out_dir.encode(), C.byref(self._s),
+                                      C.byref(md)), lib().cl_global_error)
+        self.max_dt = md.value
+        nx, ny, n = C.c_int(), C.c_int(), C.c_int()
+        dx, dy, tf, odt = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        lib().cl_solver_geometry(self._s, C.byref(nx), C.byref(ny), C.byref(n), C.byref(dx),
+                                 C.byref(dy), C.byref(tf), C.byref(odt))
+        self.nx, self.ny, self.n = nx.value, ny.value, n.value
+        self.dx, self.dy, self.t_final, self.out_delta_t = dx.value, dy.value, tf.value, odt.value
+        self.NX, self.NY = self.nx + 4, self.ny + 4
+
+    def _err(self):
+        return lib().cl_solver_last_error(self._s)
+
+    def update(self, dt):
+        _check(lib().cl_solver_update(self._s, dt), self._err)
+
+    def output_data(self, time):
+        _check(lib().cl_solver_output(self._s, time), self._err)
+
+    def context_state(self):
+        ctx = lib().cl_solver_context(self._s)
+        m = np.empty((self.NX * self.NY, self.n))
+        a = np.empty((self.NX * self.NY, self.n))
+        _check(lib().cl_get_state(ctx, _dp(m), _dp(a)), lambda: lib().cl_last_error(ctx))
+        return m.reshape(self.NX, self.NY, self.n), a.reshape(self.NX, self.NY, self.n)
+
+    def stats(self):
+        ctx = lib().cl_solver_context(self._s)
+        s = cl_stats()
+        _check(lib().cl_get_stats(ctx, C.byref(s)), lambda: lib().cl_last_error(ctx))
+        return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
+                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter}
+
+    def close(self):
+        if self._s:
+            lib().cl_solver_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_s", None):
+            self.close()
+
+
+def run_deck(deck_path, out_dir=".", max_steps=-1):
+    """main.cpp:204-230 on the device; writes out_<t>_0.{pn,opt} to out_dir."""
+    _check(lib().cl_run_deck(deck_path.encode(), out_dir.encode(), max_steps),
+           lib().cl_global_error)
+
+
+def sample_moment_vectors(angular, count, seed=12345, s_range=(0.1, 20.0)):
+    """Synthetic realizable moment vectors of the batched-optimisation workload.
+
+    alpha_k ~ N(0, s^2) for k >= 1 with s log-uniform in s_range, alpha_0 set
+    so that u_0 = 1, and u = <m exp(alpha.m)> evaluated in FP64 on the same
+    quadrature (log-sum-exp scaled).  Returns (u, alpha_exact), each [count, n].
+    """
+    rng = np.random.default_rng(seed)
+    n = angular.n
+    P = angular.p[:, :n]                     # [nq, n]
+    w = angular.w
+    s = np.exp(rng.uniform(np.log(s_range[0]), np.log(s_range[1]), size=count))
+    alpha = rng.standard_normal((count, n)) * s[:, None]
+    alpha[:, 0] = 0.0
+    u = np.empty((count, n))
+    p0 = P[0, 0]
+    for b in range(0, count, 4096):
+        a = alpha[b:b + 4096]
+        e = a @ P.T                          # [B, nq]
+        mx = e.max(axis=1, keepdims=True)
+        ex = np.exp(e - mx) * w[None, :]
+        mom = ex @ P                         # [B, n] scaled by exp(-mx)
+        # u0 = exp(mx + a0 p0) * mom0 = 1  ->  a0 = -(mx + log mom0) / p0
+        a0 = -(mx[:, 0] + np.log(mom[:, 0])) / p0
+        alpha[b:b + 4096, 0] = a0
+        u[b:b + 4096] = mom / mom[:, :1]
+    return u, alpha
+
+
+def isotropic_alpha(n, count, moment_type=CL_MN, delta=1e-10):
+    """opt.cpp:27-46 for u = (1, 0, ..., 0)."""
+    a = np.zeros((count, n))
+    a[:, 0] = (2.0 * np.sqrt(np.pi) * np.log(0.5 / np.sqrt(np.pi)) if moment_type == CL_MN
+               else 1.0 - 4.0 * delta * np.pi)
+    return a

@@ -1,0 +1,894 @@
+// capi.cu -- implementation of the C ABI declared in include/closures_gpu.h.
+//
+// Owns the device state of one grid (moments, alpha, saved moments, sigma
+// fields), the device copies of the angular set-up in the layouts the
+// kernels want, one stream and the captured RK2 graph.
+#include "closures_gpu.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../host/angular.h"
+#include "common.cuh"
+#include "flux.cuh"
+#include "newton.cuh"
+
+using namespace clb;
+
+static std::atomic<long long> g_launches{0};
+static thread_local std::string g_global_err;
+
+#define CUDA_TRY(ctx, call)                                                                    \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+            return CL_ERR_CUDA;                                                                \
+        }                                                                                      \
+    } while (0)
+
+namespace {
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// Device copy of one moment order's angular data in the kernels' layouts.
+struct DeviceBasis {
+    int n = 0, n2 = 0, nq = 0, nb = 0, K2p = 0, nqp = 0, ldP = 0, ldPf = 0, useGaunt = 0;
+    double p0 = 0;
+    double *P = nullptr, *w = nullptr;            // Newton layout
+    double *Pf = nullptr, *xi = nullptr, *eta = nullptr, *cxw = nullptr, *cyw = nullptr;  // flux
+    int *hoff = nullptr, *hidx = nullptr;
+    double *hval = nullptr;
+    unsigned short *pairs = nullptr;
+
+    void release()
+    {
+        cudaFree(P);
+        cudaFree(w);
+        cudaFree(Pf);
+        cudaFree(xi);
+        cudaFree(eta);
+        cudaFree(cxw);
+        cudaFree(cyw);
+        cudaFree(hoff);
+        cudaFree(hidx);
+        cudaFree(hval);
+        cudaFree(pairs);
+        *this = DeviceBasis();
+    }
+};
+
+template <class T>
+cudaError_t upload(T **dst, const std::vector<T> &src)
+{
+    cudaError_t e = cudaMalloc((void **)dst, sizeof(T) * (src.empty() ? 1 : src.size()));
+    if (e != cudaSuccess)
+        return e;
+    if (!src.empty())
+        e = cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// n, n2, nq, w, xi, eta, p[nq*n2], Gaunt CSR -> device layouts.
+cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGaunt, const double *w,
+                               const double *xi, const double *eta, const double *p, const int *goff,
+                               const int *gidx, const double *gval, int gnnz)
+{
+    B.n = n;
+    B.n2 = n2;
+    B.nq = nq;
+    B.useGaunt = useGaunt;
+    B.nb = round_up(n, 8);
+    const int K2 = useGaunt ? n2 : n * (n + 1) / 2;
+    B.K2p = round_up(K2, 8);
+    B.nqp = round_up(nq, 32);
+    int ldP = B.nb + B.K2p;
+    while (ldP % 16 != 4)
+        ldP++;
+    B.ldP = ldP;
+    B.ldPf = B.nb + 4;
+    B.p0 = p[0];
+    std::vector<double> P((size_t)B.nqp * ldP, 0.0), W(B.nqp, 0.0);
+    std::vector<double> Pf((size_t)B.nqp * B.ldPf, 0.0), XI(B.nqp, 0.0), ET(B.nqp, 0.0), CX(B.nqp, 0.0),
+        CY(B.nqp, 0.0);
+    for (int q = 0; q < nq; q++) {
+        const double *pq = p + (size_t)q * n2;
+        double *row = &P[(size_t)q * ldP];
+        for (int k = 0; k < n; k++)
+            row[k] = pq[k];
+        if (useGaunt) {
+            for (int k = 0; k < n2; k++)
+                row[B.nb + k] = pq[k];
+        } else {
+            int c = 0;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j <= i; j++)
+                    row[B.nb + c++] = pq[i] * pq[j];
+        }
+        W[q] = w[q];
+        for (int k = 0; k < n; k++)
+            Pf[(size_t)q * B.ldPf + k] = pq[k];
+        XI[q] = xi[q];
+        ET[q] = eta[q];
+        CX[q] = xi[q] * w[q];
+        CY[q] = eta[q] * w[q];
+    }
+    std::vector<unsigned short> pairs;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j <= i; j++)
+            pairs.push_back((unsigned short)((i << 8) | j));
+    for (int k = 0; k < n; k++)
+        for (int i = k; i < n; i++)
+            pairs.push_back((unsigned short)((i << 8) | k));
+    cudaError_t e;
+    if ((e = upload(&B.P, P)) != cudaSuccess) return e;
+    if ((e = upload(&B.w, W)) != cudaSuccess) return e;
+    if ((e = upload(&B.Pf, Pf)) != cudaSuccess) return e;
+    if ((e = upload(&B.xi, XI)) != cudaSuccess) return e;
+    if ((e = upload(&B.eta, ET)) != cudaSuccess) return e;
+    if ((e = upload(&B.cxw, CX)) != cudaSuccess) return e;
+    if ((e = upload(&B.cyw, CY)) != cudaSuccess) return e;
+    if ((e = upload(&B.pairs, pairs)) != cudaSuccess) return e;
+    if (useGaunt) {
+        std::vector<int> off(goff, goff + n * n + 1), idx(gidx, gidx + gnnz);
+        std::vector<double> val(gval, gval + gnnz);
+        if ((e = upload(&B.hoff, off)) != cudaSuccess) return e;
+        if ((e = upload(&B.hidx, idx)) != cudaSuccess) return e;
+        if ((e = upload(&B.hval, val)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+NewtonProblem make_problem(const DeviceBasis &B)
+{
+    NewtonProblem pb;
+    memset(&pb, 0, sizeof(pb));
+    pb.P = B.P;
+    pb.w = B.w;
+    pb.hoff = B.hoff;
+    pb.hidx = B.hidx;
+    pb.hval = B.hval;
+    pb.pairs = B.pairs;
+    pb.p0 = B.p0;
+    pb.n = B.n;
+    pb.nb = B.nb;
+    pb.K2p = B.K2p;
+    pb.nqp = B.nqp;
+    pb.ldP = B.ldP;
+    return pb;
+}
+
+int check_options(const cl_options *o, std::string &err)
+{
+    if (!o) {
+        err = "null options";
+        return CL_ERR_ARG;
+    }
+    if (o->opt_type != 0) {
+        err = "MOMOPT_OPTIMIZATION_TYPE " + std::to_string(o->opt_type) +
+              " (change of basis / BFGS) is not provided by the B200 path";
+        return CL_ERR_ARG;
+    }
+    if (o->moment_type != CL_MN && o->moment_type != CL_PPN) {
+        err = "moment type out of range";
+        return CL_ERR_ARG;
+    }
+    if (o->precision != CL_FP64 && o->precision != CL_MIXED) {
+        err = "precision must be CL_FP64 or CL_MIXED";
+        return CL_ERR_ARG;
+    }
+    if (o->max_iter < 1) {
+        err = "MOMOPT_MAX_ITER must be >= 1";
+        return CL_ERR_ARG;
+    }
+    return CL_OK;
+}
+
+void fill_newton_options(NewtonArgs &a, const cl_options &o, int useGaunt)
+{
+    a.momentType = o.moment_type;
+    a.maxIter = o.max_iter;
+    a.useGaunt = useGaunt;
+    a.tolRel = o.tol;
+    a.condHMax = o.cond_h_max;
+    a.deltaPPn = o.delta_ppn;
+    a.tolGamma = o.tol_gamma;
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+const char *error_text(int code)
+{
+    switch (code) {
+    case CL_ERR_U0:
+        return "u[0] < 0";
+    case CL_ERR_MAXREG:
+        return "Max regularization achieved.";
+    case CL_ERR_TIMEOUT:
+        return "device wait timed out";
+    default:
+        return "device error";
+    }
+}
+
+}  // namespace
+
+struct cl_ctx {
+    cudaStream_t stream = nullptr;
+    cl_grid grid;
+    cl_options opt;
+    int n = 0, NX = 0, NY = 0;
+    long long C = 0;
+    DeviceBasis B;
+    double *dMom = nullptr, *dAlpha = nullptr, *dOld = nullptr, *dSigT = nullptr, *dSigS = nullptr;
+    unsigned int *dQueue = nullptr;   // [4]: stage 1, stage 2, batch, spare
+    DevStats *dStats = nullptr;
+    int *dErr = nullptr;
+    int *hErr = nullptr;              // pinned [2]
+    NewtonArgs nargs;
+    FluxArgs fargs;
+    int nCtas = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double gdt = 0, gdx = 0, gdy = 0;
+    int graphKernels = 0;
+    // batch scratch (grow only)
+    double *bU = nullptr, *bA = nullptr, *bR = nullptr;
+    int *bI = nullptr, *bS = nullptr;
+    long long bCap = 0;
+    std::string err;
+};
+
+extern "C" {
+
+const char *cl_global_error(void) { return g_global_err.c_str(); }
+
+int cl_angular_create(int order, int quad_order, int use_gaunt, cl_angular *out)
+{
+    if (!out) {
+        g_global_err = "null output";
+        return CL_ERR_ARG;
+    }
+    memset(out, 0, sizeof(*out));
+    Angular A;
+    if (build_angular(order, quad_order, use_gaunt, A) != 0) {
+        g_global_err = "unsupported order/quadrature (order 1..6, Q >= 2 even)";
+        return CL_ERR_ARG;
+    }
+    out->order = A.order;
+    out->quad_order = A.Q;
+    out->use_gaunt = A.useGaunt;
+    out->n = A.n;
+    out->n2 = A.n2;
+    out->nq = A.nq;
+    auto dup = [](const std::vector<double> &v) {
+        double *p = (double *)malloc(sizeof(double) * (v.size() ? v.size() : 1));
+        if (!v.empty())
+            memcpy(p, v.data(), sizeof(double) * v.size());
+        return p;
+    };
+    out->w = dup(A.w);
+    out->xi = dup(A.xi);
+    out->eta = dup(A.eta);
+    out->p = dup(A.p);
+    out->gaunt_nnz = (int)A.gidx.size();
+    if (A.useGaunt) {
+        out->gaunt_off = (int *)malloc(sizeof(int) * A.goff.size());
+        memcpy(out->gaunt_off, A.goff.data(), sizeof(int) * A.goff.size());
+        out->gaunt_idx = (int *)malloc(sizeof(int) * (A.gidx.size() + 1));
+        memcpy(out->gaunt_idx, A.gidx.data(), sizeof(int) * A.gidx.size());
+        out->gaunt_val = dup(A.gval);
+    }
+    return CL_OK;
+}
+
+void cl_angular_free(cl_angular *a)
+{
+    if (!a)
+        return;
+    free(a->w);
+    free(a->xi);
+    free(a->eta);
+    free(a->p);
+    free(a->gaunt_off);
+    free(a->gaunt_idx);
+    free(a->gaunt_val);
+    memset(a, 0, sizeof(*a));
+}
+
+const char *cl_last_error(const cl_ctx *ctx) { return ctx ? ctx->err.c_str() : g_global_err.c_str(); }
+
+int64_t cl_launch_count(void) { return (int64_t)g_launches.load(); }
+
+static int ctx_fail(cl_ctx *ctx, int code)
+{
+    g_global_err = ctx->err;
+    cl_destroy(ctx);
+    return code;
+}
+
+int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang, const double *sigma_t,
+              const double *sigma_s, const double *moments, const double *alpha, cl_ctx **out)
+{
+    if (!out || !grid || !ang || !sigma_t || !sigma_s || !moments || !alpha) {
+        g_global_err = "null argument";
+        return CL_ERR_ARG;
+    }
+    *out = nullptr;
+    std::string e;
+    int rc = check_options(opts, e);
+    if (rc) {
+        g_global_err = e;
+        return rc;
+    }
+    if (grid->ghost != 2 || grid->nx < 1 || grid->ny < 1) {
+        g_global_err = "grid must have nx, ny >= 1 and 2 ghost cells";
+        return CL_ERR_ARG;
+    }
+    if (ang->n < 1 || ang->n > kMaxN || ang->nq < 1 || !ang->p || !ang->w) {
+        g_global_err = "angular set-up missing or order > 6";
+        return CL_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        g_global_err = "no CUDA device (the B200 path has no CPU fallback)";
+        return CL_ERR_CUDA;
+    }
+    cl_ctx *ctx = new cl_ctx();
+    ctx->grid = *grid;
+    ctx->opt = *opts;
+    ctx->n = ang->n;
+    ctx->NX = grid->nx + 4;
+    ctx->NY = grid->ny + 4;
+    ctx->C = (long long)ctx->NX * ctx->NY;
+    const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, ang->use_gaunt, ang->w, ang->xi,
+                                        ang->eta, ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
+                                        ang->gaunt_nnz);
+    if (ce != cudaSuccess) {
+        ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
+        return ctx_fail(ctx, CL_ERR_CUDA);
+    }
+    if (cudaMalloc(&ctx->dMom, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dAlpha, C * n * 8) != cudaSuccess ||
+        cudaMalloc(&ctx->dOld, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dSigT, C * 8) != cudaSuccess ||
+        cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->dStats, sizeof(DevStats)) != cudaSuccess || cudaMalloc(&ctx->dErr, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess) {
+        ctx->err = "device allocation failed";
+        return ctx_fail(ctx, CL_ERR_CUDA);
+    }
+    cudaMemcpy(ctx->dMom, moments, C * n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->dAlpha, alpha, C * n * 8, cudaMemcpyHostToDevice);
+    cudaMemset(ctx->dOld, 0, C * n * 8);
+    cudaMemcpy(ctx->dSigT, sigma_t, C * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx->dSigS, sigma_s, C * 8, cudaMemcpyHostToDevice);
+    cudaMemset(ctx->dStats, 0, sizeof(DevStats));
+    cudaMemset(ctx->dErr, 0, 2 * sizeof(int));
+    ctx->hErr[0] = ctx->hErr[1] = 0;
+
+    NewtonArgs &a = ctx->nargs;
+    memset(&a, 0, sizeof(a));
+    a.nprob = 1;
+    a.prob[0] = make_problem(ctx->B);
+    fill_newton_options(a, *opts, ang->use_gaunt);
+    a.stats = ctx->dStats;
+    a.err = ctx->dErr;
+    a.NX = ctx->NX;
+    a.NY = ctx->NY;
+    if (plan_newton(a) != 0) {
+        ctx->err = "Newton kernel layout does not fit in shared memory";
+        return ctx_fail(ctx, CL_ERR_ARG);
+    }
+    if ((ce = prepare_newton(a)) != cudaSuccess) {
+        ctx->err = std::string("Newton kernel attributes: ") + cudaGetErrorString(ce);
+        return ctx_fail(ctx, CL_ERR_CUDA);
+    }
+    ctx->nCtas = sm_count() * newton_ctas_per_sm(a);
+
+    FluxArgs &f = ctx->fargs;
+    memset(&f, 0, sizeof(f));
+    f.alpha = ctx->dAlpha;
+    f.moments = ctx->dMom;
+    f.sigmaT = ctx->dSigT;
+    f.sigmaS = ctx->dSigS;
+    f.P = ctx->B.Pf;
+    f.xi = ctx->B.xi;
+    f.eta = ctx->B.eta;
+    f.cxw = ctx->B.cxw;
+    f.cyw = ctx->B.cyw;
+    f.n = ctx->n;
+    f.nb = ctx->B.nb;
+    f.ldPf = ctx->B.ldPf;
+    f.nqp = ctx->B.nqp;
+    f.NX = ctx->NX;
+    f.NY = ctx->NY;
+    f.momentType = opts->moment_type;
+    f.initCond = grid->init_cond;
+    f.theta = grid->theta;
+    f.deltaPPn = opts->delta_ppn;
+    f.initX = grid->init_x;
+    f.initY = grid->init_y;
+    if (plan_flux(f) != 0) {
+        ctx->err = "flux kernel layout does not fit in shared memory";
+        return ctx_fail(ctx, CL_ERR_ARG);
+    }
+    if ((ce = prepare_flux(f)) != cudaSuccess) {
+        ctx->err = std::string("flux kernel attributes: ") + cudaGetErrorString(ce);
+        return ctx_fail(ctx, CL_ERR_CUDA);
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        ctx->err = std::string("set-up: ") + cudaGetErrorString(cudaGetLastError());
+        return ctx_fail(ctx, CL_ERR_CUDA);
+    }
+    *out = ctx;
+    return CL_OK;
+}
+
+void cl_destroy(cl_ctx *ctx)
+{
+    if (!ctx)
+        return;
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    if (ctx->exec)
+        cudaGraphExecDestroy(ctx->exec);
+    if (ctx->graph)
+        cudaGraphDestroy(ctx->graph);
+    ctx->B.release();
+    cudaFree(ctx->dMom);
+    cudaFree(ctx->dAlpha);
+    cudaFree(ctx->dOld);
+    cudaFree(ctx->dSigT);
+    cudaFree(ctx->dSigS);
+    cudaFree(ctx->dQueue);
+    cudaFree(ctx->dStats);
+    cudaFree(ctx->dErr);
+    cudaFreeHost(ctx->hErr);
+    cudaFree(ctx->bU);
+    cudaFree(ctx->bA);
+    cudaFree(ctx->bR);
+    cudaFree(ctx->bI);
+    cudaFree(ctx->bS);
+    if (ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// Enqueues one RK2 step on the context's stream (uncaptured form).
+static cudaError_t enqueue_step(cl_ctx *ctx, double dt, double dx, double dy, int *kernels)
+{
+    cudaError_t e;
+    int nk = 0;
+    const bool periodic = ctx->grid.init_cond == 2;
+    if ((e = cudaMemsetAsync(ctx->dQueue, 0, 2 * sizeof(unsigned), ctx->stream)) != cudaSuccess)
+        return e;
+    for (int stage = 0; stage < 2; stage++) {
+        if (periodic) {
+            if ((e = launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, ctx->stream)) != cudaSuccess)
+                return e;
+            nk += 2;
+        }
+        NewtonArgs a = ctx->nargs;
+        a.prob[0].count = (int)ctx->C;
+        a.prob[0].u = ctx->dMom;
+        a.prob[0].alpha = ctx->dAlpha;
+        a.prob[0].queue = ctx->dQueue + stage;
+        a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
+        if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
+            return e;
+        nk++;
+        FluxArgs f = ctx->fargs;
+        f.dt = dt;
+        f.dx = dx;
+        f.dy = dy;
+        f.momentsOld = (stage == 1) ? ctx->dOld : nullptr;
+        if ((e = launch_flux(f, ctx->stream)) != cudaSuccess)
+            return e;
+        nk++;
+    }
+    if (kernels)
+        *kernels = nk;
+    return cudaSuccess;
+}
+
+static int read_device_error(cl_ctx *ctx)
+{
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->hErr, ctx->dErr, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->hErr[0] != 0) {
+        long long cell = ctx->hErr[1];
+        char buf[256];
+        if (ctx->NY > 0 && cell < ctx->C)
+            snprintf(buf, sizeof(buf), "%s (cell i=%lld j=%lld)", error_text(ctx->hErr[0]), cell / ctx->NY,
+                     cell % ctx->NY);
+        else
+            snprintf(buf, sizeof(buf), "%s (vector %lld)", error_text(ctx->hErr[0]), cell);
+        ctx->err = buf;
+        return ctx->hErr[0];
+    }
+    return CL_OK;
+}
+
+int cl_step_async(cl_ctx *ctx, double dt, double dx, double dy)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    if (!ctx->exec || dt != ctx->gdt || dx != ctx->gdx || dy != ctx->gdy) {
+        if (ctx->exec) {
+            cudaGraphExecDestroy(ctx->exec);
+            ctx->exec = nullptr;
+        }
+        if (ctx->graph) {
+            cudaGraphDestroy(ctx->graph);
+            ctx->graph = nullptr;
+        }
+        CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int nk = 0;
+        cudaError_t e = enqueue_step(ctx, dt, dx, dy, &nk);
+        cudaGraph_t gph = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &gph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (gph)
+                cudaGraphDestroy(gph);
+            ctx->err = std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2);
+            return CL_ERR_CUDA;
+        }
+        ctx->graph = gph;
+        CUDA_TRY(ctx, cudaGraphInstantiate(&ctx->exec, ctx->graph, 0));
+        ctx->gdt = dt;
+        ctx->gdx = dx;
+        ctx->gdy = dy;
+        ctx->graphKernels = nk;
+    }
+    CUDA_TRY(ctx, cudaGraphLaunch(ctx->exec, ctx->stream));
+    g_launches += ctx->graphKernels;
+    return CL_OK;
+}
+
+int cl_sync(cl_ctx *ctx)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    return read_device_error(ctx);
+}
+
+int cl_step(cl_ctx *ctx, double dt, double dx, double dy)
+{
+    int rc = cl_step_async(ctx, dt, dx, dy);
+    if (rc)
+        return rc;
+    return cl_sync(ctx);
+}
+
+int cl_get_state(cl_ctx *ctx, double *moments, double *alpha)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    size_t bytes = (size_t)ctx->C * ctx->n * 8;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (moments)
+        CUDA_TRY(ctx, cudaMemcpy(moments, ctx->dMom, bytes, cudaMemcpyDeviceToHost));
+    if (alpha)
+        CUDA_TRY(ctx, cudaMemcpy(alpha, ctx->dAlpha, bytes, cudaMemcpyDeviceToHost));
+    return CL_OK;
+}
+
+int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    size_t bytes = (size_t)ctx->C * ctx->n * 8;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (moments)
+        CUDA_TRY(ctx, cudaMemcpy(ctx->dMom, moments, bytes, cudaMemcpyHostToDevice));
+    if (alpha)
+        CUDA_TRY(ctx, cudaMemcpy(ctx->dAlpha, alpha, bytes, cudaMemcpyHostToDevice));
+    return CL_OK;
+}
+
+int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    if (d_moments)
+        *d_moments = ctx->dMom;
+    if (d_alpha)
+        *d_alpha = ctx->dAlpha;
+    return CL_OK;
+}
+
+int cl_get_stats(cl_ctx *ctx, cl_stats *s)
+{
+    if (!ctx || !s)
+        return CL_ERR_ARG;
+    DevStats d;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(&d, ctx->dStats, sizeof(d), cudaMemcpyDeviceToHost));
+    s->max_iter = d.maxIter;
+    s->num_solves = (int64_t)d.numSolves;
+    s->total_iter = (int64_t)d.totalIter;
+    for (int i = 0; i < CL_NUM_REG; i++)
+        s->hist_reg[i] = (int64_t)d.hist[i];
+    s->iter_mean = d.numSolves ? (double)d.totalIter / (double)d.numSolves : 0.0;
+    return CL_OK;
+}
+
+int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha, int *d_iters, double *d_reg,
+                          int *d_status)
+{
+    if (!ctx || count < 0 || (count > 0 && (!d_u || !d_alpha)))
+        return CL_ERR_ARG;
+    if (count == 0)
+        return CL_OK;
+    NewtonArgs a = ctx->nargs;
+    a.prob[0].count = count;
+    a.prob[0].u = d_u;
+    a.prob[0].alpha = d_alpha;
+    a.prob[0].iters = d_iters;
+    a.prob[0].regs = d_reg;
+    a.prob[0].status = d_status;
+    a.prob[0].queue = ctx->dQueue + 2;
+    a.momentsOld = nullptr;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dQueue + 2, 0, sizeof(unsigned), ctx->stream));
+    CUDA_TRY(ctx, launch_newton(a, ctx->nCtas, ctx->stream));
+    g_launches += 1;
+    return CL_OK;
+}
+
+int cl_solve_batch(cl_ctx *ctx, int count, double *u, double *alpha, int *iters, double *reg, int *status)
+{
+    if (!ctx || count < 0 || (count > 0 && (!u || !alpha)))
+        return CL_ERR_ARG;
+    if (count == 0)
+        return CL_OK;
+    const size_t n = ctx->n;
+    if (count > ctx->bCap) {
+        cudaFree(ctx->bU);
+        cudaFree(ctx->bA);
+        cudaFree(ctx->bR);
+        cudaFree(ctx->bI);
+        cudaFree(ctx->bS);
+        ctx->bU = ctx->bA = ctx->bR = nullptr;
+        ctx->bI = ctx->bS = nullptr;
+        ctx->bCap = 0;
+        CUDA_TRY(ctx, cudaMalloc(&ctx->bU, (size_t)count * n * 8));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->bA, (size_t)count * n * 8));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->bR, (size_t)count * 8));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->bI, (size_t)count * 4));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->bS, (size_t)count * 4));
+        ctx->bCap = count;
+    }
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->bU, u, (size_t)count * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->bA, alpha, (size_t)count * n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dErr, 0, 2 * sizeof(int), ctx->stream));
+    int rc = cl_solve_batch_device(ctx, count, ctx->bU, ctx->bA, ctx->bI, ctx->bR, ctx->bS);
+    if (rc)
+        return rc;
+    CUDA_TRY(ctx, cudaMemcpyAsync(u, ctx->bU, (size_t)count * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(alpha, ctx->bA, (size_t)count * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (iters)
+        CUDA_TRY(ctx, cudaMemcpyAsync(iters, ctx->bI, (size_t)count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (reg)
+        CUDA_TRY(ctx, cudaMemcpyAsync(reg, ctx->bR, (size_t)count * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (status)
+        CUDA_TRY(ctx, cudaMemcpyAsync(status, ctx->bS, (size_t)count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    rc = read_device_error(ctx);
+    cudaMemsetAsync(ctx->dErr, 0, 2 * sizeof(int), ctx->stream);
+    return rc;
+}
+
+// ---------------------------------------------------------------- multi-order
+}  // extern "C"
+
+struct cl_multi {
+    cudaStream_t stream = nullptr;
+    cl_options opt;
+    int nprob = 0;
+    DeviceBasis B[kMaxProblems];
+    NewtonArgs nargs;
+    unsigned int *dQueue = nullptr;
+    DevStats *dStats = nullptr;
+    int *dErr = nullptr;
+    int nCtas = 0;
+    std::string err;
+};
+
+extern "C" {
+
+const char *cl_multi_last_error(const cl_multi *m) { return m ? m->err.c_str() : g_global_err.c_str(); }
+
+void cl_multi_destroy(cl_multi *m)
+{
+    if (!m)
+        return;
+    if (m->stream)
+        cudaStreamSynchronize(m->stream);
+    for (int p = 0; p < m->nprob; p++)
+        m->B[p].release();
+    cudaFree(m->dQueue);
+    cudaFree(m->dStats);
+    cudaFree(m->dErr);
+    if (m->stream)
+        cudaStreamDestroy(m->stream);
+    delete m;
+}
+
+int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaunt, const cl_options *opts,
+                    cl_multi **out)
+{
+    if (!out || !orders || norders < 1 || norders > kMaxProblems) {
+        g_global_err = "bad order list";
+        return CL_ERR_ARG;
+    }
+    *out = nullptr;
+    std::string e;
+    int rc = check_options(opts, e);
+    if (rc) {
+        g_global_err = e;
+        return rc;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        g_global_err = "no CUDA device (the B200 path has no CPU fallback)";
+        return CL_ERR_CUDA;
+    }
+    cl_multi *m = new cl_multi();
+    m->opt = *opts;
+    m->nprob = norders;
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        g_global_err = "stream creation failed";
+        cl_multi_destroy(m);
+        return CL_ERR_CUDA;
+    }
+    NewtonArgs &a = m->nargs;
+    memset(&a, 0, sizeof(a));
+    a.nprob = norders;
+    for (int p = 0; p < norders; p++) {
+        Angular A;
+        if (build_angular(orders[p], quad_order, use_gaunt, A) != 0) {
+            g_global_err = "unsupported order";
+            cl_multi_destroy(m);
+            return CL_ERR_ARG;
+        }
+        cudaError_t ce = build_device_basis(m->B[p], A.n, A.n2, A.nq, A.useGaunt, A.w.data(), A.xi.data(),
+                                            A.eta.data(), A.p.data(), A.goff.data(), A.gidx.data(),
+                                            A.gval.data(), (int)A.gidx.size());
+        if (ce != cudaSuccess) {
+            g_global_err = std::string("basis upload: ") + cudaGetErrorString(ce);
+            cl_multi_destroy(m);
+            return CL_ERR_CUDA;
+        }
+        a.prob[p] = make_problem(m->B[p]);
+    }
+    fill_newton_options(a, *opts, use_gaunt ? 1 : 0);
+    if (cudaMalloc(&m->dQueue, kMaxProblems * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&m->dStats, sizeof(DevStats)) != cudaSuccess || cudaMalloc(&m->dErr, 2 * sizeof(int)) != cudaSuccess) {
+        g_global_err = "device allocation failed";
+        cl_multi_destroy(m);
+        return CL_ERR_CUDA;
+    }
+    cudaMemset(m->dStats, 0, sizeof(DevStats));
+    cudaMemset(m->dErr, 0, 2 * sizeof(int));
+    a.stats = m->dStats;
+    a.err = m->dErr;
+    if (plan_newton(a) != 0) {
+        g_global_err = "Newton kernel layout does not fit in shared memory";
+        cl_multi_destroy(m);
+        return CL_ERR_ARG;
+    }
+    if (prepare_newton(a) != cudaSuccess) {
+        g_global_err = "Newton kernel attributes";
+        cl_multi_destroy(m);
+        return CL_ERR_CUDA;
+    }
+    m->nCtas = sm_count() * newton_ctas_per_sm(a);
+    cudaDeviceSynchronize();
+    *out = m;
+    return CL_OK;
+}
+
+int cl_multi_solve_device(cl_multi *m, const int *counts, double *const *d_u, double *const *d_alpha,
+                          int *const *d_iters, double *const *d_reg, int *const *d_status)
+{
+    if (!m || !counts || !d_u || !d_alpha)
+        return CL_ERR_ARG;
+    NewtonArgs a = m->nargs;
+    for (int p = 0; p < m->nprob; p++) {
+        a.prob[p].count = counts[p];
+        a.prob[p].u = d_u[p];
+        a.prob[p].alpha = d_alpha[p];
+        a.prob[p].iters = d_iters ? d_iters[p] : nullptr;
+        a.prob[p].regs = d_reg ? d_reg[p] : nullptr;
+        a.prob[p].status = d_status ? d_status[p] : nullptr;
+        a.prob[p].queue = m->dQueue + p;
+    }
+    cudaError_t e = cudaMemsetAsync(m->dQueue, 0, kMaxProblems * sizeof(unsigned), m->stream);
+    if (e == cudaSuccess)
+        e = launch_newton(a, m->nCtas, m->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(m->stream);
+    g_launches += 1;
+    if (e != cudaSuccess) {
+        m->err = std::string("multi solve: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    int herr[2];
+    cudaMemcpy(herr, m->dErr, sizeof(herr), cudaMemcpyDeviceToHost);
+    if (herr[0]) {
+        m->err = error_text(herr[0]);
+        cudaMemset(m->dErr, 0, sizeof(herr));
+        return herr[0];
+    }
+    return CL_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- self check
+namespace {
+__global__ void dmma_selftest_kernel(const double *A, const double *B, double *C)
+{
+    // one warp: C[16x8] = A[16x8] . B[8x8] (A row-major, B row-major k x n)
+    int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    double c[4] = {0, 0, 0, 0};
+    dmma16x8x8(c, A[g * 8 + t], A[(g + 8) * 8 + t], A[g * 8 + t + 4], A[(g + 8) * 8 + t + 4], B[t * 8 + g],
+               B[(t + 4) * 8 + g]);
+    C[g * 8 + 2 * t] = c[0];
+    C[g * 8 + 2 * t + 1] = c[1];
+    C[(g + 8) * 8 + 2 * t] = c[2];
+    C[(g + 8) * 8 + 2 * t + 1] = c[3];
+}
+}  // namespace
+
+extern "C" int cl_selftest(void)
+{
+    double hA[128], hB[64], hC[128], ref[128];
+    for (int i = 0; i < 128; i++)
+        hA[i] = 0.25 * (i % 13) - 1.0 + 1e-3 * i;
+    for (int i = 0; i < 64; i++)
+        hB[i] = 0.5 * (i % 7) - 1.5 + 1e-4 * i;
+    for (int r = 0; r < 16; r++)
+        for (int c = 0; c < 8; c++) {
+            double s = 0;
+            for (int k = 0; k < 8; k++)
+                s += hA[r * 8 + k] * hB[k * 8 + c];
+            ref[r * 8 + c] = s;
+        }
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 320) != cudaSuccess) {
+        g_global_err = "selftest allocation failed";
+        return CL_ERR_CUDA;
+    }
+    cudaMemcpy(d, hA, sizeof(hA), cudaMemcpyHostToDevice);
+    cudaMemcpy(d + 128, hB, sizeof(hB), cudaMemcpyHostToDevice);
+    dmma_selftest_kernel<<<1, 32>>>(d, d + 128, d + 192);
+    g_launches += 1;
+    cudaError_t e = cudaMemcpy(hC, d + 192, sizeof(hC), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        g_global_err = std::string("selftest: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    for (int i = 0; i < 128; i++)
+        if (std::fabs(hC[i] - ref[i]) > 1e-12 * (1.0 + std::fabs(ref[i]))) {
+            g_global_err = "DMMA fragment layout mismatch";
+            return CL_ERR_STATE;
+        }
+    return CL_OK;
+}
+
+// Lets the host solver layer report through cl_global_error().
+void clb_set_global_error(const char *msg) { g_global_err = msg ? msg : ""; }

@@ -1,0 +1,293 @@
+// flux.cu -- second-order kinetic flux, Euler/collision/source update and
+// Heun average for one RK stage, fused in one kernel.
+//
+// Replaces MomOptSolver::solveFlux (src/momopt/momopt_update.cpp:96-202) and
+// the stage updates (:316-336, :344-364, :367-377).  The reference loops q
+// outermost and streams a whole-grid ansatz array once per quadrature point;
+// here a CTA owns an 8 x 16 tile of interior cells and, per q-chunk:
+//   1. ansatz on the tile + 2-cell halo: S = alpha . P^T on the FP64 tensor
+//      cores (DMMA), then exp (Mn) or the PPn closure (computeAnsatz :38-69);
+//   2. the limited upwind stencil per (cell, q): slopefit / minmod with theta
+//      (:77-90), the four upwind branches by sign(xi_q), sign(eta_q)
+//      (:145-188), F = (flux1+flux2)/dx + (flux3+flux4)/dy;
+//   3. projection flux_k += F . p_qk on the tensor cores.
+// The epilogue applies u0*(1+dt sigma_s-dt sigma_t)-dt F0, u_k*(1-dt
+// sigma_t)-dt F_k, the lattice source at the cell's lower-left corner
+// coordinate, and (stage 2) the average with the saved moments.
+#include "flux.cuh"
+
+namespace clb {
+
+namespace {
+
+constexpr int TX = 8, TY = 16;             // interior tile (x slow, y fast)
+constexpr int HX = TX + 4, HY = TY + 4;    // with the 2-cell halo
+constexpr int HC = HX * HY;                // 240 halo cells (15 m16 tiles)
+constexpr int IC = TX * TY;                // 128 interior cells
+constexpr double kSqrtPi = 1.7724538509055160273;
+
+__device__ __forceinline__ double minmod(double x, double y)
+{
+    // SIGN(1.0,x)*MAX(0.0, MIN(fabs(x), y*SIGN(1.0,x)))
+    double s = (x >= 0.0) ? 1.0 : -1.0;
+    double m = fabs(x);
+    double ys = y * s;
+    double mn = (m < ys) ? m : ys;
+    double mx = (0.0 > mn) ? 0.0 : mn;
+    return s * mx;
+}
+
+__device__ __forceinline__ double slopefit(double l, double c, double r, double th)
+{
+    return minmod(th * (r - c), minmod(0.5 * (r - l), th * (c - l)));
+}
+
+__global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant__ FluxArgs f)
+{
+    extern __shared__ __align__(16) double sm[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int bx = blockIdx.x / f.tilesY, by = blockIdx.x % f.tilesY;
+    const int i0 = 2 + bx * TX, j0 = 2 + by * TY;     // first interior cell of the tile
+    const int n = f.n, nb = f.nb, kq = f.kq, ldPf = f.ldPf;
+    const int ldAl = f.ldAl, ldA = f.ldA, ldF = f.ldF;
+    double *sAl = sm + f.offAl;     // [HC][ldAl]
+    double *sA = sm + f.offA;       // [kq][ldA] ansatz, q-major
+    double *sF = sm + f.offF;       // [kq][ldF] stencil flux, q-major
+    double *sP = sm + f.offP;       // [2][kq][ldPf]
+    double *sQ = sm + f.offQ;       // [2][4][kq] xi, eta, xi*w, eta*w
+
+    // alpha of the halo region (zero outside the grid)
+    for (int idx = tid; idx < HC * nb; idx += kThreads) {
+        int h = idx / nb, k = idx % nb;
+        int hi = h / HY, hj = h % HY;
+        int i = i0 - 2 + hi, j = j0 - 2 + hj;
+        double v = 0.0;
+        if (k < n && i < f.NX && j < f.NY)
+            v = f.alpha[((size_t)i * f.NY + j) * n + k];
+        sAl[h * ldAl + k] = v;
+    }
+
+    const int nchunks = f.nqp / kq;
+    auto load_chunk = [&](int c, int buf) {
+        const double *src = f.P + (size_t)c * kq * ldPf;
+        double *dst = sP + buf * kq * ldPf;
+        for (int i = tid; i < kq * ldPf / 2; i += kThreads)
+            cp_async16(dst + 2 * i, src + 2 * i);
+        double *q = sQ + buf * 4 * kq;
+        for (int i = tid; i < kq / 2; i += kThreads) {
+            cp_async16(q + 2 * i, f.xi + c * kq + 2 * i);
+            cp_async16(q + kq + 2 * i, f.eta + c * kq + 2 * i);
+            cp_async16(q + 2 * kq + 2 * i, f.cxw + c * kq + 2 * i);
+            cp_async16(q + 3 * kq + 2 * i, f.cyw + c * kq + 2 * i);
+        }
+        cp_async_commit();
+    };
+
+    // projection accumulators: warp owns interior rows warp*16.., all k tiles
+    double acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+    const int NTf = nb / 8;
+    const int ntiles1 = (HC / 16) * (kq / 8);
+
+    load_chunk(0, 0);
+    for (int c = 0; c < nchunks; c++) {
+        const int buf = c & 1;
+        if (c + 1 < nchunks) {
+            load_chunk(c + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double *Pb = sP + buf * kq * ldPf;
+        const double *Qb = sQ + buf * 4 * kq;
+        // 1. ansatz on the halo tile
+        for (int ti = warp; ti < ntiles1; ti += kWarps) {
+            int mt = ti % (HC / 16), nt = ti / (HC / 16);
+            double cs[4] = {0.0, 0.0, 0.0, 0.0};
+            const double *A0 = sAl + (mt * 16 + g) * ldAl;
+            const double *A1 = A0 + 8 * ldAl;
+            const double *B = Pb + (nt * 8 + g) * ldPf;
+            for (int k0 = 0; k0 < nb; k0 += 8)
+                dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
+                           B[k0 + t4 + 4]);
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                double kin = cs[h];
+                double v;
+                if (f.momentType == 0) {
+                    v = exp(kin);
+                } else {
+                    double dl = f.deltaPPn;
+                    if (kin > 0)
+                        v = 0.5 * kin + 0.5 * sqrt(kin * kin + 4 * dl);
+                    else
+                        v = -dl / (0.5 * kin - 0.5 * sqrt(kin * kin + 4 * dl));
+                }
+                int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
+                int q = nt * 8 + 2 * t4 + (h & 1);
+                sA[q * ldA + cell] = v;
+            }
+        }
+        __syncthreads();
+        // 2. limited upwind stencil, one q per warp-item (uniform branches)
+        for (int item = warp; item < kq * (IC / 32); item += kWarps) {
+            int q = item / (IC / 32), cg = item % (IC / 32);
+            int ic = cg * 32 + lane;
+            int ti = ic / TY, tj = ic % TY;
+            int h = (ti + 2) * HY + (tj + 2);
+            const double *a = sA + q * ldA;
+            const double xi = Qb[q], eta = Qb[kq + q];
+            const double cx = Qb[2 * kq + q], cy = Qb[3 * kq + q];
+            const double th = f.theta;
+            double flux1 = 0, flux2 = 0, flux3 = 0, flux4 = 0;
+            if (xi > 0) {
+                double k1 = a[h - 2 * HY], k2 = a[h - HY], k3 = a[h], k4 = a[h + HY];
+                flux1 = k3 + 0.5 * slopefit(k2, k3, k4, th) - k2 - 0.5 * slopefit(k1, k2, k3, th);
+                flux1 = flux1 * cx;
+            }
+            if (xi < 0) {
+                double k1 = a[h - HY], k2 = a[h], k3 = a[h + HY], k4 = a[h + 2 * HY];
+                flux2 = k3 - 0.5 * slopefit(k2, k3, k4, th) - k2 + 0.5 * slopefit(k1, k2, k3, th);
+                flux2 = flux2 * cx;
+            }
+            if (eta > 0) {
+                double k1 = a[h - 2], k2 = a[h - 1], k3 = a[h], k4 = a[h + 1];
+                flux3 = k3 + 0.5 * slopefit(k2, k3, k4, th) - k2 - 0.5 * slopefit(k1, k2, k3, th);
+                flux3 = flux3 * cy;
+            }
+            if (eta < 0) {
+                double k1 = a[h - 1], k2 = a[h], k3 = a[h + 1], k4 = a[h + 2];
+                flux4 = k3 - 0.5 * slopefit(k2, k3, k4, th) - k2 + 0.5 * slopefit(k1, k2, k3, th);
+                flux4 = flux4 * cy;
+            }
+            sF[q * ldF + ic] = (flux1 + flux2) / f.dx + (flux3 + flux4) / f.dy;
+        }
+        __syncthreads();
+        // 3. projection on the basis: flux[ic][k] += F[ic][q] p[q][k]
+        for (int k0 = 0; k0 < kq; k0 += 8) {
+            const double *A0 = sF + (k0 + t4) * ldF + warp * 16 + g;
+            double a0 = A0[0], a1 = A0[8], a2 = A0[4 * ldF], a3 = A0[4 * ldF + 8];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (j < NTf) {
+                    const double *B0 = Pb + (k0 + t4) * ldPf + j * 8 + g;
+                    dmma16x8x8(acc[j], a0, a1, a2, a3, B0[0], B0[4 * ldPf]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // epilogue: Euler + collision + source (+ Heun average)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (j >= NTf)
+            continue;
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            int ic = warp * 16 + g + ((h & 2) ? 8 : 0);
+            int k = j * 8 + 2 * t4 + (h & 1);
+            int i = i0 + ic / TY, jj = j0 + ic % TY;
+            if (k >= n || i >= f.NX - 2 || jj >= f.NY - 2)
+                continue;
+            size_t cell = (size_t)i * f.NY + jj;
+            double st = f.sigmaT[cell], ss = f.sigmaS[cell];
+            double u = f.moments[cell * n + k];
+            double F = acc[j][h];
+            double dt = f.dt;
+            double v;
+            if (k == 0)
+                v = u * (1.0 + dt * ss - dt * st) - dt * F;
+            else
+                v = u * (1.0 - dt * st) - dt * F;
+            if (k == 0 && f.initCond == 1) {
+                double x = f.initX + (i - 2) * f.dx;
+                double y = f.initY + (jj - 2) * f.dy;
+                if (fabs(x) < 0.5 && fabs(y) < 0.5)
+                    v = v + dt * 2.0 * kSqrtPi;
+            }
+            if (f.momentsOld != nullptr)
+                v = 0.5 * (v + f.momentsOld[cell * n + k]);
+            f.moments[cell * n + k] = v;
+        }
+    }
+}
+
+__global__ void ghost_periodic_kernel(double *m, int n, int NX, int NY)
+{
+    // momopt_boundaries.cpp:190-223: x strips over interior j, then y strips
+    // over interior i (corners untouched).
+    const int ny = NY - 4, nx = NX - 4;
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int totalX = 2 * ny * n, totalY = 2 * nx * n;
+    if (idx < totalX) {
+        int k = idx % n, r = idx / n;
+        int j = 2 + r % ny, i = r / ny;   // i in {0,1}
+        m[((size_t)(0 + i) * NY + j) * n + k] = m[((size_t)(NX - 4 + i) * NY + j) * n + k];
+        m[((size_t)(NX - 2 + i) * NY + j) * n + k] = m[((size_t)(2 + i) * NY + j) * n + k];
+    }
+}
+
+__global__ void ghost_periodic_y_kernel(double *m, int n, int NX, int NY)
+{
+    const int nx = NX - 4;
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int total = 2 * nx * n;
+    if (idx < total) {
+        int k = idx % n, r = idx / n;
+        int j = r % 2, i = 2 + r / 2;
+        m[((size_t)i * NY + 0 + j) * n + k] = m[((size_t)i * NY + NY - 4 + j) * n + k];
+        m[((size_t)i * NY + NY - 2 + j) * n + k] = m[((size_t)i * NY + 2 + j) * n + k];
+    }
+}
+
+}  // namespace
+
+int plan_flux(FluxArgs &f)
+{
+    f.kq = 32;
+    f.ldAl = f.nb + 4;
+    f.ldA = HC + 2;      // ldA % 8 == 2: conflict-free fragment stores
+    f.ldF = IC + 4;      // ldF % 16 == 4
+    int off = 0;
+    auto take = [&](int nd) {
+        int o = off;
+        off += (nd + 1) & ~1;
+        return o;
+    };
+    f.offAl = take(HC * f.ldAl);
+    f.offA = take(f.kq * f.ldA);
+    f.offF = take(f.kq * f.ldF);
+    f.offP = take(2 * f.kq * f.ldPf);
+    f.offQ = take(2 * 4 * f.kq);
+    f.smemBytes = off * 8;
+    f.tilesX = (f.NX - 4 + TX - 1) / TX;
+    f.tilesY = (f.NY - 4 + TY - 1) / TY;
+    return f.smemBytes <= 227 * 1024 - 64 ? 0 : -1;
+}
+
+cudaError_t prepare_flux(const FluxArgs &f)
+{
+    return cudaFuncSetAttribute(flux_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, f.smemBytes);
+}
+
+cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream)
+{
+    flux_kernel<<<f.tilesX * f.tilesY, kThreads, f.smemBytes, stream>>>(f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost_periodic(double *moments, int n, int NX, int NY, cudaStream_t stream)
+{
+    int totalX = 2 * (NY - 4) * n;
+    ghost_periodic_kernel<<<(totalX + 255) / 256, 256, 0, stream>>>(moments, n, NX, NY);
+    int totalY = 2 * (NX - 4) * n;
+    ghost_periodic_y_kernel<<<(totalY + 255) / 256, 256, 0, stream>>>(moments, n, NX, NY);
+    return cudaGetLastError();
+}
+
+}  // namespace clb

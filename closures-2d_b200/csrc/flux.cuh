@@ -1,0 +1,35 @@
+// flux.cuh -- host interface of the kinetic-flux + RK-stage kernel (K2+K3)
+// and the periodic ghost fill (K4).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace clb {
+
+struct FluxArgs {
+    const double *alpha;        // [C][n]
+    double *moments;            // [C][n], updated in place on interior cells
+    const double *momentsOld;   // Heun average partner (stage 2) or null (stage 1)
+    const double *sigmaT, *sigmaS;  // [C]
+    const double *P;            // [nqp][ldPf] basis, columns >= n zero
+    const double *xi, *eta;     // [nqp], zero on padded rows
+    const double *cxw, *cyw;    // xi*w, eta*w per q
+    int n, nb, ldPf, nqp;
+    int NX, NY;                 // grid with ghosts
+    int momentType, initCond;
+    double theta, deltaPPn;
+    double dt, dx, dy, initX, initY;
+    // layout (doubles), filled by plan_flux()
+    int kq, ldAl, ldA, ldF;
+    int offAl, offA, offF, offP, offQ;
+    int smemBytes;
+    int tilesX, tilesY;
+};
+
+int plan_flux(FluxArgs &f);
+cudaError_t prepare_flux(const FluxArgs &f);
+cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream);
+// duplicateBoundaries (momopt_boundaries.cpp:190-223) on device moments.
+cudaError_t launch_ghost_periodic(double *moments, int n, int NX, int NY, cudaStream_t stream);
+
+}  // namespace clb

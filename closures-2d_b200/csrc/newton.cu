@@ -1,0 +1,855 @@
+// newton.cu -- persistent dual-Newton kernel for the Mn / PPn entropy closure.
+//
+// One launch solves, for every vector u of every problem, the dual problem of
+// opt() (src/momopt/opt/opt.cpp:82-343): minimise <eta*(alpha.m)> - alpha.u by
+// Newton's method with the Armijo backtracking line search of
+// linesearch.cpp:21-99 and the isotropic-restart regularisation ladder
+// r in {0, 1e-3, 1e-2, 1e-1, 0.5} (opt.h:39-40, opt.cpp:244-274).
+//
+// B200 mapping.  A CTA owns T "slots" (cells in flight).  Each round every
+// slot needs one evaluation of f, g and H at its current alpha; the rounds are
+// batched contractions over the quadrature on the FP64 tensor cores (DMMA
+// m16n8k8):
+//   S[T x kq]  = alpha[T x nb] . P[kq x nb]^T            (alpha.m per q)
+//   E          = w * exp(S)          (Mn)   or the PPn weights
+//   G[T x K]  += E[T x kq] . Phess[kq x K]               (Hessian columns)
+// with the basis streamed through shared memory in q-chunks by cp.async.
+// Then one warp per slot finishes the Newton logic in FP64: H from G (the
+// Gaunt contraction of fobj.cpp:130-144 or the packed products), Cholesky,
+// Hager/Higham 1-norm condition estimate (the quantity dpocon returns),
+// direction, stopping test, line-search bookkeeping and the ladder.
+// Converged slots write u, alpha back and are refilled from a global work
+// counter, so vectors needing 1 or 40 iterations share the launch.
+//
+// Every line-search trial evaluation also carries H: when the trial is
+// accepted (the usual case) it is reused as the next Newton iteration's
+// evaluation, which the reference recomputes at the same alpha.
+#include "newton.cuh"
+
+#include <cfloat>
+#include <cmath>
+
+namespace clb {
+
+namespace {
+
+enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
+enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_N };
+enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_N };
+
+constexpr double kSqrtPi = 1.7724538509055160273;
+constexpr double kPi = 3.14159265358979323846;
+
+struct Ctx {
+    double *sm;
+    int lane, warp, g, t4;
+};
+
+__device__ __forceinline__ void record_error(int *err, int code, int idx)
+{
+    if (atomicCAS(&err[0], 0, code) == 0)
+        err[1] = idx;
+}
+
+// Cholesky of the n x n symmetric matrix in Hs (row stride ldh) in place,
+// lower triangle; returns LAPACK-style info (0 ok, j+1 at the first
+// non-positive or NaN pivot).  Right-looking; lanes share each trailing
+// update through the column-ordered pair list.
+__device__ int chol_warp(double *Hs, int n, int ldh, const unsigned short *pairsCol, int lane)
+{
+    // pairsCol lists (i,k) with k <= i ordered by column k; start of column k
+    // is k*n - k(k-1)/2.
+    for (int j = 0; j < n; j++) {
+        double ajj = Hs[j * ldh + j];
+        if (!(ajj > 0.0))
+            return j + 1;
+        double ljj = sqrt(ajj);
+        double r = 1.0 / ljj;
+        __syncwarp();
+        if (lane > j && lane < n)
+            Hs[lane * ldh + j] *= r;
+        if (lane == j)
+            Hs[j * ldh + j] = ljj;
+        __syncwarp();
+        int start = (j + 1) * n - ((j + 1) * j) / 2;   // first pair of column j+1
+        int total = n * (n + 1) / 2;
+        for (int p = start + lane; p < total; p += 32) {
+            unsigned short pr = pairsCol[p];
+            int i = pr >> 8, k = pr & 255;
+            Hs[i * ldh + k] -= Hs[i * ldh + j] * Hs[k * ldh + j];
+        }
+        __syncwarp();
+    }
+    return 0;
+}
+
+// In-place inverse of the lower triangular factor (rows processed in order,
+// lanes over columns).
+__device__ void invert_lower_warp(double *Hs, int n, int ldh, int lane)
+{
+    for (int i = 0; i < n; i++) {
+        double acc0 = 0.0, acc1 = 0.0;
+        if (lane < i) {
+            int k = lane;
+            for (; k + 1 < i; k += 2) {
+                acc0 = fma(Hs[i * ldh + k], Hs[k * ldh + lane], acc0);
+                acc1 = fma(Hs[i * ldh + k + 1], Hs[(k + 1) * ldh + lane], acc1);
+            }
+            if (k < i)
+                acc0 = fma(Hs[i * ldh + k], Hs[k * ldh + lane], acc0);
+        }
+        double dinv = 1.0 / Hs[i * ldh + i];
+        __syncwarp();
+        if (lane < i)
+            Hs[i * ldh + lane] = -dinv * (acc0 + acc1);
+        if (lane == i)
+            Hs[i * ldh + i] = dinv;
+        __syncwarp();
+    }
+}
+
+// z = (L L^T)^-1 x with Linv in Hs; x, z held one element per lane.
+__device__ double apply_inv(const double *Hs, int n, int ldh, double *vec, double x, int lane)
+{
+    __syncwarp();
+    vec[lane] = x;
+    __syncwarp();
+    double y = 0.0;
+    if (lane < n)
+        for (int k = 0; k <= lane; k++)
+            y = fma(Hs[lane * ldh + k], vec[k], y);
+    __syncwarp();
+    vec[lane] = y;
+    __syncwarp();
+    double z = 0.0;
+    if (lane < n)
+        for (int k = lane; k < n; k++)
+            z = fma(Hs[k * ldh + lane], vec[k], z);
+    return z;
+}
+
+__device__ __forceinline__ double sgn1(double x) { return x >= 0.0 ? 1.0 : -1.0; }
+
+// Estimate of ||A^-1||_1 for A = L L^T (Higham 1988, Alg. 4.1, the estimator
+// behind LAPACK dlacn2/dpocon); returns rcond = (1/est)/anorm.
+__device__ double rcond_warp(const double *Hs, int n, int ldh, double *vec, double anorm, int lane)
+{
+    const bool act = lane < n;
+    if (anorm == 0.0)
+        return 0.0;
+    double x = act ? 1.0 / n : 0.0;
+    x = apply_inv(Hs, n, ldh, vec, x, lane);
+    double est;
+    if (n == 1) {
+        est = fabs(__shfl_sync(0xffffffffu, x, 0));
+    } else {
+        est = warp_sum(act ? fabs(x) : 0.0);
+        double isgn = act ? sgn1(x) : 0.0;
+        x = apply_inv(Hs, n, ldh, vec, isgn, lane);
+        int j = warp_argmax_first(act ? fabs(x) : -1.0, lane);
+        int iter = 2;
+        for (;;) {
+            x = (lane == j) ? 1.0 : 0.0;
+            x = apply_inv(Hs, n, ldh, vec, x, lane);
+            double estold = est;
+            est = warp_sum(act ? fabs(x) : 0.0);
+            bool same = __all_sync(0xffffffffu, !act || sgn1(x) == isgn);
+            if (same || est <= estold)
+                break;
+            isgn = act ? sgn1(x) : 0.0;
+            x = apply_inv(Hs, n, ldh, vec, isgn, lane);
+            int jlast = j;
+            j = warp_argmax_first(act ? fabs(x) : -1.0, lane);
+            double xjlast = __shfl_sync(0xffffffffu, x, jlast);
+            double xj = __shfl_sync(0xffffffffu, x, j);
+            if (xjlast != fabs(xj) && iter < 5) {
+                iter++;
+                continue;
+            }
+            break;
+        }
+        double alt = act ? ((lane & 1) ? -1.0 : 1.0) * (1.0 + (double)lane / (double)(n - 1)) : 0.0;
+        alt = apply_inv(Hs, n, ldh, vec, alt, lane);
+        double temp = 2.0 * (warp_sum(act ? fabs(alt) : 0.0) / (3.0 * n));
+        if (temp > est)
+            est = temp;
+    }
+    if (est != 0.0)
+        return (1.0 / est) / anorm;
+    return 0.0;
+}
+
+struct Layout {
+    double *alpha, *aold, *d, *u, *scal, *fpart, *P, *E, *Eg, *G, *H, *vec;
+    int *ints;
+    unsigned long long *stat;
+};
+
+__device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
+{
+    Layout L;
+    L.alpha = sm + a.offAlpha;
+    L.aold = sm + a.offAold;
+    L.d = sm + a.offD;
+    L.u = sm + a.offU;
+    L.scal = sm + a.offScal;
+    L.ints = (int *)(sm + a.offInt);
+    L.fpart = sm + a.offFpart;
+    L.stat = (unsigned long long *)(sm + a.offStat);
+    L.P = sm + a.offP;
+    L.E = sm + a.offE;
+    L.Eg = sm + a.offEg;
+    L.G = sm + a.offG;
+    L.H = sm + a.offH;
+    L.vec = sm + a.offVec;
+    return L;
+}
+
+// Writes the finished slot's results (scaled back) and updates CTA stats.
+__device__ void finish_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s,
+                            double ui, double ai, int status, int lane)
+{
+    int cell = L.ints[s * SI_N + SI_CELL];
+    int n = pb.n;
+    if (lane < n) {
+        pb.u[(size_t)cell * n + lane] = ui;
+        pb.alpha[(size_t)cell * n + lane] = ai;
+    }
+    if (lane == 0) {
+        int total = L.ints[s * SI_N + SI_TOTAL];
+        int reg = L.ints[s * SI_N + SI_REG];
+        if (pb.iters)
+            pb.iters[cell] = total;
+        if (pb.regs)
+            pb.regs[cell] = kRegularizations[reg];
+        if (pb.status)
+            pb.status[cell] = status;
+        if (status == 0) {
+            atomicAdd(&L.stat[reg], 1ull);
+            atomicAdd(&L.stat[kNumReg], (unsigned long long)total);
+            atomicAdd(&L.stat[kNumReg + 1], 1ull);
+            atomicMax((int *)&L.stat[kNumReg + 2], total);
+        } else {
+            record_error(a.err, status, cell);
+        }
+        L.ints[s * SI_N + SI_STATE] = S_IDLE;
+    }
+}
+
+// Loads and scales a newly assigned vector (opt.cpp:82-148 entry half).
+__device__ void init_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
+                          int ldv)
+{
+    const int n = pb.n;
+    const int cell = L.ints[s * SI_N + SI_CELL];
+    double ui = 0.0, ai = 0.0;
+    if (lane < n) {
+        ui = pb.u[(size_t)cell * n + lane];
+        ai = pb.alpha[(size_t)cell * n + lane];
+    }
+    if (a.momentsOld != nullptr && lane < n) {
+        int i = cell / a.NY, j = cell % a.NY;
+        if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
+            a.momentsOld[(size_t)cell * n + lane] = ui;
+    }
+    const double u0 = __shfl_sync(0xffffffffu, ui, 0);
+    if (!(u0 > 0.0)) {
+        // opt.cpp:97-101 aborts; leave the vector untouched and report.
+        if (lane == 0) {
+            L.ints[s * SI_N + SI_TOTAL] = 0;
+            L.ints[s * SI_N + SI_REG] = 0;
+        }
+        __syncwarp();
+        finish_slot(a, pb, L, s, ui, ai, -3, lane);
+        return;
+    }
+    double *sc = L.scal + s * SC_N;
+    double delta = a.deltaPPn;
+    if (a.momentType == 0) {
+        double ascale = log(u0) * 2.0 * kSqrtPi;
+        if (lane == 0)
+            ai = ai - ascale;
+        ui = ui / u0;
+        if (lane == 0)
+            sc[SC_ASCALE] = ascale;
+    } else {
+        ai = ai / u0;
+        ui = ui / u0;
+        delta = delta / (u0 * u0);
+    }
+    if (lane < ldv) {
+        L.u[s * ldv + lane] = (lane < n) ? ui : 0.0;
+        L.alpha[s * ldv + lane] = (lane < n) ? ai : 0.0;
+    }
+    double rtol = sqrt(warp_sum(ui * ui)) * a.tolRel;
+    if (lane == 0) {
+        sc[SC_T] = 1.0;
+        sc[SC_RTOL] = rtol;
+        sc[SC_U0] = u0;
+        sc[SC_DELTA] = delta;
+        int *si = L.ints + s * SI_N;
+        si[SI_ITER] = 0;
+        si[SI_TOTAL] = 0;
+        si[SI_REG] = 0;
+        si[SI_MAXITER] = a.maxIter;
+        si[SI_STATE] = S_NEWTON;
+    }
+}
+
+// Isotropic restart with the next regularisation (opt.cpp:244-274).
+__device__ void regularize(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
+                           int ldv, double ui, double ai)
+{
+    const int n = pb.n;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    int reg = si[SI_REG];
+    if (reg >= kNumReg - 1) {
+        // opt.cpp:256-261 aborts; report and return the unscaled state.
+        double u0 = sc[SC_U0];
+        if (a.momentType == 0) {
+            ui *= u0;
+            if (lane == 0)
+                ai += sc[SC_ASCALE];
+        } else {
+            ui *= u0;
+            ai *= u0;
+        }
+        __syncwarp();
+        finish_slot(a, pb, L, s, ui, ai, -4, lane);
+        return;
+    }
+    reg++;
+    const double r = kRegularizations[reg];
+    const int cell = si[SI_CELL];
+    const double u0 = sc[SC_U0];
+    double unew = 0.0;
+    if (lane < n) {
+        double uorig = pb.u[(size_t)cell * n + lane] / u0;   // scaled original (unchanged in memory)
+        unew = (lane == 0) ? 1.0 : uorig * (1.0 - r);
+        L.u[s * ldv + lane] = unew;
+        double a0 = (a.momentType == 0) ? 2.0 * kSqrtPi * log(0.5 / kSqrtPi)
+                                        : 1.0 - 4.0 * sc[SC_DELTA] * kPi;
+        L.alpha[s * ldv + lane] = (lane == 0) ? a0 : 0.0;
+    }
+    double rtol = sqrt(warp_sum(unew * unew)) * a.tolRel;
+    __syncwarp();
+    if (lane == 0) {
+        si[SI_REG] = reg;
+        si[SI_ITER] = 0;
+        sc[SC_T] = 1.0;
+        sc[SC_RTOL] = rtol;
+        if (reg == kNumReg - 1)
+            si[SI_MAXITER] = 10 * si[SI_MAXITER];
+        si[SI_STATE] = S_NEWTON;
+    }
+}
+
+__device__ double modcfl(double di, int n, int lane, int momentType)
+{
+    double da1 = warp_sum(lane < n ? fabs(di) : 0.0);
+    int pnOrder = (int)floor(sqrt((double)n)) + 1;
+    double minf = sqrt((2 * pnOrder + 1) / (2 * kPi));
+    return momentType == 0 ? exp(2.0 * da1 * minf) : 1.0 + 2.0 * da1 * minf;
+}
+
+// Newton logic for one slot after its evaluation (warp-wide).
+__device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
+                           int warp)
+{
+    const int n = pb.n;
+    const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
+    const bool act = lane < n;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    double *Hs = L.H + warp * (kMaxN * ldh);
+    double *vec = L.vec + warp * 64;
+    const double *Gs = L.G + s * ldG;
+    const int npairs = n * (n + 1) / 2;
+
+    // H from the contraction results (fobj.cpp:129-155)
+    for (int pi = lane; pi < npairs; pi += 32) {
+        unsigned short pr = pb.pairs[pi];
+        int i = pr >> 8, j = pr & 255;
+        double v;
+        if (a.useGaunt) {
+            int row = j * n + i;
+            v = 0.0;
+            for (int e = __ldg(&pb.hoff[row]); e < __ldg(&pb.hoff[row + 1]); e++)
+                v += __ldg(&pb.hval[e]) * Gs[__ldg(&pb.hidx[e])];
+        } else {
+            v = Gs[pi];
+        }
+        Hs[i * ldh + j] = v;
+        Hs[j * ldh + i] = v;
+    }
+    __syncwarp();
+
+    const double ui = act ? L.u[s * ldv + lane] : 0.0;
+    const double ai = act ? L.alpha[s * ldv + lane] : 0.0;
+    double gi;
+    if (a.momentType == 0)
+        gi = act ? Hs[lane] / pb.p0 - ui : 0.0;     // fobj.cpp:303-306
+    else
+        gi = act ? Gs[pb.K2p + lane] - ui : 0.0;    // fobj.cpp:427-431 / :445-452
+    const double au = warp_sum(ai * ui);
+    double fpart = 0.0;
+    for (int k = 0; k < a.ntq; k++)
+        fpart += L.fpart[s * a.ntq + k];
+    const double fsum = fpart - au;                  // no-Hessian f (linesearch's fobj)
+    const double fH = (a.momentType == 0) ? Hs[0] / (pb.p0 * pb.p0) - au : fsum;
+
+    int state = si[SI_STATE];
+    if (state == S_TRIAL) {
+        double t = sc[SC_T];
+        if (!(fsum <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD])) {
+            t = 0.5 * t;
+            double ao = act ? L.aold[s * ldv + lane] : 0.0;
+            if (t * sc[SC_MAXF] > DBL_EPSILON / 2) {
+                if (act)
+                    L.alpha[s * ldv + lane] = ao + t * L.d[s * ldv + lane];
+                __syncwarp();
+                if (lane == 0)
+                    sc[SC_T] = t;
+                return;
+            }
+            // backtracked all the way (linesearch.cpp:84-98): alpha restored,
+            // the next iteration regularises because t == 0.
+            __syncwarp();
+            if (lane == 0) {
+                si[SI_ITER] += 1;
+                si[SI_TOTAL] += 1;
+            }
+            __syncwarp();
+            regularize(a, pb, L, s, lane, ldv, ui, ao);
+            return;
+        }
+        // accepted: this evaluation is the next Newton iteration's (opt.cpp:262-274)
+    }
+
+    // one Newton iteration (opt.cpp:258-368)
+    const int iter = si[SI_ITER] + 1;
+    __syncwarp();
+    if (lane == 0) {
+        si[SI_ITER] = iter;
+        si[SI_TOTAL] += 1;
+    }
+    double rowsum = 0.0;
+    if (act)
+        for (int j = 0; j < n; j++)
+            rowsum += fabs(Hs[lane * ldh + j]);
+    const double anorm = warp_max(rowsum);          // utils_norm1
+    __syncwarp();
+    int info = chol_warp(Hs, n, ldh, pb.pairs + npairs, lane);
+    double condest = 0.0;
+    if (info == 0) {
+        invert_lower_warp(Hs, n, ldh, lane);
+        double rc = rcond_warp(Hs, n, ldh, vec, anorm, lane);
+        condest = 1.0 / rc;
+    }
+    if (iter >= si[SI_MAXITER] || info != 0 || sc[SC_T] == 0.0 || condest > a.condHMax) {
+        __syncwarp();
+        regularize(a, pb, L, s, lane, ldv, ui, ai);
+        return;
+    }
+    const double di = -apply_inv(Hs, n, ldh, vec, gi, lane);
+    const double err = sqrt(warp_sum(gi * gi));
+    bool gammaOk = true;
+    if (a.tolGamma > 0.0)
+        gammaOk = modcfl(di, n, lane, a.momentType) <= a.tolGamma;
+    if (err <= sc[SC_RTOL] && gammaOk) {
+        // converged (opt.cpp:293-306), then opt()'s rescaling (:107-109, :133-138)
+        double uo = ui, ao = ai;
+        const double u0 = sc[SC_U0];
+        if (a.momentType == 0) {
+            double u0w = __shfl_sync(0xffffffffu, ui + gi, 0);
+            uo = (ui + gi) / u0w;
+            if (lane == 0)
+                ao = ai - log(u0w) * 2.0 * kSqrtPi;
+            uo = uo * u0;
+            if (lane == 0)
+                ao = ao + sc[SC_ASCALE];
+        } else {
+            ao = ai * u0;
+            uo = ui * u0;
+        }
+        __syncwarp();
+        finish_slot(a, pb, L, s, uo, ao, 0, lane);
+        return;
+    }
+    // line search set-up (linesearch.cpp:21-52)
+    const double gd = warp_sum(gi * di);
+    const double maxf = warp_max(act ? fabs(di) / (fabs(ai) + 1e-100) : 0.0);
+    if (act) {
+        L.aold[s * ldv + lane] = ai;
+        L.d[s * ldv + lane] = di;
+    }
+    if (1.0 * maxf > DBL_EPSILON / 2) {
+        if (act)
+            L.alpha[s * ldv + lane] = ai + 1.0 * di;
+        __syncwarp();
+        if (lane == 0) {
+            sc[SC_T] = 1.0;
+            sc[SC_FREF] = fH;
+            sc[SC_GD] = gd;
+            sc[SC_MAXF] = maxf;
+            si[SI_STATE] = S_TRIAL;
+        }
+        return;
+    }
+    // zero-length search: linesearch returns 0 without evaluating
+    __syncwarp();
+    if (lane == 0) {
+        sc[SC_T] = 0.0;
+        si[SI_ITER] += 1;
+        si[SI_TOTAL] += 1;
+    }
+    __syncwarp();
+    regularize(a, pb, L, s, lane, ldv, ui, ai);
+}
+
+template <int TPW>
+__global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
+{
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int ctl[4];   // [0] problem, [1] done, [2] exhausted
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int T = a.T, MT = a.T / 16, kq = a.kq, ldv = a.ldv, ldE = a.ldE, ldG = a.ldG;
+    Layout L = make_layout(sm, a);
+
+    for (int i = tid; i < 4 * T * ldv; i += kThreads)
+        L.alpha[i] = 0.0;   // alpha, aold, d, u are contiguous
+    for (int i = tid; i < T * SI_N; i += kThreads)
+        L.ints[i] = (i % SI_N == SI_STATE) ? S_IDLE : 0;
+    for (int i = tid; i < kNumReg + 3; i += kThreads)
+        L.stat[i] = 0ull;
+    if (tid == 0) {
+        ctl[0] = 0;
+        ctl[1] = 0;
+        ctl[2] = 0;
+    }
+    __syncthreads();
+
+    for (;;) {
+        // ---- refill idle slots from the work counter of the current problem
+        if (tid == 0) {
+            int p = ctl[0];
+            int nIdle = 0, nActive = 0;
+            for (int s = 0; s < T; s++) {
+                if (L.ints[s * SI_N + SI_STATE] == S_IDLE)
+                    nIdle++;
+                else
+                    nActive++;
+            }
+            bool exhausted = ctl[2] != 0;
+            while (nIdle > 0) {
+                if (exhausted) {
+                    if (nActive == 0 && p + 1 < a.nprob) {
+                        p++;
+                        exhausted = false;
+                        continue;
+                    }
+                    break;
+                }
+                const NewtonProblem &pb = a.prob[p];
+                unsigned base = atomicAdd(pb.queue, (unsigned)nIdle);
+                if (base >= (unsigned)pb.count) {
+                    exhausted = true;
+                    continue;
+                }
+                int take = min(nIdle, pb.count - (int)base);
+                int c = 0;
+                for (int s = 0; s < T && c < take; s++) {
+                    if (L.ints[s * SI_N + SI_STATE] == S_IDLE) {
+                        L.ints[s * SI_N + SI_CELL] = (int)base + c;
+                        L.ints[s * SI_N + SI_STATE] = S_NEW;
+                        c++;
+                    }
+                }
+                nIdle -= take;
+                nActive += take;
+                if (nIdle > 0)
+                    exhausted = true;
+            }
+            ctl[0] = p;
+            ctl[2] = exhausted ? 1 : 0;
+            ctl[1] = (nActive == 0) ? 1 : 0;
+        }
+        __syncthreads();
+        if (ctl[1])
+            break;
+        const NewtonProblem &pb = a.prob[ctl[0]];
+        for (int s = warp; s < T; s += kWarps)
+            if (L.ints[s * SI_N + SI_STATE] == S_NEW)
+                init_slot(a, pb, L, s, lane, ldv);
+        __syncthreads();
+
+        // ---- phase A: evaluation contractions over the quadrature
+        const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
+        const int NTH = K2p / 8;
+        const int NT2 = NTH + (a.momentType == 1 ? nb / 8 : 0);
+        const int ntiles2 = MT * NT2;
+        const int nchunks = pb.nqp / kq;
+        const int chunkDoubles = kq * ldP;
+        const int mt1 = warp % MT, ntq = warp / MT;
+        double acc[TPW][4];
+#pragma unroll
+        for (int j = 0; j < TPW; j++)
+            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+        double facc0 = 0.0, facc1 = 0.0;
+        const int r0 = mt1 * 16 + g, r1 = r0 + 8;
+        const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
+
+        auto load_chunk = [&](int c, int buf) {
+            const double *src = pb.P + (size_t)c * chunkDoubles;
+            double *dst = L.P + buf * chunkDoubles;
+            for (int i = tid; i < chunkDoubles / 2; i += kThreads)
+                cp_async16(dst + 2 * i, src + 2 * i);
+            cp_async_commit();
+        };
+        if (a.doubleBuffer)
+            load_chunk(0, 0);
+        for (int c = 0; c < nchunks; c++) {
+            int buf = a.doubleBuffer ? (c & 1) : 0;
+            if (a.doubleBuffer) {
+                if (c + 1 < nchunks) {
+                    load_chunk(c + 1, buf ^ 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+            } else {
+                load_chunk(c, 0);
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            const double *Pb = L.P + buf * chunkDoubles;
+            // GEMM1: S = alpha . P^T for this warp's 16 x 8 tile
+            {
+                double cs[4] = {0.0, 0.0, 0.0, 0.0};
+                const double *A0 = L.alpha + r0 * ldv, *A1 = L.alpha + r1 * ldv;
+                const double *B = Pb + (ntq * 8 + g) * ldP;
+                for (int k0 = 0; k0 < nb; k0 += 8)
+                    dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4],
+                               B[k0 + t4], B[k0 + t4 + 4]);
+                const int ql = ntq * 8 + 2 * t4;
+                const int qg = c * kq + ql;
+                const double w0 = __ldg(&pb.w[qg]), w1 = __ldg(&pb.w[qg + 1]);
+                if (a.momentType == 0) {
+                    double e0 = w0 * exp(cs[0]), e1 = w1 * exp(cs[1]);
+                    double e2 = w0 * exp(cs[2]), e3 = w1 * exp(cs[3]);
+                    L.E[r0 * ldE + ql] = e0;
+                    L.E[r0 * ldE + ql + 1] = e1;
+                    L.E[r1 * ldE + ql] = e2;
+                    L.E[r1 * ldE + ql + 1] = e3;
+                    facc0 += e0 + e1;
+                    facc1 += e2 + e3;
+                } else {
+                    // fobj.cpp:408-434 and :196-210 (PPn)
+                    double wv[2] = {w0, w1};
+#pragma unroll
+                    for (int h = 0; h < 4; h++) {
+                        double dl = (h < 2) ? dl0 : dl1;
+                        double ww = wv[h & 1];
+                        double k = 0.5 * cs[h];
+                        double s2 = sqrt(k * k + dl);
+                        double G = k + s2;
+                        if (k < 0)
+                            G = -dl / (k - sqrt(k * k + dl));
+                        double eh = 0.5 * ww * (G / s2);
+                        double eg = ww * G;
+                        double ft = ww * (k * G - 0.5 * dl + dl * log(G));
+                        int row = (h < 2) ? r0 : r1;
+                        L.E[row * ldE + ql + (h & 1)] = eh;
+                        L.Eg[row * ldE + ql + (h & 1)] = eg;
+                        if (h < 2)
+                            facc0 += ft;
+                        else
+                            facc1 += ft;
+                    }
+                }
+            }
+            __syncthreads();
+            // GEMM2: G += E . Phess (and Eg . P for the PPn gradient)
+            for (int k0 = 0; k0 < kq; k0 += 8) {
+#pragma unroll
+                for (int j = 0; j < TPW; j++) {
+                    int ti = warp + kWarps * j;
+                    if (ti < ntiles2) {
+                        int mt2 = ti % MT, nt2 = ti / MT;
+                        const double *Ab = (nt2 < NTH) ? L.E : L.Eg;
+                        int col = (nt2 < NTH) ? nb + nt2 * 8 : (nt2 - NTH) * 8;
+                        const double *A0 = Ab + (mt2 * 16 + g) * ldE + k0 + t4;
+                        const double *A1 = A0 + 8 * ldE;
+                        const double *B0 = Pb + (k0 + t4) * ldP + col + g;
+                        dmma16x8x8(acc[j], A0[0], A1[0], A0[4], A1[4], B0[0], B0[4 * ldP]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // dump accumulators and f partial sums
+#pragma unroll
+        for (int j = 0; j < TPW; j++) {
+            int ti = warp + kWarps * j;
+            if (ti < ntiles2) {
+                int mt2 = ti % MT, nt2 = ti / MT;
+                double *G0 = L.G + (mt2 * 16 + g) * ldG + nt2 * 8 + 2 * t4;
+                G0[0] = acc[j][0];
+                G0[1] = acc[j][1];
+                G0[8 * ldG] = acc[j][2];
+                G0[8 * ldG + 1] = acc[j][3];
+            }
+        }
+        facc0 += __shfl_xor_sync(0xffffffffu, facc0, 1);
+        facc0 += __shfl_xor_sync(0xffffffffu, facc0, 2);
+        facc1 += __shfl_xor_sync(0xffffffffu, facc1, 1);
+        facc1 += __shfl_xor_sync(0xffffffffu, facc1, 2);
+        if (t4 == 0) {
+            L.fpart[r0 * a.ntq + ntq] = facc0;
+            L.fpart[r1 * a.ntq + ntq] = facc1;
+        }
+        __syncthreads();
+
+        // ---- phase B: per-slot Newton logic, one warp per slot
+        for (int s = warp; s < T; s += kWarps) {
+            int st = L.ints[s * SI_N + SI_STATE];
+            if (st == S_NEWTON || st == S_TRIAL)
+                slot_logic(a, pb, L, s, lane, warp);
+        }
+        __syncthreads();
+    }
+
+    // flush CTA statistics
+    if (tid < kNumReg + 2) {
+        unsigned long long v = L.stat[tid];
+        if (v)
+            atomicAdd(&a.stats->hist[0] + tid, v);   // hist[0..4], totalIter, numSolves contiguous
+    } else if (tid == kNumReg + 2) {
+        atomicMax(&a.stats->maxIter, *(int *)&L.stat[kNumReg + 2]);
+    }
+}
+
+}  // namespace
+
+int plan_newton(NewtonArgs &a)
+{
+    int nbMax = 8, ldPMax = 0, K2tot = 0, nMax = 1;
+    for (int p = 0; p < a.nprob; p++) {
+        const NewtonProblem &pb = a.prob[p];
+        nbMax = pb.nb > nbMax ? pb.nb : nbMax;
+        ldPMax = pb.ldP > ldPMax ? pb.ldP : ldPMax;
+        int kt = pb.K2p + (a.momentType == 1 ? pb.nb : 0);
+        K2tot = kt > K2tot ? kt : K2tot;
+        nMax = pb.n > nMax ? pb.n : nMax;
+    }
+    a.T = 32;
+    a.kq = 32;
+    a.ntq = a.kq / 8;
+    a.ldv = nbMax + 4;
+    a.ldE = a.kq + 4;
+    a.ldG = K2tot + 4;
+    a.ldh = (nMax % 2 == 0) ? nMax + 1 : nMax;
+    const int T = a.T;
+    int off = 0;
+    auto take = [&](int ndoubles) {
+        int o = off;
+        off += (ndoubles + 1) & ~1;   // keep 16-byte alignment
+        return o;
+    };
+    a.offAlpha = take(T * a.ldv);
+    a.offAold = take(T * a.ldv);
+    a.offD = take(T * a.ldv);
+    a.offU = take(T * a.ldv);
+    a.offScal = take(T * SC_N);
+    a.offInt = take((T * SI_N + 1) / 2);
+    a.offFpart = take(T * a.ntq);
+    a.offStat = take(kNumReg + 3);
+    const int unionBase = off;
+    const int ntiles2 = (T / 16) * (K2tot / 8);
+    a.tpw = (ntiles2 + kWarps - 1) / kWarps;
+    // phase-B region
+    int offG = unionBase;
+    int offH = offG + ((T * a.ldG + 1) & ~1);
+    int offVec = offH + ((kWarps * kMaxN * a.ldh + 1) & ~1);
+    int endB = offVec + kWarps * 64;
+    // phase-A region
+    const int maxDoubles = (232448 - 1024) / 8;   // opt-in limit minus static shared
+    for (int db = 1; db >= 0; db--) {
+        int offP = unionBase;
+        int offE = offP + (db ? 2 : 1) * a.kq * ldPMax;
+        int offEg = offE + T * a.ldE;
+        int endA = offEg + T * a.ldE;
+        int end = endA > endB ? endA : endB;
+        if (end <= maxDoubles) {
+            a.doubleBuffer = db;
+            a.offP = offP;
+            a.offE = offE;
+            a.offEg = offEg;
+            a.offG = offG;
+            a.offH = offH;
+            a.offVec = offVec;
+            a.smemBytes = end * 8;
+            return 0;
+        }
+    }
+    return -1;
+}
+
+template <int TPW>
+static cudaError_t launch_t(const NewtonArgs &a, int grid, cudaStream_t stream, bool prepare)
+{
+    if (prepare)
+        return cudaFuncSetAttribute(newton_kernel<TPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    a.smemBytes);
+    newton_kernel<TPW><<<grid, kThreads, a.smemBytes, stream>>>(a);
+    return cudaGetLastError();
+}
+
+static cudaError_t dispatch(const NewtonArgs &a, int grid, cudaStream_t stream, bool prepare)
+{
+    if (a.tpw <= 1)
+        return launch_t<1>(a, grid, stream, prepare);
+    if (a.tpw <= 2)
+        return launch_t<2>(a, grid, stream, prepare);
+    if (a.tpw <= 4)
+        return launch_t<4>(a, grid, stream, prepare);
+    if (a.tpw <= 8)
+        return launch_t<8>(a, grid, stream, prepare);
+    if (a.tpw <= 16)
+        return launch_t<16>(a, grid, stream, prepare);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t prepare_newton(const NewtonArgs &a) { return dispatch(a, 0, nullptr, true); }
+
+cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream)
+{
+    return dispatch(a, grid, stream, false);
+}
+
+template <int TPW>
+static int occupancy_t(const NewtonArgs &a)
+{
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, newton_kernel<TPW>, kThreads, a.smemBytes) !=
+        cudaSuccess)
+        return 1;
+    return blocks < 1 ? 1 : blocks;
+}
+
+int newton_ctas_per_sm(const NewtonArgs &a)
+{
+    if (a.tpw <= 1)
+        return occupancy_t<1>(a);
+    if (a.tpw <= 2)
+        return occupancy_t<2>(a);
+    if (a.tpw <= 4)
+        return occupancy_t<4>(a);
+    if (a.tpw <= 8)
+        return occupancy_t<8>(a);
+    return occupancy_t<16>(a);
+}
+
+}  // namespace clb

@@ -1,0 +1,59 @@
+// newton.cuh -- host interface of the persistent dual-Newton kernel (K1).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace clb {
+
+// One moment order ("problem") of a launch.  Basis rows are padded to
+// nqp = multiple of the q-chunk, columns laid out as
+//   [0, nb)              basis p_k, k < n (zero for n <= k < nb)
+//   [nb, nb + K2p)       Hessian columns: extended basis (Gaunt) or the
+//                        products p_i p_j, j <= i, at column i(i+1)/2 + j
+// with row stride ldP (ldP % 16 == 4 doubles, conflict-free fragments).
+struct NewtonProblem {
+    const double *P;
+    const double *w;            // [nqp], zero on padded rows
+    const int *hoff;            // Gaunt CSR (row j*n+i for j <= i); null without Gaunt
+    const int *hidx;
+    const double *hval;
+    const unsigned short *pairs;  // n(n+1)/2 entries (i << 8) | j, j <= i, column order
+    double p0;                  // p[0] = Y_00 (fobj.cpp:305 divides by it)
+    int n, nb, K2p, nqp, ldP;
+    int count;                  // vectors to solve
+    double *u, *alpha;          // [count][n]
+    int *iters;                 // nullable [count]
+    double *regs;               // nullable [count]
+    int *status;                // nullable [count]
+    unsigned int *queue;        // work counter, zero before the launch
+};
+
+struct NewtonArgs {
+    NewtonProblem prob[kMaxProblems];
+    int nprob;
+    int momentType, maxIter, useGaunt;
+    double tolRel, condHMax, deltaPPn, tolGamma;
+    // grid mode: copy interior moments to momentsOld before solving them
+    // (momopt_update.cpp:298-308); null otherwise
+    double *momentsOld;
+    int NX, NY;
+    DevStats *stats;
+    int *err;                   // [0] first error code, [1] its vector index
+    // launch layout (doubles unless noted), filled by plan_newton()
+    int T, kq, ldv, ldE, ldG, ldh, ntq, doubleBuffer;
+    int offAlpha, offAold, offD, offU, offScal, offInt, offFpart, offStat;
+    int offP, offE, offEg, offG, offH, offVec;
+    int smemBytes;
+    int tpw;
+};
+
+// Fills the layout fields from the problems' sizes; returns 0 or -1 when
+// the configuration does not fit in shared memory.
+int plan_newton(NewtonArgs &a);
+// Sets the kernel's shared-memory attribute (call once, outside capture).
+cudaError_t prepare_newton(const NewtonArgs &a);
+// Launches the persistent kernel on `stream` over `grid` CTAs.
+cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream);
+int newton_ctas_per_sm(const NewtonArgs &a);
+
+}  // namespace clb

@@ -1,0 +1,189 @@
+/*
+ * closures_gpu.h -- C ABI of libclosures_gpu.so, the B200 (sm_100a) Mn/PPn
+ * entropy-closure path of closures-2d.
+ *
+ * The library replaces, behind plain pointers and sizes, the reference's
+ * momopt hot path:
+ *   - MomOptSolver::update        src/momopt/momopt_update.cpp:283-382
+ *       (solveOptimization :208-277, solveFlux :96-202, Euler/collision/
+ *        source :316-336,:344-364, Heun average :367-377)
+ *   - opt() per-cell dual solve   src/momopt/opt/opt.cpp:82-343 with
+ *       fobj.cpp:37-428 and linesearch.cpp:21-99
+ *   - communicateBoundaries       src/comm.cpp:149-154 (serial: periodic copy,
+ *       momopt_boundaries.cpp:190-223), done on the device
+ *   - angular set-up              src/momopt/momopt_init.cpp:88-259
+ *   - the MomOptSolver state      src/momopt/momopt_solver.h:74-78 (moments,
+ *       alpha, flux) lives in device memory owned by the context.
+ *
+ * Conventions: every int-returning call returns CL_OK (0) or a negative
+ * CL_ERR_* code and records a message retrievable with cl_last_error(); the
+ * context owns all device memory, one CUDA stream and the captured RK2 graph;
+ * the caller owns every host buffer.  A context is used by one host thread at
+ * a time.  There is no CPU fallback: without a usable sm_100 device
+ * cl_create() fails with CL_ERR_CUDA.
+ */
+#ifndef CLOSURES_GPU_H
+#define CLOSURES_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CL_ABI_VERSION 1
+
+enum {
+    CL_OK = 0,
+    CL_ERR_ARG = -1,       /* bad argument / unsupported configuration */
+    CL_ERR_CUDA = -2,      /* CUDA runtime error or no usable device */
+    CL_ERR_U0 = -3,        /* a cell had u0 <= 0 (opt.cpp:97-101 aborts) */
+    CL_ERR_MAXREG = -4,    /* regularisation ladder exhausted (opt.cpp:256-261) */
+    CL_ERR_TIMEOUT = -5,   /* a bounded device wait gave up */
+    CL_ERR_STATE = -6      /* call order / state error */
+};
+
+enum { CL_MN = 0, CL_PPN = 1 };            /* opt/opt.h:34-37 */
+enum { CL_FP64 = 0, CL_MIXED = 1 };        /* arithmetic of the Hessian assembly */
+#define CL_NUM_REG 5                       /* opt/opt.h:39-40 */
+
+/* Angular discretisation: momopt_init.cpp:88-259.  Arrays are owned by the
+ * library and released by cl_angular_free(). */
+typedef struct {
+    int order;          /* MOMOPT_MOMENT_ORDER N */
+    int quad_order;     /* MOMOPT_QUAD_ORDER Q */
+    int use_gaunt;      /* MOMOPT_USE_GAUNT */
+    int n;              /* (N+1)(N+2)/2 moments */
+    int n2;             /* (2N+1)(2N+2)/2 if use_gaunt else n */
+    int nq;             /* Q*Q quadrature points */
+    double *w, *xi, *eta;   /* [nq] weights (sum 4*pi) and directions */
+    double *p;              /* [nq*n2] basis, p[q*n2+k] */
+    int gaunt_nnz;
+    int *gaunt_off;         /* [n*n+1] CSR over (i,j) pairs, row-major i*n+j */
+    int *gaunt_idx;         /* [nnz] extended-moment index */
+    double *gaunt_val;      /* [nnz] coefficient (|beta| > 1e-9 kept) */
+} cl_angular;
+
+/* Builds the quadrature, the z-even real spherical-harmonic basis (with the
+ * Condon-Shortley phase) and, if use_gaunt, the product table, in FP64 on
+ * the host.  Replaces MomOptSolver::init's set-up, momopt_init.cpp:88-259. */
+int cl_angular_create(int order, int quad_order, int use_gaunt, cl_angular *out);
+void cl_angular_free(cl_angular *a);
+
+/* Solver options: the MOMOPT_* deck keys read at momopt_init.cpp:56-68. */
+typedef struct {
+    int moment_type;        /* CL_MN or CL_PPN */
+    int opt_type;           /* must be 0 (Newton, opt.cpp); 1 and 2 are rejected */
+    int max_iter;           /* MOMOPT_MAX_ITER */
+    double tol;             /* MOMOPT_TOL (relative gradient tolerance) */
+    double cond_h_max;      /* MOMOPT_COND_H_MAX */
+    double delta_ppn;       /* MOMOPT_DELTA_PPN */
+    double tol_gamma;       /* optional supplementary test, 0 = off (see DESIGN) */
+    int precision;          /* CL_FP64 or CL_MIXED */
+} cl_options;
+
+/* Grid description: Solver fields of solver.h:15-61 for one node. */
+typedef struct {
+    int nx, ny;             /* interior cells (c_sizeX, c_sizeY) */
+    int ghost;              /* must be 2 (MomOptSolver::getNumGhostCells) */
+    int init_cond;          /* 0 line source/gaussian, 1 lattice, 2 periodic */
+    double init_x, init_y;  /* c_initX, c_initY: least x,y of the interior */
+    double theta;           /* MOMOPT_THETA limiter parameter */
+} cl_grid;
+
+typedef struct {
+    int max_iter;                   /* c_optStats.maxIter */
+    double iter_mean;               /* c_optStats.iterMean */
+    int64_t num_solves;             /* c_optStats.numDualSolves */
+    int64_t hist_reg[CL_NUM_REG];   /* c_optStats.histReg */
+    int64_t total_iter;             /* sum of iterations (device counter) */
+} cl_stats;
+
+typedef struct cl_ctx cl_ctx;
+
+/* Creates a context holding the state of one grid (ghosts included,
+ * (nx+4)*(ny+4) cells, layout I3D(i,j,k) = ((i*(ny+4))+j)*n+k of
+ * solver.h:12-13) and uploads the angular set-up, sigma fields and the
+ * initial moments/alpha.  Replaces MomOptSolver::init's allocations
+ * (momopt_init.cpp:103-160). */
+int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang,
+              const double *sigma_t, const double *sigma_s,
+              const double *moments, const double *alpha, cl_ctx **out);
+void cl_destroy(cl_ctx *ctx);
+const char *cl_last_error(const cl_ctx *ctx);
+/* Message of the last failure of a call that had no context (cl_create,
+ * cl_angular_create). */
+const char *cl_global_error(void);
+
+/* One Heun RK2 step (MomOptSolver::update, momopt_update.cpp:283-382) on the
+ * device, replayed from a captured CUDA graph.  Blocks until the step is
+ * done and reports a device-side error (u0 <= 0, ladder exhausted). */
+int cl_step(cl_ctx *ctx, double dt, double dx, double dy);
+/* Same, without waiting: errors surface at the next cl_sync(). */
+int cl_step_async(cl_ctx *ctx, double dt, double dx, double dy);
+int cl_sync(cl_ctx *ctx);
+
+/* Copies the full state (all cells, ghosts included) to / from the host. */
+int cl_get_state(cl_ctx *ctx, double *moments, double *alpha);
+int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha);
+/* Cumulative optimisation statistics (momopt_update.cpp:256-275). */
+int cl_get_stats(cl_ctx *ctx, cl_stats *s);
+
+/* Batched per-vector operator: the GPU equivalent of calling
+ * opt(n, n2, nq, u, alpha, options, w, p, &outs) (opt.cpp:82-148) on `count`
+ * vectors, in place on u and alpha (host arrays, [count*n] each, the order of
+ * the context's angular set-up).  iters/reg/status (nullable, [count]) receive
+ * outs.iter, outs.r and the per-vector status (0, CL_ERR_U0, CL_ERR_MAXREG). */
+int cl_solve_batch(cl_ctx *ctx, int count, double *u, double *alpha,
+                   int *iters, double *reg, int *status);
+
+/* Same on device pointers (no host copies), on the context's stream. */
+int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
+                          int *d_iters, double *d_reg, int *d_status);
+
+/* Mixed-order batch: a solver context for several moment orders at one
+ * quadrature order, so vectors of different N share one persistent launch.
+ * Device pointers; vectors of order orders[s] are packed in segment s. */
+typedef struct cl_multi cl_multi;
+int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaunt,
+                    const cl_options *opts, cl_multi **out);
+void cl_multi_destroy(cl_multi *m);
+const char *cl_multi_last_error(const cl_multi *m);
+int cl_multi_solve_device(cl_multi *m, const int *counts, double *const *d_u,
+                          double *const *d_alpha, int *const *d_iters,
+                          double *const *d_reg, int *const *d_status);
+/* ------------------------------------------------------------------------
+ * Whole solver behind the reference's Solver interface (solver.h:15-61) for
+ * SOLVER momopt on one node: deck parsing (input_deck_reader.cpp), grid and
+ * initial condition (main.cpp:257-372), MomOptSolver::init
+ * (momopt_init.cpp:51-272), update (momopt_update.cpp:283-382) and
+ * outputData (momopt_output.cpp:21-77, files out_<t>_0.pn / .opt). */
+typedef struct cl_solver cl_solver;
+/* Reads deck_path (input.deck semantics, every MOMOPT_* key required as in
+ * momopt_init.cpp:56-68) and creates the solver; *max_dt receives init()'s
+ * return value (momopt_init.cpp:72).  Output files go to out_dir. */
+int cl_solver_create(const char *deck_path, const char *out_dir, cl_solver **out, double *max_dt);
+int cl_solver_geometry(cl_solver *s, int *nx, int *ny, int *n, double *dx, double *dy, double *t_final,
+                       double *out_delta_t);
+int cl_solver_update(cl_solver *s, double dt);          /* Solver::update */
+int cl_solver_output(cl_solver *s, double time);        /* Solver::outputData */
+cl_ctx *cl_solver_context(cl_solver *s);
+const char *cl_solver_last_error(const cl_solver *s);
+void cl_solver_destroy(cl_solver *s);
+/* main.cpp:204-230: outputs at t = 0 and every OUT_DELTA_T up to T_FINAL;
+ * max_steps >= 0 stops after that many RK2 steps. */
+int cl_run_deck(const char *deck_path, const char *out_dir, int max_steps);
+
+/* Kernel launches issued by the library since load (for the bench). */
+int64_t cl_launch_count(void);
+/* Device pointers of the context's state (ghosts included) for callers that
+ * keep data resident. */
+int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha);
+/* Runs the library's DMMA fragment-layout self check on the device; returns
+ * CL_OK when the FP64 tensor-core GEMM matches a host GEMM. */
+int cl_selftest(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,142 @@
+/*
+ * pyapi.c -- flat entry points of the oracle for ctypes callers
+ * (TEST INFRASTRUCTURE ONLY: tests/, smoke() and the bench's CPU baseline).
+ */
+#include "oracle.h"
+#include <stdlib.h>
+#include <string.h>
+
+/* Batched opt() with a freshly built angular set-up. */
+int orc_batch(int order, int Q, int useGaunt, int momentType, int maxIter, double tol,
+              double condHMax, double deltaPPn, double tolGamma, int count, double *u,
+              double *alpha, int *iters, double *regs, int *status)
+{
+    orc_setup s;
+    int st = orc_setup_create(order, Q, useGaunt, &s);
+    if (st)
+        return st;
+    orc_options o;
+    o.momentType = momentType;
+    o.maxIter = maxIter;
+    o.tolRel = tol;
+    o.condHMax = condHMax;
+    o.deltaPPn = deltaPPn;
+    o.useGaunt = useGaunt;
+    o.tolGamma = tolGamma;
+    st = orc_opt_batch(&s, o, count, u, alpha, iters, regs, status);
+    orc_setup_free(&s);
+    return st;
+}
+
+/* Angular set-up copied into caller buffers (sizes from orc_setup_dims). */
+int orc_setup_dims(int order, int Q, int useGaunt, int *n, int *n2, int *nq, int *nnz)
+{
+    orc_setup s;
+    int st = orc_setup_create(order, Q, useGaunt, &s);
+    if (st)
+        return st;
+    *n = s.n;
+    *n2 = s.n2;
+    *nq = s.nq;
+    *nnz = useGaunt ? s.gaunt.off[s.n * s.n] : 0;
+    orc_setup_free(&s);
+    return 0;
+}
+
+int orc_setup_copy(int order, int Q, int useGaunt, double *w, double *xi, double *eta, double *p,
+                   int *off, int *idx, double *val)
+{
+    orc_setup s;
+    int st = orc_setup_create(order, Q, useGaunt, &s);
+    if (st)
+        return st;
+    memcpy(w, s.w, sizeof(double) * s.nq);
+    memcpy(xi, s.xi, sizeof(double) * s.nq);
+    memcpy(eta, s.eta, sizeof(double) * s.nq);
+    memcpy(p, s.p, sizeof(double) * s.nq * s.n2);
+    if (useGaunt) {
+        int nnz = s.gaunt.off[s.n * s.n];
+        memcpy(off, s.gaunt.off, sizeof(int) * (s.n * s.n + 1));
+        memcpy(idx, s.gaunt.idx, sizeof(int) * nnz);
+        memcpy(val, s.gaunt.val, sizeof(double) * nnz);
+    }
+    orc_setup_free(&s);
+    return 0;
+}
+
+/* Whole-grid solver handle. */
+void *orc_solver_open(const char *deckPath)
+{
+    orc_deck d;
+    if (orc_deck_read(deckPath, &d))
+        return NULL;
+    orc_solver *s = (orc_solver *)malloc(sizeof(orc_solver));
+    if (orc_solver_create(&d, s)) {
+        free(s);
+        return NULL;
+    }
+    return s;
+}
+
+void orc_solver_dims(void *h, int *NX, int *NY, int *n, double *maxDt, double *dx, double *dy)
+{
+    orc_solver *s = (orc_solver *)h;
+    *NX = s->NX;
+    *NY = s->NY;
+    *n = s->set.n;
+    *maxDt = s->maxDt;
+    *dx = s->dx;
+    *dy = s->dy;
+}
+
+/* Runs the time loop of main.cpp but stops after nsteps (no outputs). */
+int orc_solver_steps(void *h, int nsteps)
+{
+    orc_solver *s = (orc_solver *)h;
+    for (int k = 0; k < nsteps; k++) {
+        int st = orc_solver_update(s, s->maxDt);
+        if (st)
+            return st;
+    }
+    return 0;
+}
+
+int orc_solver_step_dt(void *h, double dt) { return orc_solver_update((orc_solver *)h, dt); }
+
+void orc_solver_state(void *h, double *moments, double *alpha)
+{
+    orc_solver *s = (orc_solver *)h;
+    size_t bytes = sizeof(double) * (size_t)s->NX * s->NY * s->set.n;
+    if (moments)
+        memcpy(moments, s->moments, bytes);
+    if (alpha)
+        memcpy(alpha, s->alpha, bytes);
+}
+
+void orc_solver_set_state(void *h, const double *moments, const double *alpha)
+{
+    orc_solver *s = (orc_solver *)h;
+    size_t bytes = sizeof(double) * (size_t)s->NX * s->NY * s->set.n;
+    if (moments)
+        memcpy(s->moments, moments, bytes);
+    if (alpha)
+        memcpy(s->alpha, alpha, bytes);
+}
+
+void orc_solver_stats(void *h, int *maxIter, double *iterMean, long long *numSolves, int *hist)
+{
+    orc_solver *s = (orc_solver *)h;
+    *maxIter = s->stats.maxIter;
+    *iterMean = s->stats.iterMean;
+    *numSolves = s->stats.numDualSolves;
+    for (int i = 0; i < ORC_NUM_REG; i++)
+        hist[i] = s->stats.histReg[i];
+}
+
+void orc_solver_close(void *h)
+{
+    if (!h)
+        return;
+    orc_solver_free((orc_solver *)h);
+    free(h);
+}

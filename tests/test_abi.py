@@ -1,0 +1,104 @@
+"""CPU checks of the C ABI library: it loads, exports every declared entry
+point, its host-side angular set-up matches the oracle's, and the compute
+entry points refuse to run without a GPU (no CPU fallback)."""
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+import closures_b200 as cb
+import decks
+import helpers
+import oracle_lib
+
+HEADER = os.path.join(helpers.REPO, "include", "closures_gpu.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cl_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = cb.lib()
+    names = declared_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert missing == []
+
+
+@pytest.mark.parametrize("order,Q,gaunt", [(1, 8, 0), (2, 20, 0), (2, 20, 1), (3, 30, 1),
+                                           (4, 30, 1), (5, 40, 0), (6, 40, 1)])
+def test_angular_setup_matches_oracle(order, Q, gaunt):
+    a = cb.Angular(order, Q, gaunt)
+    o = oracle_lib.setup(order, Q, gaunt)
+    assert (a.n, a.n2, a.nq) == (o["n"], o["n2"], o["nq"])
+    np.testing.assert_allclose(a.w, o["w"], rtol=1e-13, atol=0)
+    assert abs(a.w.sum() - 4 * np.pi) < 1e-12
+    np.testing.assert_allclose(a.xi, o["xi"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(a.eta, o["eta"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(a.p, o["p"], rtol=0, atol=1e-13)
+    if gaunt:
+        assert (a.gaunt_off == o["off"]).all()
+        assert (a.gaunt_idx == o["idx"]).all()
+        np.testing.assert_allclose(a.gaunt_val, o["val"], rtol=1e-11, atol=1e-13)
+
+
+def test_basis_orthonormal_and_condon_shortley():
+    a = cb.Angular(3, 30, 0)
+    G = (a.p * a.w[:, None]).T @ a.p
+    # the z-even harmonics are orthonormal over the sphere (hemisphere x2)
+    np.testing.assert_allclose(G, np.eye(a.n), atol=1e-13)
+    # Y_{1,1} ~ -sqrt(3/4pi) sin(theta) cos(phi) with the Condon-Shortley phase
+    q = 0
+    mu = np.sqrt(1 - a.xi[q] ** 2 - a.eta[q] ** 2)
+    assert a.p[q, 2] * a.xi[q] < 0
+
+
+def test_sampler_realizable_and_normalised():
+    a = cb.Angular(3, 20, 0)
+    u, alpha = cb.sample_moment_vectors(a, 64, seed=1)
+    assert np.allclose(u[:, 0], 1.0)
+    m = np.exp(alpha @ a.p[:, :a.n].T) @ (a.p[:, :a.n] * a.w[:, None])
+    np.testing.assert_allclose(m, u, rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_no_cpu_fallback():
+    a = cb.Angular(2, 8, 0)
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Context.for_batches(a, cb.make_options())
+    assert e.value.code == cb.CL_ERR_CUDA
+
+
+def test_rejects_change_of_basis_and_bfgs(tmp_path):
+    for opt_type in (1, 2):
+        d = tmp_path / ("deck%d" % opt_type)
+        decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=opt_type,
+                                                  moment_order=1, quad_order=4))
+        with pytest.raises(cb.ClosuresError) as e:
+            cb.Solver(str(d), str(tmp_path))
+        assert e.value.code == cb.CL_ERR_ARG
+        assert "OPTIMIZATION_TYPE" in str(e.value)
+
+
+def test_missing_deck_key_is_an_input_error(tmp_path):
+    text = decks.deck_text(num_cells_x=4, num_cells_y=4, moment_order=1, quad_order=4)
+    text = "\n".join(l for l in text.splitlines() if not l.startswith("MOMOPT_MAX_BFGS_ITER"))
+    d = tmp_path / "deck"
+    decks.write_deck(str(d), text + "\n")
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert e.value.code == cb.CL_ERR_ARG
+    assert "MOMOPT_MAX_BFGS_ITER" in str(e.value)
+
+
+def test_wrong_solver_type(tmp_path):
+    d = tmp_path / "deck"
+    decks.write_deck(str(d), decks.deck_text(solver="kinetic", num_cells_x=4, num_cells_y=4))
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert "Solver type does not exist" in str(e.value)
