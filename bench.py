@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Headline benchmark of the B200 Mn/PPn entropy-closure path.
+
+Metric: Mn cell-solves per second (one cell-solve = one opt() call on one
+cell in one RK stage, ghost cells included, 2 (nx+4)(ny+4) per RK2 step, as
+MomOptSolver::update does) at gradient tolerance 1e-8, plus RK2 steps/s.
+
+Default workload: the M6 800x800 deck (n = 28 moments, Q = 40 -> 1600
+quadrature points, narrow Gaussian pulse sigma = 0.03, floor 1e-8, Gaunt
+Hessian as in the reference's example deck), plain Newton, all FP64,
+advanced W warm-up RK2 steps from t = 0 and then timed for K steps.  The
+state (646,416 cells x 28 moments x {u, alpha}) is 290 MB, larger than L2,
+so no explicit L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+                  [--workload m6_800|pp6_800|m4_lattice_200|m2_50]
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle restatement, OpenMP over all host threads) on the same deck.
+Under torchrun each rank runs an independent replica (weak scaling); the
+timed region is bracketed by barriers and the max over ranks is reported.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "closures-2d_b200"))
+
+import decks  # noqa: E402
+
+METRIC = "Mn cell-solves/s at ||grad||<=1e-8 and steps/s: NN warm-start vs plain, 1 B200"
+
+WORKLOADS = {
+    # the M6 / PP6 800x800 pulse (configs of the headline)
+    "m6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
+                   gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
+                   moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
+                   moment_type="mn"),
+    "pp6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
+                    gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
+                    moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
+                    moment_type="ppn"),
+    # M4 lattice, 200x200 on [-3.5,3.5]^2, Q=30
+    "m4_lattice_200": dict(num_cells_x=200, num_cells_y=200, a_x=-3.5, b_x=3.5, a_y=-3.5,
+                           b_y=3.5, init_cond="lattice", floor=1e-10, moment_order=4,
+                           quad_order=30, tol=1e-8, use_gaunt=1, t_final=3.2),
+    # M2 50x50 Gaussian, Q=20 (the reference's CPU-runnable case)
+    "m2_50": dict(num_cells_x=50, num_cells_y=50, gaussian_sigma=0.4, floor=1e-4,
+                  moment_order=2, quad_order=20, tol=1e-8, use_gaunt=0, t_final=0.5),
+}
+
+
+def flops_per_iteration(n, n2, nq, use_gaunt, nnz):
+    """Algorithmic FLOPs of one Newton iteration (FMA = 2, exp not counted):
+    alpha.m and the Hessian sums over the quadrature, the Gaunt contraction,
+    Cholesky and the small dense solves (fobj.cpp:37-129, opt.cpp:209-318)."""
+    if use_gaunt:
+        per_q = 2 * n + 2 * n2
+        return nq * per_q + 2 * nnz + n ** 3 / 3.0 + 6 * n * n
+    return nq * (2 * n + n * (n + 1)) + n ** 3 / 3.0 + 6 * n * n
+
+
+def flops_per_trial(n, nq):
+    """One line-search function evaluation (linesearch.cpp:53-82)."""
+    return nq * (2 * n + 2)
+
+
+def flops_flux_stage(C, C_int, n, nq):
+    """solveFlux per stage: ansatz alpha.m on all cells, stencil + projection
+    on interior cells (momopt_update.cpp:96-202)."""
+    return C * nq * 2 * n + C_int * nq * (2 * n + 40)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def write_deck(tmpdir, workload):
+    path = os.path.join(tmpdir, "input.deck")
+    decks.write_deck(path, decks.deck_text(**WORKLOADS[workload]))
+    return path
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_oracle_steps(deck, max_steps, budget_s):
+    """The reference algorithm on the host cores (oracle restatement):
+    full RK2 steps of the deck from t = 0.  Returns (steps, seconds, solves)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    threads = cpu_threads()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import pyoracle
+    pyoracle.build()
+    g = pyoracle.GridSolver(deck)
+    C = g.NX * g.NY
+    done, t_total = 0, 0.0
+    while done < max_steps:
+        t0 = time.perf_counter()
+        g.steps(1)
+        t_total += time.perf_counter() - t0
+        done += 1
+        if t_total * (done + 1) / done > budget_s:
+            break
+    g.close()
+    return done, t_total, 2 * C * done, threads
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = write_deck(tmp, args.workload)
+        steps, secs, solves, threads = run_oracle_steps(deck, args.steps, budget_s=150.0)
+    value = solves / secs
+    w = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-solves/s",
+        "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * secs / steps,
+        "steps_per_s": steps / secs, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+                   "moment_order": w["moment_order"], "quad_order": w["quad_order"],
+                   "use_gaunt": w["use_gaunt"], "tol": w["tol"]},
+        "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "first %d RK2 step(s) of the deck from t=0, full grid" % steps},
+        "e2e": {"value": value, "unit": "cell-solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def native_arm(args, world, rank, local):
+    import torch
+    import closures_b200 as cb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    w = WORKLOADS[args.workload]
+    tmp = tempfile.mkdtemp(prefix="bench_")
+    deck = write_deck(tmp, args.workload)
+    solver = cb.Solver(deck, tmp)
+    ctx = solver.context()
+    dt, dx, dy = solver.max_dt, solver.dx, solver.dy
+    C = solver.NX * solver.NY
+    C_int = solver.nx * solver.ny
+    n = solver.n
+    ang = cb.Angular(w["moment_order"], w["quad_order"], w["use_gaunt"])
+    nnz = 0
+    if w["use_gaunt"]:
+        off = ang.gaunt_off
+        for i in range(n):
+            for j in range(i, n):
+                nnz += int(off[i * n + j + 1] - off[i * n + j])
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (advances the simulation from t = 0)
+    for _ in range(args.warmup):
+        solver.update(dt)
+    peak = cb.fp64_peak_tflops()
+
+    st0 = solver.stats()
+    launches0 = cb.launch_count()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    t0 = time.perf_counter()
+    kernel_ms = np.zeros(4)
+    for _ in range(args.steps):
+        kernel_ms += np.array(ctx.step_timed(dt, dx, dy))
+    barrier()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    launches = cb.launch_count() - launches0
+    st1 = solver.stats()
+    device_ms = float(kernel_ms.sum())
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([device_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        device_ms = float(tt.item())
+
+    solves = 2 * C * args.steps
+    value = world * solves / (device_ms * 1e-3)
+    iters = st1["total_iter"] - st0["total_iter"]
+    trials = st1["total_trials"] - st0["total_trials"]
+    newton_ms = float(kernel_ms[0] + kernel_ms[2])
+    flux_ms = float(kernel_ms[1] + kernel_ms[3])
+    f_newton = iters * flops_per_iteration(n, ang.n2, ang.nq, w["use_gaunt"], nnz) + \
+        trials * flops_per_trial(n, ang.nq)
+    f_flux = 2 * args.steps * flops_flux_stage(C, C_int, n, ang.nq)
+    ach_newton = f_newton / (newton_ms * 1e-3) / 1e12
+    ach_flux = f_flux / (flux_ms * 1e-3) / 1e12
+    dominant = "newton" if newton_ms >= flux_ms else "flux"
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state from pinned host memory, runs the RK2 step and reads it back
+    e2e_steps = max(1, min(args.steps, 5))
+    hm = torch.empty((C, n), dtype=torch.float64).pin_memory().numpy()
+    ha = torch.empty((C, n), dtype=torch.float64).pin_memory().numpy()
+    hm2, ha2 = ctx.get_state()
+    hm[:] = hm2.reshape(C, n)
+    ha[:] = ha2.reshape(C, n)
+    barrier()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.set_state(hm, ha)
+        ctx.step(dt, dx, dy)
+        lib = cb.lib()
+        rc = lib.cl_get_state(ctx._ctx, cb._dp(hm), cb._dp(ha))
+        if rc:
+            raise cb.ClosuresError(rc, lib.cl_last_error(ctx._ctx))
+    barrier()
+    e2e_s = time.perf_counter() - t1
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * 2 * C * e2e_steps / e2e_s
+    state_bytes = 2 * C * n * 8
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        steps, secs, solves_cpu, threads = run_oracle_steps(deck, 1, budget_s=60.0)
+        cpu = {"value": solves_cpu / secs, "unit": "cell-solves/s", "cores": threads,
+               "kind": "port",
+               "sample": "first RK2 step of the same deck from t=0 on all %d host threads "
+                         "(oracle restatement, -O3 -fopenmp)" % threads}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": device_ms / args.steps, "steps_per_s": 1e3 * args.steps / device_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+                       "moment_order": w["moment_order"], "n": n, "quad_order": w["quad_order"],
+                       "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
+                       "moment_type": w["moment_type"] if "moment_type" in w else "mn",
+                       "newton": "plain", "precision": "fp64", "t_start": args.warmup * dt,
+                       "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "iter_mean": iters / solves, "trials_per_solve": trials / solves,
+            "kernel_ms": {"newton": newton_ms, "flux": flux_ms},
+            "roofline": {
+                "bound": "fp64", "kernel": dominant,
+                "achieved": ach_newton if dominant == "newton" else ach_flux,
+                "peak": peak, "unit": "TFLOP/s",
+                "frac": (ach_newton if dominant == "newton" else ach_flux) / peak,
+                "traffic": None,
+                "peak_source": "FP64 DMMA m16n8k8 throughput measured live (cl_fp64_peak)",
+                "other": {"newton_tflops": ach_newton, "flux_tflops": ach_flux},
+            },
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-solves/s",
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                    "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--workload", default="m6_800", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+    return native_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

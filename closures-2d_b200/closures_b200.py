@@ -55,7 +55,8 @@ class cl_grid(C.Structure):
 
 class cl_stats(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
-                ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64)]
+                ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64),
+                ("total_trials", C.c_int64)]
 
 
 _lib = None
@@ -80,10 +81,13 @@ def lib():
             "cl_global_error": (C.c_char_p, []),
             "cl_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "cl_step_async": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+            "cl_step_timed": (C.c_int, [vp, C.c_double, C.c_double, C.c_double,
+                                        C.POINTER(C.c_float)]),
             "cl_sync": (C.c_int, [vp]),
             "cl_get_state": (C.c_int, [vp, dp, dp]),
             "cl_set_state": (C.c_int, [vp, dp, dp]),
             "cl_get_stats": (C.c_int, [vp, C.POINTER(cl_stats)]),
+            "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
             "cl_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
@@ -95,6 +99,7 @@ def lib():
                                                 C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
             "cl_launch_count": (C.c_int64, []),
             "cl_selftest": (C.c_int, []),
+            "cl_fp64_peak": (C.c_int, [C.POINTER(C.c_double)]),
             "cl_solver_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(vp), dp]),
             "cl_solver_geometry": (C.c_int, [vp, ip, ip, ip, dp, dp, dp, dp]),
             "cl_solver_update": (C.c_int, [vp, C.c_double]),
@@ -136,6 +141,13 @@ def launch_count():
 
 def selftest():
     _check(lib().cl_selftest(), lib().cl_global_error)
+
+
+def fp64_peak_tflops():
+    """Measured FP64 tensor-core throughput of the current device."""
+    v = C.c_double()
+    _check(lib().cl_fp64_peak(C.byref(v)), lib().cl_global_error)
+    return v.value
 
 
 class Angular:
@@ -198,9 +210,9 @@ class Context:
         return cls(g, options, angular, np.ones(C_), np.ones(C_), m, a)
 
     def close(self):
-        if self._ctx:
+        if self._ctx and not getattr(self, "_borrowed", False):
             lib().cl_destroy(self._ctx)
-            self._ctx = C.c_void_p()
+        self._ctx = C.c_void_p()
 
     def __del__(self):
         if _lib is not None and getattr(self, "_ctx", None):
@@ -211,6 +223,12 @@ class Context:
 
     def step(self, dt, dx, dy):
         _check(lib().cl_step(self._ctx, dt, dx, dy), self._err)
+
+    def step_timed(self, dt, dx, dy):
+        """One RK2 step kernel by kernel; returns the four kernel durations (ms)."""
+        ms = (C.c_float * 4)()
+        _check(lib().cl_step_timed(self._ctx, dt, dx, dy, ms), self._err)
+        return list(ms)
 
     def step_async(self, dt, dx, dy):
         _check(lib().cl_step_async(self._ctx, dt, dx, dy), self._err)
@@ -229,11 +247,17 @@ class Context:
         a = np.ascontiguousarray(alpha, dtype=np.float64)
         _check(lib().cl_set_state(self._ctx, _dp(m), _dp(a)), self._err)
 
+    def last_iterations(self):
+        it = np.empty(self.NX * self.NY, np.int32)
+        _check(lib().cl_get_last_iterations(self._ctx, _ip(it)), self._err)
+        return it.reshape(self.NX, self.NY)
+
     def stats(self):
         s = cl_stats()
         _check(lib().cl_get_stats(self._ctx, C.byref(s)), self._err)
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
-                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter}
+                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
+                "total_trials": s.total_trials}
 
     def solve_batch(self, u, alpha, check=True):
         """opt() on every row of u/alpha (in place).  Returns iters, reg, status."""
@@ -316,6 +340,14 @@ class Solver:
     def output_data(self, time):
         _check(lib().cl_solver_output(self._s, time), self._err)
 
+    def context(self):
+        """The device context (shares the solver's state)."""
+        c = Context.__new__(Context)
+        c._ctx = C.c_void_p(lib().cl_solver_context(self._s))
+        c._borrowed = True
+        c.n, c.NX, c.NY = self.n, self.NX, self.NY
+        return c
+
     def context_state(self):
         ctx = lib().cl_solver_context(self._s)
         m = np.empty((self.NX * self.NY, self.n))
@@ -323,12 +355,19 @@ class Solver:
         _check(lib().cl_get_state(ctx, _dp(m), _dp(a)), lambda: lib().cl_last_error(ctx))
         return m.reshape(self.NX, self.NY, self.n), a.reshape(self.NX, self.NY, self.n)
 
+    def last_iterations(self):
+        ctx = lib().cl_solver_context(self._s)
+        it = np.empty(self.NX * self.NY, np.int32)
+        _check(lib().cl_get_last_iterations(ctx, _ip(it)), lambda: lib().cl_last_error(ctx))
+        return it.reshape(self.NX, self.NY)
+
     def stats(self):
         ctx = lib().cl_solver_context(self._s)
         s = cl_stats()
         _check(lib().cl_get_stats(ctx, C.byref(s)), lambda: lib().cl_last_error(ctx))
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
-                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter}
+                "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
+                "total_trials": s.total_trials}
 
     def close(self):
         if self._s:

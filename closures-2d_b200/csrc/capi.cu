@@ -236,6 +236,7 @@ struct cl_ctx {
     DevStats *dStats = nullptr;
     int *dErr = nullptr;
     int *hErr = nullptr;              // pinned [2]
+    int *dIters = nullptr;            // [C] iterations of each cell in the last stage
     NewtonArgs nargs;
     FluxArgs fargs;
     int nCtas = 0;
@@ -365,7 +366,8 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         cudaMalloc(&ctx->dOld, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dSigT, C * 8) != cudaSuccess ||
         cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, 4 * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&ctx->dStats, sizeof(DevStats)) != cudaSuccess || cudaMalloc(&ctx->dErr, 2 * sizeof(int)) != cudaSuccess ||
-        cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess) {
+        cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dIters, C * sizeof(int)) != cudaSuccess) {
         ctx->err = "device allocation failed";
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
@@ -456,6 +458,7 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->dStats);
     cudaFree(ctx->dErr);
     cudaFreeHost(ctx->hErr);
+    cudaFree(ctx->dIters);
     cudaFree(ctx->bU);
     cudaFree(ctx->bA);
     cudaFree(ctx->bR);
@@ -485,6 +488,7 @@ static cudaError_t enqueue_step(cl_ctx *ctx, double dt, double dx, double dy, in
         a.prob[0].u = ctx->dMom;
         a.prob[0].alpha = ctx->dAlpha;
         a.prob[0].queue = ctx->dQueue + stage;
+        a.prob[0].iters = ctx->dIters;
         a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
         if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
             return e;
@@ -557,6 +561,61 @@ int cl_step_async(cl_ctx *ctx, double dt, double dx, double dy)
     return CL_OK;
 }
 
+int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms)
+{
+    if (!ctx || !ms)
+        return CL_ERR_ARG;
+    cudaEvent_t ev[7];
+    for (int i = 0; i < 7; i++)
+        CUDA_TRY(ctx, cudaEventCreate(&ev[i]));
+    const bool periodic = ctx->grid.init_cond == 2;
+    cudaError_t e = cudaMemsetAsync(ctx->dQueue, 0, 2 * sizeof(unsigned), ctx->stream);
+    int nk = 0;
+    for (int stage = 0; stage < 2 && e == cudaSuccess; stage++) {
+        cudaEventRecord(ev[3 * stage], ctx->stream);
+        if (periodic) {
+            e = launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, ctx->stream);
+            nk += 2;
+        }
+        NewtonArgs a = ctx->nargs;
+        a.prob[0].count = (int)ctx->C;
+        a.prob[0].u = ctx->dMom;
+        a.prob[0].alpha = ctx->dAlpha;
+        a.prob[0].queue = ctx->dQueue + stage;
+        a.prob[0].iters = ctx->dIters;
+        a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
+        if (e == cudaSuccess)
+            e = launch_newton(a, ctx->nCtas, ctx->stream);
+        nk++;
+        cudaEventRecord(ev[3 * stage + 1], ctx->stream);
+        FluxArgs f = ctx->fargs;
+        f.dt = dt;
+        f.dx = dx;
+        f.dy = dy;
+        f.momentsOld = (stage == 1) ? ctx->dOld : nullptr;
+        if (e == cudaSuccess)
+            e = launch_flux(f, ctx->stream);
+        nk++;
+        cudaEventRecord(ev[3 * stage + 2], ctx->stream);
+    }
+    g_launches += nk;
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) {
+        cudaEventElapsedTime(&ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[1], ev[1], ev[2]);
+        cudaEventElapsedTime(&ms[2], ev[3], ev[4]);
+        cudaEventElapsedTime(&ms[3], ev[4], ev[5]);
+    }
+    for (int i = 0; i < 7; i++)
+        cudaEventDestroy(ev[i]);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("timed step: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return read_device_error(ctx);
+}
+
 int cl_sync(cl_ctx *ctx)
 {
     if (!ctx)
@@ -598,6 +657,15 @@ int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha)
     return CL_OK;
 }
 
+int cl_get_last_iterations(cl_ctx *ctx, int *iters)
+{
+    if (!ctx || !iters)
+        return CL_ERR_ARG;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(iters, ctx->dIters, (size_t)ctx->C * sizeof(int), cudaMemcpyDeviceToHost));
+    return CL_OK;
+}
+
 int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha)
 {
     if (!ctx)
@@ -622,6 +690,7 @@ int cl_get_stats(cl_ctx *ctx, cl_stats *s)
     for (int i = 0; i < CL_NUM_REG; i++)
         s->hist_reg[i] = (int64_t)d.hist[i];
     s->iter_mean = d.numSolves ? (double)d.totalIter / (double)d.numSolves : 0.0;
+    s->total_trials = (int64_t)d.trials;
     return CL_OK;
 }
 
@@ -892,3 +961,70 @@ extern "C" int cl_selftest(void)
 
 // Lets the host solver layer report through cl_global_error().
 void clb_set_global_error(const char *msg) { g_global_err = msg ? msg : ""; }
+
+// ------------------------------------------------------------- FP64 peak
+namespace {
+// Independent DMMA chains per warp; each m16n8k8 is 1024 FMA = 2048 flops.
+__global__ void dmma_peak_kernel(double *out, int iters)
+{
+    double a0 = 1e-3 * threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3;
+    double b0 = 2e-3 * threadIdx.x, b1 = b0 + 1;
+    double c[8][4];
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+        c[u][0] = c[u][1] = c[u][2] = c[u][3] = 0.0;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            dmma16x8x8(c[u], a0, a1, a2, a3, b0, b1);
+    }
+    double s = 0;
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+        s += c[u][0] + c[u][1] + c[u][2] + c[u][3];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+}  // namespace
+
+extern "C" int cl_fp64_peak(double *tflops)
+{
+    if (!tflops)
+        return CL_ERR_ARG;
+    int sms = sm_count();
+    if (sms <= 0) {
+        g_global_err = "no CUDA device";
+        return CL_ERR_CUDA;
+    }
+    const int blocks = sms * 4, threads = 256, iters = 4000;
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * blocks * threads) != cudaSuccess) {
+        g_global_err = "peak probe allocation failed";
+        return CL_ERR_CUDA;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    dmma_peak_kernel<<<blocks, threads>>>(d, 100);
+    float best = 1e30f;
+    for (int r = 0; r < 3; r++) {
+        cudaEventRecord(e0);
+        dmma_peak_kernel<<<blocks, threads>>>(d, iters);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = ms < best ? ms : best;
+    }
+    g_launches += 4;
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        g_global_err = std::string("peak probe: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    double flops = 2048.0 * 8.0 * iters * (blocks * (threads / 32));
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return CL_OK;
+}

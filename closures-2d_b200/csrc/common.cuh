@@ -69,12 +69,16 @@ __device__ __forceinline__ int warp_argmax_first(double v, int lane)
     return idx;
 }
 
+// Device counters of the optimisation stages; the first kStatU64 fields are
+// 64-bit sums, laid out contiguously so a CTA can flush them by index.
 struct DevStats {
-    unsigned long long hist[kNumReg];
-    unsigned long long totalIter;
+    unsigned long long hist[kNumReg];   // solves per regularisation level
+    unsigned long long totalIter;       // sum of outs.iter
     unsigned long long numSolves;
+    unsigned long long trials;          // line-search evaluations
     int maxIter;
     int pad;
 };
+constexpr int kStatU64 = kNumReg + 3;
 
 }  // namespace clb

@@ -228,7 +228,7 @@ __device__ void finish_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout
             atomicAdd(&L.stat[reg], 1ull);
             atomicAdd(&L.stat[kNumReg], (unsigned long long)total);
             atomicAdd(&L.stat[kNumReg + 1], 1ull);
-            atomicMax((int *)&L.stat[kNumReg + 2], total);
+            atomicMax((int *)&L.stat[kStatU64], total);
         } else {
             record_error(a.err, status, cell);
         }
@@ -401,6 +401,8 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
 
     int state = si[SI_STATE];
     if (state == S_TRIAL) {
+        if (lane == 0)
+            atomicAdd(&L.stat[kNumReg + 2], 1ull);
         double t = sc[SC_T];
         if (!(fsum <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD])) {
             t = 0.5 * t;
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         L.alpha[i] = 0.0;   // alpha, aold, d, u are contiguous
     for (int i = tid; i < T * SI_N; i += kThreads)
         L.ints[i] = (i % SI_N == SI_STATE) ? S_IDLE : 0;
-    for (int i = tid; i < kNumReg + 3; i += kThreads)
+    for (int i = tid; i <= kStatU64; i += kThreads)
         L.stat[i] = 0ull;
     if (tid == 0) {
         ctl[0] = 0;
@@ -721,13 +723,13 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         __syncthreads();
     }
 
-    // flush CTA statistics
-    if (tid < kNumReg + 2) {
+    // flush CTA statistics (hist, totalIter, numSolves, trials are contiguous)
+    if (tid < kStatU64) {
         unsigned long long v = L.stat[tid];
         if (v)
-            atomicAdd(&a.stats->hist[0] + tid, v);   // hist[0..4], totalIter, numSolves contiguous
-    } else if (tid == kNumReg + 2) {
-        atomicMax(&a.stats->maxIter, *(int *)&L.stat[kNumReg + 2]);
+            atomicAdd(&a.stats->hist[0] + tid, v);
+    } else if (tid == kStatU64) {
+        atomicMax(&a.stats->maxIter, *(int *)&L.stat[kStatU64]);
     }
 }
 
@@ -765,7 +767,7 @@ int plan_newton(NewtonArgs &a)
     a.offScal = take(T * SC_N);
     a.offInt = take((T * SI_N + 1) / 2);
     a.offFpart = take(T * a.ntq);
-    a.offStat = take(kNumReg + 3);
+    a.offStat = take(kStatU64 + 1);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
     a.tpw = (ntiles2 + kWarps - 1) / kWarps;

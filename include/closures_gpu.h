@@ -97,6 +97,7 @@ typedef struct {
     int64_t num_solves;             /* c_optStats.numDualSolves */
     int64_t hist_reg[CL_NUM_REG];   /* c_optStats.histReg */
     int64_t total_iter;             /* sum of iterations (device counter) */
+    int64_t total_trials;           /* line-search function evaluations */
 } cl_stats;
 
 typedef struct cl_ctx cl_ctx;
@@ -119,6 +120,11 @@ const char *cl_global_error(void);
  * device, replayed from a captured CUDA graph.  Blocks until the step is
  * done and reports a device-side error (u0 <= 0, ladder exhausted). */
 int cl_step(cl_ctx *ctx, double dt, double dx, double dy);
+/* Same step launched kernel by kernel (no graph) with CUDA events on the
+ * context's stream; ms[0..3] receive the durations of the stage-1
+ * optimisation, stage-1 flux/update, stage-2 optimisation and stage-2
+ * flux/update/average kernels. */
+int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms);
 /* Same, without waiting: errors surface at the next cl_sync(). */
 int cl_step_async(cl_ctx *ctx, double dt, double dx, double dy);
 int cl_sync(cl_ctx *ctx);
@@ -128,6 +134,8 @@ int cl_get_state(cl_ctx *ctx, double *moments, double *alpha);
 int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha);
 /* Cumulative optimisation statistics (momopt_update.cpp:256-275). */
 int cl_get_stats(cl_ctx *ctx, cl_stats *s);
+/* outs.iter of every cell (ghosts included) in the last optimisation stage. */
+int cl_get_last_iterations(cl_ctx *ctx, int *iters);
 
 /* Batched per-vector operator: the GPU equivalent of calling
  * opt(n, n2, nq, u, alpha, options, w, p, &outs) (opt.cpp:82-148) on `count`
@@ -179,6 +187,9 @@ int64_t cl_launch_count(void);
 /* Device pointers of the context's state (ghosts included) for callers that
  * keep data resident. */
 int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha);
+/* Measures the FP64 tensor-core (DMMA m16n8k8) throughput of the current
+ * device in TFLOP/s: the roofline denominator of the FP64-bound kernels. */
+int cl_fp64_peak(double *tflops);
 /* Runs the library's DMMA fragment-layout self check on the device; returns
  * CL_OK when the FP64 tensor-core GEMM matches a host GEMM. */
 int cl_selftest(void);

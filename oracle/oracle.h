@@ -132,6 +132,7 @@ typedef struct {
     double *initialGrid, *sigmaT, *sigmaS;   /* [NX*NY] */
     double *moments, *alpha, *flux, *momentsOld, *ansatzGrid;
     orc_stats stats;
+    int *lastIters;         /* per-cell iterations of the last stage */
     int status;             /* first error code seen */
     int64_t errCell;
 } orc_solver;

@@ -140,3 +140,13 @@ void orc_solver_close(void *h)
     orc_solver_free((orc_solver *)h);
     free(h);
 }
+
+int orc_solver_stage(orc_solver *s, double dt);
+int orc_solver_stage_h(void *h, double dt) { return orc_solver_stage((orc_solver *)h, dt); }
+long long orc_solver_err_cell(void *h) { return ((orc_solver *)h)->errCell; }
+
+void orc_solver_last_iters(void *h, int *iters)
+{
+    orc_solver *s = (orc_solver *)h;
+    memcpy(iters, s->lastIters, sizeof(int) * (size_t)s->NX * s->NY);
+}

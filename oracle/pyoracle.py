@@ -1,23 +1,51 @@
-"""ctypes binding of the oracle (oracle/liboracle.so) for the tests.
+"""ctypes binding of the oracle (liboracle.so in this directory).
 
-The oracle is the checker: a CPU restatement of the reference algorithm,
-pinned to the reference's regression goldens (test_oracle_golden.py).
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+CPU-baseline / reference arm of bench.py.  The oracle is the checker, a CPU
+restatement of the reference algorithm pinned to the reference's regression
+goldens (tests/test_oracle_golden.py).
 """
 import ctypes as C
 import os
+import subprocess
+import threading
 
 import numpy as np
 
-import helpers
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+_build_lock = threading.Lock()
+_built = False
+
+
+def build():
+    """Builds the oracle libraries and driver once per process."""
+    global _built
+    with _build_lock:
+        if not _built:
+            subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+            _built = True
+    return os.path.join(ORACLE_DIR, "oracle_momopt")
 
 _lib = None
+_lib_fma = None
 
 
-def lib():
-    global _lib
+def lib(fma=False):
+    """The oracle; fma=True gives the same code compiled with FMA contraction."""
+    global _lib, _lib_fma
+    if fma:
+        if _lib_fma is None:
+            build()
+            _lib_fma = _bind(C.CDLL(os.path.join(ORACLE_DIR, "liboracle_fma.so")))
+        return _lib_fma
     if _lib is None:
-        helpers.build_oracle()
-        L = C.CDLL(os.path.join(helpers.ORACLE_DIR, "liboracle.so"))
+        build()
+        _lib = _bind(C.CDLL(os.path.join(ORACLE_DIR, "liboracle.so")))
+    return _lib
+
+
+def _bind(L):
+    if True:
         dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
         L.orc_batch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                 C.c_double, C.c_double, C.c_int, dp, dp, ip, dp, ip]
@@ -32,8 +60,8 @@ def lib():
         L.orc_solver_set_state.argtypes = [vp, dp, dp]
         L.orc_solver_stats.argtypes = [vp, ip, dp, C.POINTER(C.c_longlong), ip]
         L.orc_solver_close.argtypes = [vp]
-        _lib = L
-    return _lib
+        L.orc_solver_last_iters.argtypes = [vp, ip]
+    return L
 
 
 def _dp(a):
@@ -62,53 +90,59 @@ def setup(order, Q, use_gaunt):
 
 
 def opt_batch(order, Q, use_gaunt, u, alpha, moment_type=0, max_iter=100, tol=1e-8,
-              cond_h_max=1e10, delta_ppn=1e-10, tol_gamma=0.0):
+              cond_h_max=1e10, delta_ppn=1e-10, tol_gamma=0.0, fma=False):
     """opt() on each row of u/alpha in place; returns iters, regs, status."""
     count = u.shape[0]
     iters = np.zeros(count, np.int32)
     regs = np.zeros(count)
     status = np.zeros(count, np.int32)
-    lib().orc_batch(order, Q, int(use_gaunt), moment_type, max_iter, tol, cond_h_max, delta_ppn,
+    lib(fma).orc_batch(order, Q, int(use_gaunt), moment_type, max_iter, tol, cond_h_max, delta_ppn,
                     tol_gamma, count, _dp(u), _dp(alpha), _ip(iters), _dp(regs), _ip(status))
     return iters, regs, status
 
 
 class GridSolver:
-    def __init__(self, deck_path):
-        self.h = lib().orc_solver_open(deck_path.encode())
+    def __init__(self, deck_path, fma=False):
+        self.L = lib(fma)
+        self.h = self.L.orc_solver_open(deck_path.encode())
         assert self.h, "oracle rejected the deck"
         NX, NY, n = C.c_int(), C.c_int(), C.c_int()
         md, dx, dy = C.c_double(), C.c_double(), C.c_double()
-        lib().orc_solver_dims(self.h, C.byref(NX), C.byref(NY), C.byref(n), C.byref(md),
+        self.L.orc_solver_dims(self.h, C.byref(NX), C.byref(NY), C.byref(n), C.byref(md),
                               C.byref(dx), C.byref(dy))
         self.NX, self.NY, self.n = NX.value, NY.value, n.value
         self.max_dt, self.dx, self.dy = md.value, dx.value, dy.value
 
     def steps(self, k):
-        st = lib().orc_solver_steps(self.h, k)
+        st = self.L.orc_solver_steps(self.h, k)
         assert st == 0, "oracle error %d" % st
 
     def state(self):
         m = np.empty((self.NX, self.NY, self.n))
         a = np.empty((self.NX, self.NY, self.n))
-        lib().orc_solver_state(self.h, _dp(m), _dp(a))
+        self.L.orc_solver_state(self.h, _dp(m), _dp(a))
         return m, a
 
     def set_state(self, m, a):
         m = np.ascontiguousarray(m, dtype=np.float64)
         a = np.ascontiguousarray(a, dtype=np.float64)
-        lib().orc_solver_set_state(self.h, _dp(m), _dp(a))
+        self.L.orc_solver_set_state(self.h, _dp(m), _dp(a))
+
+    def last_iterations(self):
+        it = np.empty(self.NX * self.NY, np.int32)
+        self.L.orc_solver_last_iters(self.h, _ip(it))
+        return it.reshape(self.NX, self.NY)
 
     def stats(self):
         mi, im, ns = C.c_int(), C.c_double(), C.c_longlong()
         hist = np.zeros(5, np.int32)
-        lib().orc_solver_stats(self.h, C.byref(mi), C.byref(im), C.byref(ns), _ip(hist))
+        self.L.orc_solver_stats(self.h, C.byref(mi), C.byref(im), C.byref(ns), _ip(hist))
         return {"max_iter": mi.value, "iter_mean": im.value, "num_solves": ns.value,
                 "hist_reg": hist.tolist()}
 
     def close(self):
         if self.h:
-            lib().orc_solver_close(self.h)
+            self.L.orc_solver_close(self.h)
             self.h = None
 
     def __del__(self):

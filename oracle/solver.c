@@ -246,6 +246,7 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
     s->flux = (double *)calloc(C * n, sizeof(double));
     s->momentsOld = (double *)calloc(C * n, sizeof(double));
     s->ansatzGrid = (double *)malloc(sizeof(double) * C);
+    s->lastIters = (int *)calloc(C, sizeof(int));
     /* momopt_init.cpp:120-143 */
     for (int i = s->gX[0]; i <= s->gX[3]; i++)
         for (int j = s->gY[0]; j <= s->gY[3]; j++) {
@@ -277,6 +278,7 @@ void orc_solver_free(orc_solver *s)
     free(s->flux);
     free(s->momentsOld);
     free(s->ansatzGrid);
+    free(s->lastIters);
     orc_setup_free(&s->set);
     memset(s, 0, sizeof(*s));
 }
@@ -320,6 +322,7 @@ static void solve_optimization(orc_solver *s)
         orc_outs outs = {0.0, 0, 0.0};
         int st = orc_opt(n, s->set.n2, s->set.nq, &s->moments[(size_t)index * n],
                          &s->alpha[(size_t)index * n], o, s->set.w, s->set.p, &s->set.gaunt, &outs);
+        s->lastIters[index] = outs.iter;
 #pragma omp critical
         {
             if (st != ORC_OK && s->status == ORC_OK) {
@@ -536,5 +539,18 @@ int orc_solver_run(orc_solver *s, const char *dir, int nsteps_max)
         if (tOut > tFinal - 1e-12 * tFinal)
             break;
     }
+    return ORC_OK;
+}
+
+/* One RK stage without the Heun average (diagnostics for the tests). */
+int orc_solver_stage(orc_solver *s, double dt)
+{
+    if (s->deck.initCond == 2)
+        duplicate_boundaries(s);
+    solve_optimization(s);
+    if (s->status != ORC_OK)
+        return s->status;
+    solve_flux(s, s->dx, s->dy);
+    euler_collide(s, dt, s->dx, s->dy);
     return ORC_OK;
 }

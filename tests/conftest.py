@@ -7,6 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.join(REPO, "closures-2d_b200"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
 
 
 def pytest_configure(config):

@@ -16,18 +16,12 @@ PKG_DIR = os.path.join(REPO, "closures-2d_b200")
 # util/formats.py:168-191 -- "=2q4dq" header then [nx][ny][n] doubles
 PN_HEADER = struct.Struct("=2q4dq")
 
-_build_lock = threading.Lock()
-_oracle_built = False
 
 
 def build_oracle():
     """Builds the oracle (test infrastructure) once per session."""
-    global _oracle_built
-    with _build_lock:
-        if not _oracle_built:
-            subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
-            _oracle_built = True
-    return os.path.join(ORACLE_DIR, "oracle_momopt")
+    import pyoracle
+    return pyoracle.build()
 
 
 def parse_pn(data):

@@ -11,7 +11,7 @@ import torch
 import closures_b200 as cb
 import decks
 import helpers
-import oracle_lib
+import pyoracle as oracle_lib
 
 HEADER = os.path.join(helpers.REPO, "include", "closures_gpu.h")
 
