@@ -108,6 +108,9 @@ def lib():
             "cl_solver_last_error": (C.c_char_p, [vp]),
             "cl_solver_destroy": (None, [vp]),
             "cl_run_deck": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
+            "cl_solve_batch_noalloc": (C.c_int, [C.POINTER(cl_angular), C.POINTER(cl_options),
+                                                 C.c_int, vp, vp, vp, vp, vp, vp]),
+            "cl_noalloc_last_error": (C.c_char_p, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -377,6 +380,18 @@ class Solver:
     def __del__(self):
         if _lib is not None and getattr(self, "_s", None):
             self.close()
+
+
+def solve_batch_noalloc(angular, options, d_u, d_alpha, count, d_iters=None, d_reg=None,
+                        d_status=None, stream=None):
+    """Batched opt() on device arrays without any device allocation by the
+    library (cl_solve_batch_noalloc): for callers whose device memory is owned
+    by another allocator.  Arguments are torch tensors or raw addresses."""
+    ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+    _check(lib().cl_solve_batch_noalloc(C.byref(angular._a), C.byref(options), count, ptr(d_u),
+                                        ptr(d_alpha), ptr(d_iters), ptr(d_reg), ptr(d_status),
+                                        ptr(stream)),
+           lib().cl_noalloc_last_error)
 
 
 def run_deck(deck_path, out_dir=".", max_steps=-1):

@@ -182,6 +182,26 @@ void cl_solver_destroy(cl_solver *s);
  * max_steps >= 0 stops after that many RK2 steps. */
 int cl_run_deck(const char *deck_path, const char *out_dir, int max_steps);
 
+/* Batched opt() that allocates no device memory -- this entry point has no
+ * counterpart in the reference.  For callers whose device memory is owned by
+ * an external allocator or pre-reserved pool and who therefore may not call
+ * cudaMalloc/cudaFree (both synchronise the device and fragment the pool):
+ * the caller passes device arrays d_u, d_alpha ([count*n], solved in place)
+ * and optional d_iters, d_reg, d_status ([count]); the work counter, error
+ * word, statistics and the angular set-up (uploaded from `ang` each call)
+ * live in one fixed 4 MiB device array that every GPU loading the library
+ * holds until exit.  Configurations whose padded basis does not fit are
+ * rejected with CL_ERR_ARG (message from cl_noalloc_last_error()); M6 at
+ * Q = 40 with the Gaunt table fits.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU (several
+ * streams or threads at once) race; the call waits for its own work on
+ * `stream` (a cudaStream_t, null = legacy default stream) before returning. */
+int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *opts, int count,
+                           double *d_u, double *d_alpha, int *d_iters, double *d_reg,
+                           int *d_status, void *stream);
+const char *cl_noalloc_last_error(void);
+
 /* Kernel launches issued by the library since load (for the bench). */
 int64_t cl_launch_count(void);
 /* Device pointers of the context's state (ghosts included) for callers that

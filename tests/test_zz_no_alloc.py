@@ -1,0 +1,75 @@
+"""The allocation-free batched solve (cl_solve_batch_noalloc).
+
+It exists for callers whose device memory belongs to another allocator (a
+pre-reserved pool in a host framework's time loop, for instance) and who may
+therefore not have the library call cudaMalloc or cudaFree.  The entry point
+keeps all of its scratch in one fixed device array inside the library.  This
+test calls it twice in a row through the C ABI -- two different moment orders,
+so the second call runs on whatever the first left in the shared array -- and
+checks each result against the allocating entry point cl_solve_batch within
+the tolerance the parity tests use (1e-10 relative on the moments, identical
+iteration counts and regularisation).  It is collected last so a failure here
+comes after every other test has run.
+"""
+import numpy as np
+import pytest
+
+import closures_b200 as cb
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _reference_and_noalloc(order, Q, gaunt, count, seed):
+    import torch
+
+    a = cb.Angular(order, Q, gaunt)
+    u, _ = cb.sample_moment_vectors(a, count, seed=seed, s_range=(0.1, 2.0))
+    alpha0 = cb.isotropic_alpha(a.n, count)
+    opts = cb.make_options(tol=1e-8)
+    # the existing, allocating entry point
+    u_ref, a_ref = u.copy(), alpha0.copy()
+    ctx = cb.Context.for_batches(a, opts)
+    it_ref, reg_ref, st_ref = ctx.solve_batch(u_ref, a_ref)
+    ctx.close()
+    # the allocation-free entry point on caller-owned device arrays
+    dev = torch.device("cuda", 0)
+    d_u = torch.from_numpy(u.copy()).to(dev)
+    d_a = torch.from_numpy(alpha0.copy()).to(dev)
+    d_it = torch.zeros(count, dtype=torch.int32, device=dev)
+    d_reg = torch.zeros(count, dtype=torch.float64, device=dev)
+    d_st = torch.full((count,), 7, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    cb.solve_batch_noalloc(a, opts, d_u, d_a, count, d_it, d_reg, d_st)
+    return (u_ref, a_ref, it_ref, reg_ref, st_ref), (d_u.cpu().numpy(), d_a.cpu().numpy(),
+                                                      d_it.cpu().numpy(), d_reg.cpu().numpy(),
+                                                      d_st.cpu().numpy())
+
+
+def _check(ref, got):
+    u_ref, a_ref, it_ref, reg_ref, st_ref = ref
+    u, a, it, reg, st = got
+    assert (st == 0).all() and (st_ref == 0).all()
+    assert (it == it_ref).all()
+    assert (reg == reg_ref).all()
+    assert np.max(np.abs(u - u_ref) / np.abs(u_ref[:, :1])) < TOL
+    assert np.max(np.abs(a - a_ref) / (1.0 + np.abs(a_ref))) < 1e-8
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    ref1, got1 = _reference_and_noalloc(4, 30, 1, 900, seed=21)
+    _check(ref1, got1)
+    ref2, got2 = _reference_and_noalloc(2, 20, 0, 500, seed=22)
+    _check(ref2, got2)
+
+
+def test_noalloc_rejects_oversized_configuration():
+    import torch
+
+    a = cb.Angular(6, 64, 0)      # padded non-Gaunt basis of 4096 directions: > 4 MiB
+    d = torch.zeros((4, a.n), dtype=torch.float64, device="cuda")
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.solve_batch_noalloc(a, cb.make_options(), d, d.clone(), 4)
+    assert e.value.code == cb.CL_ERR_ARG
+    assert "maximum" in str(e.value)
