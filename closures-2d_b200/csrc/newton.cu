@@ -51,60 +51,64 @@ __device__ __forceinline__ void record_error(int *err, int code, int idx)
         err[1] = idx;
 }
 
-// Cholesky of the n x n symmetric matrix in Hs (row stride ldh) in place,
-// lower triangle; returns LAPACK-style info (0 ok, j+1 at the first
-// non-positive or NaN pivot).  Right-looking; lanes share each trailing
-// update through the column-ordered pair list.
-__device__ int chol_warp(double *Hs, int n, int ldh, const unsigned short *pairsCol, int lane)
+// Cholesky of the symmetric matrix whose row `lane` is h[] (registers), in
+// the dot-product (Crout) form by columns: lane i >= j forms
+// L_ij = (H_ij - sum_k<j L_ik L_jk) / L_jj with row j of L broadcast from
+// lane j.  On return h[k] = L_lane,k for k <= lane.  LAPACK-style info: 0, or
+// j+1 at the first non-positive or NaN pivot (dpotrf semantics).
+__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], int n, int lane)
 {
-    // pairsCol lists (i,k) with k <= i ordered by column k; start of column k
-    // is k*n - k(k-1)/2.
-    for (int j = 0; j < n; j++) {
-        double ajj = Hs[j * ldh + j];
-        if (!(ajj > 0.0))
-            return j + 1;
-        double ljj = sqrt(ajj);
-        double r = 1.0 / ljj;
-        __syncwarp();
-        if (lane > j && lane < n)
-            Hs[lane * ldh + j] *= r;
-        if (lane == j)
-            Hs[j * ldh + j] = ljj;
-        __syncwarp();
-        int start = (j + 1) * n - ((j + 1) * j) / 2;   // first pair of column j+1
-        int total = n * (n + 1) / 2;
-        for (int p = start + lane; p < total; p += 32) {
-            unsigned short pr = pairsCol[p];
-            int i = pr >> 8, k = pr & 255;
-            Hs[i * ldh + k] -= Hs[i * ldh + j] * Hs[k * ldh + j];
+#pragma unroll
+    for (int j = 0; j < kMaxN; j++) {
+        if (j < n) {
+            double s0 = h[j], s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < j; k++) {
+                double ljk = __shfl_sync(0xffffffffu, h[k], j);
+                if (k & 1)
+                    s1 = fma(-h[k], ljk, s1);
+                else
+                    s0 = fma(-h[k], ljk, s0);
+            }
+            double s = s0 + s1;
+            double djj = __shfl_sync(0xffffffffu, s, j);
+            if (!(djj > 0.0))
+                return j + 1;
+            double ljj = sqrt(djj);
+            double r = 1.0 / ljj;
+            if (lane == j)
+                h[j] = ljj;
+            else if (lane > j)
+                h[j] = s * r;
         }
-        __syncwarp();
     }
     return 0;
 }
 
-// In-place inverse of the lower triangular factor (rows processed in order,
-// lanes over columns).
-__device__ void invert_lower_warp(double *Hs, int n, int ldh, int lane)
+// Column `lane` of L^-1 into v[] from the factor rows in h[] (lane i holds
+// row i): Linv_ic = -(sum_{k=c}^{i-1} L_ik Linv_kc) / L_ii, rows in order.
+__device__ __forceinline__ void invert_regs(const double (&h)[kMaxN], double (&v)[kMaxN], int n, int lane)
 {
-    for (int i = 0; i < n; i++) {
-        double acc0 = 0.0, acc1 = 0.0;
-        if (lane < i) {
-            int k = lane;
-            for (; k + 1 < i; k += 2) {
-                acc0 = fma(Hs[i * ldh + k], Hs[k * ldh + lane], acc0);
-                acc1 = fma(Hs[i * ldh + k + 1], Hs[(k + 1) * ldh + lane], acc1);
+#pragma unroll
+    for (int i = 0; i < kMaxN; i++) {
+        v[i] = 0.0;
+        if (i < n) {
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < i; k++) {
+                double lik = __shfl_sync(0xffffffffu, h[k], i);
+                if (k & 1)
+                    a1 = fma(lik, v[k], a1);
+                else
+                    a0 = fma(lik, v[k], a0);
             }
-            if (k < i)
-                acc0 = fma(Hs[i * ldh + k], Hs[k * ldh + lane], acc0);
+            double lii = __shfl_sync(0xffffffffu, h[i], i);
+            double rinv = 1.0 / lii;
+            if (lane == i)
+                v[i] = rinv;
+            else if (lane < i)
+                v[i] = -(a0 + a1) * rinv;
         }
-        double dinv = 1.0 / Hs[i * ldh + i];
-        __syncwarp();
-        if (lane < i)
-            Hs[i * ldh + lane] = -dinv * (acc0 + acc1);
-        if (lane == i)
-            Hs[i * ldh + i] = dinv;
-        __syncwarp();
     }
 }
 
@@ -436,25 +440,64 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         si[SI_ITER] = iter;
         si[SI_TOTAL] += 1;
     }
+    // row `lane` of H in registers; utils_norm1 = max absolute row sum
+    double h[kMaxN], v[kMaxN];
     double rowsum = 0.0;
-    if (act)
-        for (int j = 0; j < n; j++)
-            rowsum += fabs(Hs[lane * ldh + j]);
-    const double anorm = warp_max(rowsum);          // utils_norm1
-    __syncwarp();
-    int info = chol_warp(Hs, n, ldh, pb.pairs + npairs, lane);
+#pragma unroll
+    for (int k = 0; k < kMaxN; k++) {
+        h[k] = (act && k < n) ? Hs[lane * ldh + k] : 0.0;
+        rowsum += fabs(h[k]);
+    }
+    const double anorm = warp_max(rowsum);
+    int info = chol_regs(h, n, lane);
     double condest = 0.0;
     if (info == 0) {
-        invert_lower_warp(Hs, n, ldh, lane);
-        double rc = rcond_warp(Hs, n, ldh, vec, anorm, lane);
-        condest = 1.0 / rc;
+        // column `lane` of L^-1 in v[], rows of L^-1 in Hs
+        invert_regs(h, v, n, lane);
+        __syncwarp();
+        double colsum = 0.0;
+#pragma unroll
+        for (int i = 0; i < kMaxN; i++) {
+            if (i < n && act)
+                Hs[i * ldh + lane] = v[i];
+            colsum += fabs(v[i]);
+        }
+        __syncwarp();
+        double rs = 0.0;
+        if (act)
+            for (int c = 0; c <= lane; c++)
+                rs += fabs(Hs[lane * ldh + c]);
+        // ||A^-1||_1 <= ||L^-1||_1 ||L^-1||_inf, and the Higham estimate never
+        // exceeds ||A^-1||_1: when the bound already shows cond <= COND_H_MAX
+        // (with a factor-2 margin for rounding) the estimate cannot trigger
+        // regularisation and is not needed.
+        const double bound = anorm * warp_max(colsum) * warp_max(rs);
+        if (!(bound <= 0.5 * a.condHMax)) {
+            double rc = rcond_warp(Hs, n, ldh, vec, anorm, lane);
+            condest = 1.0 / rc;
+        }
     }
     if (iter >= si[SI_MAXITER] || info != 0 || sc[SC_T] == 0.0 || condest > a.condHMax) {
         __syncwarp();
         regularize(a, pb, L, s, lane, ldv, ui, ai);
         return;
     }
-    const double di = -apply_inv(Hs, n, ldh, vec, gi, lane);
+    // d = -L^-T (L^-1 g): rows of L^-1 from Hs, columns from registers
+    __syncwarp();
+    vec[lane] = gi;
+    __syncwarp();
+    double y = 0.0;
+    if (act)
+        for (int c = 0; c <= lane; c++)
+            y = fma(Hs[lane * ldh + c], vec[c], y);
+    double z = 0.0;
+#pragma unroll
+    for (int i = 0; i < kMaxN; i++) {
+        double yi = __shfl_sync(0xffffffffu, y, i);
+        if (i < n)
+            z = fma(v[i], yi, z);
+    }
+    const double di = act ? -z : 0.0;
     const double err = sqrt(warp_sum(gi * gi));
     bool gammaOk = true;
     if (a.tolGamma > 0.0)

@@ -164,7 +164,10 @@ def test_regularization_ladder_within_envelope():
     reg_fo = (f[3] != o[3]).sum()
     assert reg_go <= 3 * reg_fo + 5
     m = _agree(g, o) & _agree(f, o) & (o[4] == 0)
-    assert _du(g, o, m) <= max(1e-9, 5.0 * _du(f, o, m))
+    # Regularised solves are ill conditioned: both results still satisfy the
+    # stopping test ||g|| <= tol ||u|| on the same regularised target, so they
+    # can differ by up to 2 tol relative whatever the rounding.
+    assert _du(g, o, m) <= max(2 * 1e-8, 5.0 * _du(f, o, m))
 
 
 GOLDEN = [(ic, t) for ic in ["delta", "gaussian", "lattice", "smooth"] for t in ["mn", "ppn"]]
