@@ -44,6 +44,10 @@ struct DeviceBasis {
     int *hoff = nullptr, *hidx = nullptr;
     double *hval = nullptr;
     unsigned short *pairs = nullptr;
+    unsigned short *ellPair = nullptr, *ellIdx = nullptr;
+    double *ellVal = nullptr;
+    int *ellOff = nullptr;
+    int ellChunks = 0, ellRows = 0;
 
     void release()
     {
@@ -58,6 +62,10 @@ struct DeviceBasis {
         cudaFree(hidx);
         cudaFree(hval);
         cudaFree(pairs);
+        cudaFree(ellPair);
+        cudaFree(ellIdx);
+        cudaFree(ellVal);
+        cudaFree(ellOff);
         *this = DeviceBasis();
     }
 };
@@ -139,6 +147,22 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         if ((e = upload(&B.hoff, off)) != cudaSuccess) return e;
         if ((e = upload(&B.hidx, idx)) != cudaSuccess) return e;
         if ((e = upload(&B.hval, val)) != cudaSuccess) return e;
+        const int chunks = gaunt_ell_chunks(n), maxRows = 32 * chunks * 64;
+        std::vector<unsigned short> epair(chunks * 32), eidx((size_t)maxRows * 32);
+        std::vector<double> eval((size_t)maxRows * 32);
+        std::vector<int> eoff(chunks + 1);
+        int rows = build_gaunt_ell(n, goff, gidx, gval, epair.data(), eidx.data(), eval.data(), eoff.data(),
+                                   maxRows);
+        if (rows < 0)
+            return cudaErrorInvalidValue;
+        eidx.resize((size_t)rows * 32);
+        eval.resize((size_t)rows * 32);
+        B.ellChunks = chunks;
+        B.ellRows = rows;
+        if ((e = upload(&B.ellPair, epair)) != cudaSuccess) return e;
+        if ((e = upload(&B.ellIdx, eidx)) != cudaSuccess) return e;
+        if ((e = upload(&B.ellVal, eval)) != cudaSuccess) return e;
+        if ((e = upload(&B.ellOff, eoff)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -153,6 +177,12 @@ NewtonProblem make_problem(const DeviceBasis &B)
     pb.hidx = B.hidx;
     pb.hval = B.hval;
     pb.pairs = B.pairs;
+    pb.ellPair = B.ellPair;
+    pb.ellIdx = B.ellIdx;
+    pb.ellVal = B.ellVal;
+    pb.ellOff = B.ellOff;
+    pb.ellChunks = B.ellChunks;
+    pb.ellRows = B.ellRows;
     pb.p0 = B.p0;
     pb.n = B.n;
     pb.nb = B.nb;

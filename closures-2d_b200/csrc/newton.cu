@@ -54,9 +54,10 @@ __device__ __forceinline__ void record_error(int *err, int code, int idx)
 // Cholesky of the symmetric matrix whose row `lane` is h[] (registers), in
 // the dot-product (Crout) form by columns: lane i >= j forms
 // L_ij = (H_ij - sum_k<j L_ik L_jk) / L_jj with row j of L broadcast from
-// lane j.  On return h[k] = L_lane,k for k <= lane.  LAPACK-style info: 0, or
-// j+1 at the first non-positive or NaN pivot (dpotrf semantics).
-__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], int n, int lane)
+// lane j.  On return h[k] = L_lane,k for k <= lane and rdiag = 1/L_lane,lane.
+// LAPACK-style info: 0, or j+1 at the first non-positive or NaN pivot
+// (dpotrf semantics).
+__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], double &rdiag, int n, int lane)
 {
 #pragma unroll
     for (int j = 0; j < kMaxN; j++) {
@@ -74,12 +75,13 @@ __device__ __forceinline__ int chol_regs(double (&h)[kMaxN], int n, int lane)
             double djj = __shfl_sync(0xffffffffu, s, j);
             if (!(djj > 0.0))
                 return j + 1;
-            double ljj = sqrt(djj);
-            double r = 1.0 / ljj;
-            if (lane == j)
-                h[j] = ljj;
-            else if (lane > j)
+            double r = rsqrt(djj);
+            if (lane == j) {
+                h[j] = djj * r;
+                rdiag = r;
+            } else if (lane > j) {
                 h[j] = s * r;
+            }
         }
     }
     return 0;
@@ -87,7 +89,8 @@ __device__ __forceinline__ int chol_regs(double (&h)[kMaxN], int n, int lane)
 
 // Column `lane` of L^-1 into v[] from the factor rows in h[] (lane i holds
 // row i): Linv_ic = -(sum_{k=c}^{i-1} L_ik Linv_kc) / L_ii, rows in order.
-__device__ __forceinline__ void invert_regs(const double (&h)[kMaxN], double (&v)[kMaxN], int n, int lane)
+__device__ __forceinline__ void invert_regs(const double (&h)[kMaxN], double rdiag, double (&v)[kMaxN], int n,
+                                            int lane)
 {
 #pragma unroll
     for (int i = 0; i < kMaxN; i++) {
@@ -102,8 +105,7 @@ __device__ __forceinline__ void invert_regs(const double (&h)[kMaxN], double (&v
                 else
                     a0 = fma(lik, v[k], a0);
             }
-            double lii = __shfl_sync(0xffffffffu, h[i], i);
-            double rinv = 1.0 / lii;
+            double rinv = __shfl_sync(0xffffffffu, rdiag, i);
             if (lane == i)
                 v[i] = rinv;
             else if (lane < i)
@@ -187,6 +189,9 @@ struct Layout {
     double *alpha, *aold, *d, *u, *scal, *fpart, *P, *E, *Eg, *G, *H, *vec;
     int *ints;
     unsigned long long *stat;
+    double *ellVal;
+    unsigned short *ellIdx, *ellPair;
+    int *ellOff;
 };
 
 __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
@@ -206,6 +211,10 @@ __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
     L.G = sm + a.offG;
     L.H = sm + a.offH;
     L.vec = sm + a.offVec;
+    L.ellVal = sm + a.offEllVal;
+    L.ellIdx = (unsigned short *)(sm + a.offEllIdx);
+    L.ellPair = (unsigned short *)(sm + a.offEllPair);
+    L.ellOff = (int *)(sm + a.offEllOff);
     return L;
 }
 
@@ -372,20 +381,26 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     const int npairs = n * (n + 1) / 2;
 
     // H from the contraction results (fobj.cpp:129-155)
-    for (int pi = lane; pi < npairs; pi += 32) {
-        unsigned short pr = pb.pairs[pi];
-        int i = pr >> 8, j = pr & 255;
-        double v;
-        if (a.useGaunt) {
-            int row = j * n + i;
-            v = 0.0;
-            for (int e = __ldg(&pb.hoff[row]); e < __ldg(&pb.hoff[row + 1]); e++)
-                v += __ldg(&pb.hval[e]) * Gs[__ldg(&pb.hidx[e])];
-        } else {
-            v = Gs[pi];
+    if (a.useGaunt) {
+        for (int c = 0; c < pb.ellChunks; c++) {
+            unsigned short pr = L.ellPair[c * 32 + lane];
+            double v = 0.0;
+            for (int e = L.ellOff[c]; e < L.ellOff[c + 1]; e++)
+                v += L.ellVal[e * 32 + lane] * Gs[L.ellIdx[e * 32 + lane]];
+            if (pr != 0xFFFF) {
+                int i = pr >> 8, j = pr & 255;
+                Hs[i * ldh + j] = v;
+                Hs[j * ldh + i] = v;
+            }
         }
-        Hs[i * ldh + j] = v;
-        Hs[j * ldh + i] = v;
+    } else {
+        for (int pi = lane; pi < npairs; pi += 32) {
+            unsigned short pr = pb.pairs[pi];
+            int i = pr >> 8, j = pr & 255;
+            double v = Gs[pi];
+            Hs[i * ldh + j] = v;
+            Hs[j * ldh + i] = v;
+        }
     }
     __syncwarp();
 
@@ -449,11 +464,12 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         rowsum += fabs(h[k]);
     }
     const double anorm = warp_max(rowsum);
-    int info = chol_regs(h, n, lane);
+    double rdiag = 1.0;
+    int info = chol_regs(h, rdiag, n, lane);
     double condest = 0.0;
     if (info == 0) {
         // column `lane` of L^-1 in v[], rows of L^-1 in Hs
-        invert_regs(h, v, n, lane);
+        invert_regs(h, rdiag, v, n, lane);
         __syncwarp();
         double colsum = 0.0;
 #pragma unroll
@@ -575,6 +591,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         ctl[2] = 0;
     }
     __syncthreads();
+    int loadedProb = -1;
 
     for (;;) {
         // ---- refill idle slots from the work counter of the current problem
@@ -625,6 +642,20 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         if (ctl[1])
             break;
         const NewtonProblem &pb = a.prob[ctl[0]];
+        if (ctl[0] != loadedProb) {
+            // stage this order's Gaunt contraction table in shared memory
+            loadedProb = ctl[0];
+            if (a.useGaunt) {
+                for (int i = tid; i < pb.ellRows * 32; i += kThreads) {
+                    L.ellVal[i] = pb.ellVal[i];
+                    L.ellIdx[i] = pb.ellIdx[i];
+                }
+                for (int i = tid; i < pb.ellChunks * 32; i += kThreads)
+                    L.ellPair[i] = pb.ellPair[i];
+                for (int i = tid; i <= pb.ellChunks; i += kThreads)
+                    L.ellOff[i] = pb.ellOff[i];
+            }
+        }
         for (int s = warp; s < T; s += kWarps)
             if (L.ints[s * SI_N + SI_STATE] == S_NEW)
                 init_slot(a, pb, L, s, lane, ldv);
@@ -780,9 +811,11 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
 int plan_newton(NewtonArgs &a)
 {
-    int nbMax = 8, ldPMax = 0, K2tot = 0, nMax = 1;
+    int nbMax = 8, ldPMax = 0, K2tot = 0, nMax = 1, ellRows = 0, ellChunks = 0;
     for (int p = 0; p < a.nprob; p++) {
         const NewtonProblem &pb = a.prob[p];
+        ellRows = pb.ellRows > ellRows ? pb.ellRows : ellRows;
+        ellChunks = pb.ellChunks > ellChunks ? pb.ellChunks : ellChunks;
         nbMax = pb.nb > nbMax ? pb.nb : nbMax;
         ldPMax = pb.ldP > ldPMax ? pb.ldP : ldPMax;
         int kt = pb.K2p + (a.momentType == 1 ? pb.nb : 0);
@@ -811,6 +844,10 @@ int plan_newton(NewtonArgs &a)
     a.offInt = take((T * SI_N + 1) / 2);
     a.offFpart = take(T * a.ntq);
     a.offStat = take(kStatU64 + 1);
+    a.offEllVal = take(ellRows * 32);
+    a.offEllIdx = take((ellRows * 32 + 3) / 4);
+    a.offEllPair = take((ellChunks * 32 + 3) / 4);
+    a.offEllOff = take((ellChunks + 2) / 2);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
     a.tpw = (ntiles2 + kWarps - 1) / kWarps;

@@ -18,6 +18,12 @@ struct NewtonProblem {
     const int *hidx;
     const double *hval;
     const unsigned short *pairs;  // n(n+1)/2 entries (i << 8) | j, j <= i, column order
+    // Gaunt contraction in lane-major chunks (build_gaunt_ell), staged in
+    // shared memory when the CTA starts on this problem
+    const unsigned short *ellPair, *ellIdx;
+    const double *ellVal;
+    const int *ellOff;
+    int ellChunks, ellRows;
     double p0;                  // p[0] = Y_00 (fobj.cpp:305 divides by it)
     int n, nb, K2p, nqp, ldP;
     int count;                  // vectors to solve
@@ -43,6 +49,7 @@ struct NewtonArgs {
     int T, kq, ldv, ldE, ldG, ldh, ntq, doubleBuffer;
     int offAlpha, offAold, offD, offU, offScal, offInt, offFpart, offStat;
     int offP, offE, offEg, offG, offH, offVec;
+    int offEllVal, offEllIdx, offEllPair, offEllOff;
     int smemBytes;
     int tpw;
 };

@@ -14,8 +14,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 
+#include "../host/angular.h"
 #include "common.cuh"
 #include "newton.cuh"
 
@@ -88,6 +90,22 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     off = align_up(off + sizeof(int) * (size_t)(nnz ? nnz : 1), 256);
     const size_t offHval = off;
     off = align_up(off + sizeof(double) * (size_t)(nnz ? nnz : 1), 256);
+    // Gaunt table in lane-major chunks; rows bounded by the pair count times
+    // the longest entry list, which the CSR gives
+    const int chunks = gaunt ? gaunt_ell_chunks(n) : 0;
+    int maxPer = 0;
+    if (gaunt)
+        for (int r = 0; r < n * n; r++)
+            maxPer = std::max(maxPer, ang->gaunt_off[r + 1] - ang->gaunt_off[r]);
+    const int maxRows = chunks * maxPer;
+    const size_t offEllPair = off;
+    off = align_up(off + sizeof(unsigned short) * (size_t)(chunks * 32 + 1), 256);
+    const size_t offEllOff = off;
+    off = align_up(off + sizeof(int) * (size_t)(chunks + 1), 256);
+    const size_t offEllIdx = off;
+    off = align_up(off + sizeof(unsigned short) * (size_t)(maxRows * 32 + 1), 256);
+    const size_t offEllVal = off;
+    off = align_up(off + sizeof(double) * (size_t)(maxRows * 32 + 1), 256);
     if (off > kNoAllocBytes) {
         char buf[200];
         std::snprintf(buf, sizeof(buf),
@@ -139,12 +157,18 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     for (int k = 0; k < n; k++)
         for (int i = k; i < n; i++)
             pairs[c++] = (unsigned short)((i << 8) | k);
+    int ellRows = 0;
     if (gaunt) {
         std::memcpy(g_stage + offHoff, ang->gaunt_off, sizeof(int) * (n * n + 1));
         if (nnz) {
             std::memcpy(g_stage + offHidx, ang->gaunt_idx, sizeof(int) * nnz);
             std::memcpy(g_stage + offHval, ang->gaunt_val, sizeof(double) * nnz);
         }
+        ellRows = build_gaunt_ell(n, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
+                                  (unsigned short *)(g_stage + offEllPair), (unsigned short *)(g_stage + offEllIdx),
+                                  (double *)(g_stage + offEllVal), (int *)(g_stage + offEllOff), maxRows);
+        if (ellRows < 0)
+            return fail(CL_ERR_ARG, "Gaunt table layout failed");
     }
     // the header (work counter, error word, statistics) starts at zero each call
     cudaError_t e = cudaMemcpyAsync(base, g_stage, off, cudaMemcpyHostToDevice, stream);
@@ -161,6 +185,12 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     pb.hoff = gaunt ? (const int *)(base + offHoff) : nullptr;
     pb.hidx = gaunt ? (const int *)(base + offHidx) : nullptr;
     pb.hval = gaunt ? (const double *)(base + offHval) : nullptr;
+    pb.ellPair = gaunt ? (const unsigned short *)(base + offEllPair) : nullptr;
+    pb.ellIdx = gaunt ? (const unsigned short *)(base + offEllIdx) : nullptr;
+    pb.ellVal = gaunt ? (const double *)(base + offEllVal) : nullptr;
+    pb.ellOff = gaunt ? (const int *)(base + offEllOff) : nullptr;
+    pb.ellChunks = chunks;
+    pb.ellRows = ellRows;
     pb.p0 = ang->p[0];
     pb.n = n;
     pb.nb = nb;

@@ -230,3 +230,63 @@ int build_angular(int order, int Q, int useGaunt, Angular &A)
 }
 
 }  // namespace clb
+
+namespace clb {
+
+int build_gaunt_ell(int n, const int *off, const int *idx, const double *val, unsigned short *pair,
+                    unsigned short *eidx, double *eval, int *eoff, int maxRows)
+{
+    const int np = n * (n + 1) / 2;
+    int pi[528], pj[528], pc[528];   // n <= 32
+    if (np > 528)
+        return -1;
+    int m = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            pi[m] = i;
+            pj[m] = j;
+            pc[m] = off[i * n + j + 1] - off[i * n + j];
+            m++;
+        }
+    // stable insertion sort by descending entry count
+    for (int a = 1; a < m; a++) {
+        int ti = pi[a], tj = pj[a], tc = pc[a], b = a - 1;
+        while (b >= 0 && pc[b] < tc) {
+            pi[b + 1] = pi[b];
+            pj[b + 1] = pj[b];
+            pc[b + 1] = pc[b];
+            b--;
+        }
+        pi[b + 1] = ti;
+        pj[b + 1] = tj;
+        pc[b + 1] = tc;
+    }
+    const int chunks = gaunt_ell_chunks(n);
+    int rows = 0;
+    for (int c = 0; c < chunks; c++) {
+        eoff[c] = rows;
+        int rc = 0;
+        for (int l = 0; l < 32; l++) {
+            int p = c * 32 + l;
+            if (p < m && pc[p] > rc)
+                rc = pc[p];
+        }
+        if (rows + rc > maxRows)
+            return -1;
+        for (int l = 0; l < 32; l++) {
+            int p = c * 32 + l;
+            pair[c * 32 + l] = (p < m) ? (unsigned short)((pi[p] << 8) | pj[p]) : (unsigned short)0xFFFF;
+            int r0 = (p < m) ? off[pi[p] * n + pj[p]] : 0;
+            for (int e = 0; e < rc; e++) {
+                bool live = p < m && e < pc[p];
+                eidx[(size_t)(rows + e) * 32 + l] = live ? (unsigned short)idx[r0 + e] : (unsigned short)0;
+                eval[(size_t)(rows + e) * 32 + l] = live ? val[r0 + e] : 0.0;
+            }
+        }
+        rows += rc;
+    }
+    eoff[chunks] = rows;
+    return rows;
+}
+
+}  // namespace clb

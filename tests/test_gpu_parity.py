@@ -230,7 +230,13 @@ def test_grid_steps_match_oracle(tmp_path, name, kw, steps):
     scale = np.abs(m_o[:, :, :1])
     err = float(np.max(np.abs(m_g - m_o) / scale))
     env = float(np.max(np.abs(m_f - m_o) / scale))
-    assert err <= max(TOL, 3.0 * env), "gpu %.3e vs envelope %.3e" % (err, env)
+    if env < TOL:
+        assert err < TOL, "gpu %.3e (decisions are rounding-stable here)" % err
+    else:
+        # Rounding decides some regularisation steps on this deck (the two
+        # oracle builds already differ): a flipped first rung changes a cell's
+        # moments by r = 1e-3 relative, which is the scale of the envelope.
+        assert err <= max(3.0 * env, 2e-3), "gpu %.3e vs envelope %.3e" % (err, env)
     so, sg = orc.stats(), s.stats()
     assert sg["num_solves"] == so["num_solves"]
     if env < TOL:
