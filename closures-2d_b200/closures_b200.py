@@ -100,6 +100,7 @@ def lib():
             "cl_launch_count": (C.c_int64, []),
             "cl_selftest": (C.c_int, []),
             "cl_fp64_peak": (C.c_int, [C.POINTER(C.c_double)]),
+            "cl_exp_check": (C.c_int, [dp, C.c_int, dp, dp]),
             "cl_solver_create": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(vp), dp]),
             "cl_solver_geometry": (C.c_int, [vp, ip, ip, ip, dp, dp, dp, dp]),
             "cl_solver_update": (C.c_int, [vp, C.c_double]),
@@ -144,6 +145,14 @@ def launch_count():
 
 def selftest():
     _check(lib().cl_selftest(), lib().cl_global_error)
+
+
+def exp_check(x):
+    """(table-driven exp, CUDA exp) of the points x, both evaluated on the device."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    fast, ref = np.empty_like(x), np.empty_like(x)
+    _check(lib().cl_exp_check(_dp(x), x.size, _dp(fast), _dp(ref)), lib().cl_global_error)
+    return fast, ref
 
 
 def fp64_peak_tflops():

@@ -1058,3 +1058,43 @@ extern "C" int cl_fp64_peak(double *tflops)
     *tflops = flops / (best * 1e-3) / 1e12;
     return CL_OK;
 }
+
+// ---------------------------------------------------------- exp accuracy
+namespace {
+__global__ void exp_check_kernel(const double *x, int n, double *fast, double *ref, ExpConsts ex)
+{
+    __shared__ double tab[64];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x)
+        tab[i] = ex.tab[i];
+    __syncthreads();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        fast[i] = fast_exp(x[i], tab, ex.invL, ex.L1, ex.L2);
+        ref[i] = exp(x[i]);
+    }
+}
+}  // namespace
+
+extern "C" int cl_exp_check(const double *x, int n, double *fast, double *ref)
+{
+    if (!x || !fast || !ref || n <= 0)
+        return CL_ERR_ARG;
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 3 * (size_t)n) != cudaSuccess) {
+        g_global_err = "exp check allocation failed";
+        return CL_ERR_CUDA;
+    }
+    ExpConsts ex;
+    exp_consts_init(ex);
+    cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    exp_check_kernel<<<(n + 255) / 256, 256>>>(d, n, d + n, d + 2 * (size_t)n, ex);
+    g_launches += 1;
+    cudaMemcpy(fast, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(ref, d + 2 * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        g_global_err = std::string("exp check: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return CL_OK;
+}

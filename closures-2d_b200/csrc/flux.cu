@@ -20,10 +20,13 @@ namespace clb {
 
 namespace {
 
-constexpr int TX = 8, TY = 16;             // interior tile (x slow, y fast)
+constexpr int TX = 16, TY = 16;            // interior tile (x slow, y fast)
 constexpr int HX = TX + 4, HY = TY + 4;    // with the 2-cell halo
-constexpr int HC = HX * HY;                // 240 halo cells (15 m16 tiles)
-constexpr int IC = TX * TY;                // 128 interior cells
+constexpr int HC = HX * HY;                // 400 halo cells (25 m16 tiles)
+constexpr int IC = TX * TY;                // 256 interior cells (16 m16 tiles)
+constexpr int kFluxThreads = 512;          // 16 warps: one interior m-tile each
+constexpr int kFluxWarps = kFluxThreads / 32;
+constexpr int kQ = 16;                     // directions per chunk
 constexpr double kSqrtPi = 1.7724538509055160273;
 
 __device__ __forceinline__ double minmod(double x, double y)
@@ -42,23 +45,27 @@ __device__ __forceinline__ double slopefit(double l, double c, double r, double 
     return minmod(th * (r - c), minmod(0.5 * (r - l), th * (c - l)));
 }
 
-__global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant__ FluxArgs f)
+__global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_constant__ FluxArgs f)
 {
     extern __shared__ __align__(16) double sm[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
     const int bx = blockIdx.x / f.tilesY, by = blockIdx.x % f.tilesY;
     const int i0 = 2 + bx * TX, j0 = 2 + by * TY;     // first interior cell of the tile
-    const int n = f.n, nb = f.nb, kq = f.kq, ldPf = f.ldPf;
+    const int n = f.n, nb = f.nb, ldPf = f.ldPf;
+    constexpr int kq = kQ;
     const int ldAl = f.ldAl, ldA = f.ldA, ldF = f.ldF;
     double *sAl = sm + f.offAl;     // [HC][ldAl]
     double *sA = sm + f.offA;       // [kq][ldA] ansatz, q-major
     double *sF = sm + f.offF;       // [kq][ldF] stencil flux, q-major
     double *sP = sm + f.offP;       // [2][kq][ldPf]
     double *sQ = sm + f.offQ;       // [2][4][kq] xi, eta, xi*w, eta*w
+    double *sExp = sm + f.offExp;   // fast_exp table
+    for (int i = tid; i < 64; i += kFluxThreads)
+        sExp[i] = f.ex.tab[i];
 
     // alpha of the halo region (zero outside the grid)
-    for (int idx = tid; idx < HC * nb; idx += kThreads) {
+    for (int idx = tid; idx < HC * nb; idx += kFluxThreads) {
         int h = idx / nb, k = idx % nb;
         int hi = h / HY, hj = h % HY;
         int i = i0 - 2 + hi, j = j0 - 2 + hj;
@@ -72,10 +79,10 @@ __global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant
     auto load_chunk = [&](int c, int buf) {
         const double *src = f.P + (size_t)c * kq * ldPf;
         double *dst = sP + buf * kq * ldPf;
-        for (int i = tid; i < kq * ldPf / 2; i += kThreads)
+        for (int i = tid; i < kq * ldPf / 2; i += kFluxThreads)
             cp_async16(dst + 2 * i, src + 2 * i);
         double *q = sQ + buf * 4 * kq;
-        for (int i = tid; i < kq / 2; i += kThreads) {
+        for (int i = tid; i < kq / 2; i += kFluxThreads) {
             cp_async16(q + 2 * i, f.xi + c * kq + 2 * i);
             cp_async16(q + kq + 2 * i, f.eta + c * kq + 2 * i);
             cp_async16(q + 2 * kq + 2 * i, f.cxw + c * kq + 2 * i);
@@ -84,7 +91,7 @@ __global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant
         cp_async_commit();
     };
 
-    // projection accumulators: warp owns interior rows warp*16.., all k tiles
+    // projection accumulators: warp owns interior m-tile `warp` (16 cells), all k tiles
     double acc[4][4];
 #pragma unroll
     for (int j = 0; j < 4; j++)
@@ -105,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant
         const double *Pb = sP + buf * kq * ldPf;
         const double *Qb = sQ + buf * 4 * kq;
         // 1. ansatz on the halo tile
-        for (int ti = warp; ti < ntiles1; ti += kWarps) {
+        for (int ti = warp; ti < ntiles1; ti += kFluxWarps) {
             int mt = ti % (HC / 16), nt = ti / (HC / 16);
             double cs[4] = {0.0, 0.0, 0.0, 0.0};
             const double *A0 = sAl + (mt * 16 + g) * ldAl;
@@ -119,7 +126,7 @@ __global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant
                 double kin = cs[h];
                 double v;
                 if (f.momentType == 0) {
-                    v = exp(kin);
+                    v = fast_exp(kin, sExp, f.ex.invL, f.ex.L1, f.ex.L2);
                 } else {
                     double dl = f.deltaPPn;
                     if (kin > 0)
@@ -134,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, 1) flux_kernel(const __grid_constant
         }
         __syncthreads();
         // 2. limited upwind stencil, one q per warp-item (uniform branches)
-        for (int item = warp; item < kq * (IC / 32); item += kWarps) {
+        for (int item = warp; item < kq * (IC / 32); item += kFluxWarps) {
             int q = item / (IC / 32), cg = item % (IC / 32);
             int ic = cg * 32 + lane;
             int ti = ic / TY, tj = ic % TY;
@@ -249,7 +256,7 @@ __global__ void ghost_periodic_y_kernel(double *m, int n, int NX, int NY)
 
 int plan_flux(FluxArgs &f)
 {
-    f.kq = 32;
+    f.kq = kQ;
     f.ldAl = f.nb + 4;
     f.ldA = HC + 2;      // ldA % 8 == 2: conflict-free fragment stores
     f.ldF = IC + 4;      // ldF % 16 == 4
@@ -264,6 +271,8 @@ int plan_flux(FluxArgs &f)
     f.offF = take(f.kq * f.ldF);
     f.offP = take(2 * f.kq * f.ldPf);
     f.offQ = take(2 * 4 * f.kq);
+    f.offExp = take(64);
+    exp_consts_init(f.ex);
     f.smemBytes = off * 8;
     f.tilesX = (f.NX - 4 + TX - 1) / TX;
     f.tilesY = (f.NY - 4 + TY - 1) / TY;
@@ -277,7 +286,7 @@ cudaError_t prepare_flux(const FluxArgs &f)
 
 cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream)
 {
-    flux_kernel<<<f.tilesX * f.tilesY, kThreads, f.smemBytes, stream>>>(f);
+    flux_kernel<<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
     return cudaGetLastError();
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "fexp.cuh"
 
 namespace clb {
 
@@ -21,7 +22,8 @@ struct FluxArgs {
     double dt, dx, dy, initX, initY;
     // layout (doubles), filled by plan_flux()
     int kq, ldAl, ldA, ldF;
-    int offAl, offA, offF, offP, offQ;
+    int offAl, offA, offF, offP, offQ, offExp;
+    ExpConsts ex;
     int smemBytes;
     int tilesX, tilesY;
 };

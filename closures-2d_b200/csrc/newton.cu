@@ -192,6 +192,7 @@ struct Layout {
     double *ellVal;
     unsigned short *ellIdx, *ellPair;
     int *ellOff;
+    double *exptab;
 };
 
 __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
@@ -215,6 +216,7 @@ __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
     L.ellIdx = (unsigned short *)(sm + a.offEllIdx);
     L.ellPair = (unsigned short *)(sm + a.offEllPair);
     L.ellOff = (int *)(sm + a.offEllOff);
+    L.exptab = sm + a.offExp;
     return L;
 }
 
@@ -585,6 +587,10 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         L.ints[i] = (i % SI_N == SI_STATE) ? S_IDLE : 0;
     for (int i = tid; i <= kStatU64; i += kThreads)
         L.stat[i] = 0ull;
+    for (int i = tid; i < 64; i += kThreads)
+        L.exptab[i] = a.ex.tab[i];
+    for (int i = tid; i < T * SC_N; i += kThreads)
+        L.scal[i] = 0.0;
     if (tid == 0) {
         ctl[0] = 0;
         ctl[1] = 0;
@@ -713,8 +719,11 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                 const int qg = c * kq + ql;
                 const double w0 = __ldg(&pb.w[qg]), w1 = __ldg(&pb.w[qg + 1]);
                 if (a.momentType == 0) {
-                    double e0 = w0 * exp(cs[0]), e1 = w1 * exp(cs[1]);
-                    double e2 = w0 * exp(cs[2]), e3 = w1 * exp(cs[3]);
+                    const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
+                    double e0 = w0 * fast_exp(cs[0], L.exptab, invL, L1, L2);
+                    double e1 = w1 * fast_exp(cs[1], L.exptab, invL, L1, L2);
+                    double e2 = w0 * fast_exp(cs[2], L.exptab, invL, L1, L2);
+                    double e3 = w1 * fast_exp(cs[3], L.exptab, invL, L1, L2);
                     L.E[r0 * ldE + ql] = e0;
                     L.E[r0 * ldE + ql + 1] = e1;
                     L.E[r1 * ldE + ql] = e2;
@@ -848,6 +857,8 @@ int plan_newton(NewtonArgs &a)
     a.offEllIdx = take((ellRows * 32 + 3) / 4);
     a.offEllPair = take((ellChunks * 32 + 3) / 4);
     a.offEllOff = take((ellChunks + 2) / 2);
+    a.offExp = take(64);
+    exp_consts_init(a.ex);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
     a.tpw = (ntiles2 + kWarps - 1) / kWarps;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "fexp.cuh"
 
 namespace clb {
 
@@ -49,7 +50,8 @@ struct NewtonArgs {
     int T, kq, ldv, ldE, ldG, ldh, ntq, doubleBuffer;
     int offAlpha, offAold, offD, offU, offScal, offInt, offFpart, offStat;
     int offP, offE, offEg, offG, offH, offVec;
-    int offEllVal, offEllIdx, offEllPair, offEllOff;
+    int offEllVal, offEllIdx, offEllPair, offEllOff, offExp;
+    ExpConsts ex;               // table-driven exp constants (staged in shared memory)
     int smemBytes;
     int tpw;
 };

@@ -210,6 +210,9 @@ int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha);
 /* Measures the FP64 tensor-core (DMMA m16n8k8) throughput of the current
  * device in TFLOP/s: the roofline denominator of the FP64-bound kernels. */
 int cl_fp64_peak(double *tflops);
+/* Evaluates the kernels' table-driven exp and the CUDA library exp on the
+ * device for n host points (accuracy check of the former against the latter). */
+int cl_exp_check(const double *x, int n, double *fast, double *ref);
 /* Runs the library's DMMA fragment-layout self check on the device; returns
  * CL_OK when the FP64 tensor-core GEMM matches a host GEMM. */
 int cl_selftest(void);
