@@ -347,16 +347,136 @@ def native_arm(args, world, rank, local):
     return 0
 
 
+BATCH_ORDERS = [5, 4, 3, 2, 1]   # most expensive first (longest-processing-time order)
+
+
+def sample_batch_torch(angular, count, gen, device):
+    """Batched-optimisation workload on the device (FP64): alpha_k ~ N(0, s^2),
+    s log-uniform in [0.1, 20], alpha_0 such that u_0 = 1, u = <m e^{alpha.m}>."""
+    import torch
+    n = angular.n
+    P = torch.from_numpy(angular.p[:, :n].copy()).to(device)
+    w = torch.from_numpy(angular.w.copy()).to(device)
+    s = torch.exp(torch.empty(count, dtype=torch.float64, device=device).uniform_(
+        np.log(0.1), np.log(20.0), generator=gen))
+    alpha = torch.randn((count, n), dtype=torch.float64, device=device, generator=gen) * s[:, None]
+    alpha[:, 0] = 0.0
+    u = torch.empty((count, n), dtype=torch.float64, device=device)
+    p0 = float(angular.p[0, 0])
+    for b in range(0, count, 65536):
+        a = alpha[b:b + 65536]
+        e = a @ P.T
+        mx = e.max(dim=1, keepdim=True).values
+        ex = torch.exp(e - mx) * w[None, :]
+        mom = ex @ P
+        alpha[b:b + 65536, 0] = -(mx[:, 0] + torch.log(mom[:, 0])) / p0
+        u[b:b + 65536] = mom / mom[:, :1]
+    return u, alpha
+
+
+def batch_arm(args, world, rank, local):
+    """Batched opt() bench: 2^20 vectors of orders 1..5 at Q = 40 in one
+    persistent launch from the isotropic start, tolerance 1e-8."""
+    import torch
+    import closures_b200 as cb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    total = 1 << 20
+    Q, gaunt = 40, 1
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(12345 + rank)
+    rng = np.random.default_rng(12345 + rank)
+    counts = np.bincount(rng.integers(0, len(BATCH_ORDERS), total), minlength=len(BATCH_ORDERS))
+    counts = [int(c) for c in counts]
+    angs = [cb.Angular(o, Q, gaunt) for o in BATCH_ORDERS]
+    inputs = [sample_batch_torch(a, c, gen, dev) for a, c in zip(angs, counts)]
+    u0 = [u for u, _ in inputs]
+    a_iso = [torch.from_numpy(cb.isotropic_alpha(a.n, c)).to(dev) for a, c in zip(angs, counts)]
+    du = [u.clone() for u in u0]
+    da = [a.clone() for a in a_iso]
+    dit = [torch.zeros(c, dtype=torch.int32, device=dev) for c in counts]
+    dreg = [torch.zeros(c, dtype=torch.float64, device=dev) for c in counts]
+    dst = [torch.zeros(c, dtype=torch.int32, device=dev) for c in counts]
+    opts = cb.make_options(tol=1e-8)
+    m = cb.MultiSolver(BATCH_ORDERS, Q, gaunt, opts)
+
+    def one():
+        for k in range(len(counts)):
+            du[k].copy_(u0[k])
+            da[k].copy_(a_iso[k])
+        m.solve_device(counts, du, da, dit, dreg, dst)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    launches0 = cb.launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = cb.launch_count() - launches0
+    value = total * args.steps / (ms * 1e-3)
+    per = {}
+    for k, o in enumerate(BATCH_ORDERS):
+        it = dit[k].cpu().numpy()
+        per[str(o)] = {"count": counts[k], "iter_mean": float(it.mean()),
+                       "hist": np.bincount(np.minimum(it, 40), minlength=41).tolist(),
+                       "status_nonzero": int((dst[k] != 0).sum().item())}
+    # error against the FP64 oracle on a sample per order (CPU, all threads)
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        os.environ["OMP_NUM_THREADS"] = str(cpu_threads())
+        import pyoracle
+        pyoracle.build()
+        t_cpu, n_cpu = 0.0, 0
+        for k, o in enumerate(BATCH_ORDERS):
+            sl = slice(0, 2000)
+            uo = u0[k][sl].cpu().numpy().copy()
+            ao = a_iso[k][sl].cpu().numpy().copy()
+            t0 = time.perf_counter()
+            it_o, _, st_o = pyoracle.opt_batch(o, Q, gaunt, uo, ao, tol=1e-8)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += uo.shape[0]
+            ug = du[k][sl].cpu().numpy()
+            err = np.abs(ug - uo) / np.abs(uo[:, :1])
+            per[str(o)]["oracle_max_rel_err"] = float(err.max())
+            per[str(o)]["oracle_iter_agree"] = float((it_o == dit[k][sl].cpu().numpy()).mean())
+        cpu = {"value": n_cpu / t_cpu, "unit": "cell-solves/s", "cores": cpu_threads(), "kind": "port",
+               "sample": "first 2000 vectors of each order, opt() from the isotropic start"}
+    else:
+        cpu = None
+    line = {"metric": METRIC, "value": value * world, "unit": "cell-solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "batch_2e20", "vectors": total,
+                                             "orders": BATCH_ORDERS, "quad_order": Q,
+                                             "use_gaunt": gaunt, "tol": 1e-8, "start": "isotropic"},
+            "per_order": per, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    m.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--workload", default="m6_800", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="m6_800", choices=sorted(WORKLOADS) + ["batch_2e20"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.workload == "batch_2e20":
+        return batch_arm(args, world, rank, local)
     if args.impl == "reference":
         return reference_arm(args, world, rank)
     return native_arm(args, world, rank, local)

@@ -247,3 +247,39 @@ def test_grid_steps_match_oracle(tmp_path, name, kw, steps):
         it_g, it_o = s.last_iterations(), orc.last_iterations()
         assert (it_g != it_o).mean() <= 0.01
         assert abs(sg["iter_mean"] - so["iter_mean"]) <= 0.02 * so["iter_mean"]
+
+
+def test_multi_order_launch_matches_oracle():
+    """Vectors of five moment orders share one persistent launch (cl_multi_*)."""
+    import torch
+
+    orders, Q, gaunt = [5, 4, 3, 2, 1], 20, 1
+    counts = [120, 200, 150, 300, 64]
+    opts = cb.make_options(tol=1e-8)
+    m = cb.MultiSolver(orders, Q, gaunt, opts)
+    dev = torch.device("cuda", 0)
+    host, dev_u, dev_a, dev_it, dev_reg, dev_st = [], [], [], [], [], []
+    for order, count in zip(orders, counts):
+        a = cb.Angular(order, Q, gaunt)
+        u, _ = cb.sample_moment_vectors(a, count, seed=100 + order, s_range=(0.1, 2.0))
+        a0 = cb.isotropic_alpha(a.n, count)
+        host.append((u, a0))
+        dev_u.append(torch.from_numpy(u.copy()).to(dev))
+        dev_a.append(torch.from_numpy(a0.copy()).to(dev))
+        dev_it.append(torch.zeros(count, dtype=torch.int32, device=dev))
+        dev_reg.append(torch.zeros(count, dtype=torch.float64, device=dev))
+        dev_st.append(torch.full((count,), 9, dtype=torch.int32, device=dev))
+    m.solve_device(counts, dev_u, dev_a, dev_it, dev_reg, dev_st)
+    torch.cuda.synchronize()
+    for k, (order, count) in enumerate(zip(orders, counts)):
+        u, a0 = host[k]
+        uo, ao = u.copy(), a0.copy()
+        it_o, reg_o, st_o = oracle_lib.opt_batch(order, Q, gaunt, uo, ao, tol=1e-8)
+        ug = dev_u[k].cpu().numpy()
+        it_g = dev_it[k].cpu().numpy()
+        st_g = dev_st[k].cpu().numpy()
+        assert (st_g == 0).all() and (st_o == 0).all()
+        agree = it_g == it_o
+        assert agree.mean() >= 0.98
+        assert np.max(np.abs(ug - uo)[agree] / np.abs(uo[agree, :1])) < TOL
+    m.close()
