@@ -56,7 +56,7 @@ class cl_grid(C.Structure):
 class cl_stats(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
                 ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64),
-                ("total_trials", C.c_int64)]
+                ("total_trials", C.c_int64), ("fallbacks", C.c_int64)]
 
 
 _lib = None
@@ -90,6 +90,7 @@ def lib():
             "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
+            "cl_solve_batch_device_start": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp]),
             "cl_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
             "cl_multi_create": (C.c_int, [C.c_int, ip, C.c_int, C.c_int, C.POINTER(cl_options),
                                           C.POINTER(vp)]),
@@ -97,6 +98,9 @@ def lib():
             "cl_multi_last_error": (C.c_char_p, [vp]),
             "cl_multi_solve_device": (C.c_int, [vp, ip, C.POINTER(vp), C.POINTER(vp),
                                                 C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+            "cl_multi_solve_device_start": (C.c_int, [vp, ip, C.POINTER(vp), C.POINTER(vp),
+                                                      C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                                      C.POINTER(vp)]),
             "cl_launch_count": (C.c_int64, []),
             "cl_selftest": (C.c_int, []),
             "cl_fp64_peak": (C.c_int, [C.POINTER(C.c_double)]),
@@ -109,6 +113,22 @@ def lib():
             "cl_solver_last_error": (C.c_char_p, [vp]),
             "cl_solver_destroy": (None, [vp]),
             "cl_run_deck": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
+            "cl_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong,
+                                        C.POINTER(vp)]),
+            "cl_mlp_destroy": (None, [vp]),
+            "cl_mlp_last_error": (C.c_char_p, [vp]),
+            "cl_mlp_set_output_scaling": (C.c_int, [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+            "cl_mlp_train": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       C.c_ulonglong, C.POINTER(C.c_float)]),
+            "cl_mlp_predict": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, ip, vp]),
+            "cl_mlp_loss_and_grads": (C.c_int, [vp, dp, dp, C.c_int, C.POINTER(C.c_float),
+                                                C.POINTER(C.POINTER(C.c_float)),
+                                                C.POINTER(C.POINTER(C.c_float))]),
+            "cl_mlp_get_params": (C.c_int, [vp, C.POINTER(C.POINTER(C.c_float)),
+                                            C.POINTER(C.POINTER(C.c_float))]),
+            "cl_mlp_set_params": (C.c_int, [vp, C.POINTER(C.POINTER(C.c_float)),
+                                            C.POINTER(C.POINTER(C.c_float))]),
+            "cl_set_warm_start": (C.c_int, [vp, vp]),
             "cl_solve_batch_noalloc": (C.c_int, [C.POINTER(cl_angular), C.POINTER(cl_options),
                                                  C.c_int, vp, vp, vp, vp, vp, vp]),
             "cl_noalloc_last_error": (C.c_char_p, []),
@@ -269,7 +289,7 @@ class Context:
         _check(lib().cl_get_stats(self._ctx, C.byref(s)), self._err)
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
-                "total_trials": s.total_trials}
+                "total_trials": s.total_trials, "fallbacks": s.fallbacks}
 
     def solve_batch(self, u, alpha, check=True):
         """opt() on every row of u/alpha (in place).  Returns iters, reg, status."""
@@ -285,11 +305,18 @@ class Context:
             _check(rc, self._err)
         return iters, reg, status
 
-    def solve_batch_device(self, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None, count=None):
-        """Device-pointer form (torch tensors or raw addresses)."""
+    def solve_batch_device(self, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None, count=None,
+                           d_alpha_start=None):
+        """Device-pointer form (torch tensors or raw addresses); with
+        d_alpha_start the solve starts there and d_alpha is the fallback start."""
         ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
-        _check(lib().cl_solve_batch_device(self._ctx, count, ptr(d_u), ptr(d_alpha), ptr(d_iters),
-                                           ptr(d_reg), ptr(d_status)), self._err)
+        _check(lib().cl_solve_batch_device_start(self._ctx, count, ptr(d_u), ptr(d_alpha),
+                                                 ptr(d_alpha_start), ptr(d_iters), ptr(d_reg),
+                                                 ptr(d_status)), self._err)
+
+    def set_warm_start(self, mlp):
+        """Predict alpha with `mlp` before every optimisation stage (None: off)."""
+        _check(lib().cl_set_warm_start(self._ctx, mlp._m if mlp is not None else None), self._err)
 
     def device_state(self):
         m, a = C.c_void_p(), C.c_void_p()
@@ -307,13 +334,15 @@ class MultiSolver:
         _check(lib().cl_multi_create(len(orders), arr, quad_order, int(use_gaunt),
                                      C.byref(options), C.byref(self._m)), lib().cl_global_error)
 
-    def solve_device(self, counts, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None):
+    def solve_device(self, counts, d_u, d_alpha, d_iters=None, d_reg=None, d_status=None,
+                     d_alpha_start=None):
         k = len(self.orders)
         ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
         arr = lambda ts: None if ts is None else (C.c_void_p * k)(*[ptr(t) for t in ts])
         cnt = (C.c_int * k)(*counts)
-        _check(lib().cl_multi_solve_device(self._m, cnt, arr(d_u), arr(d_alpha), arr(d_iters),
-                                           arr(d_reg), arr(d_status)),
+        _check(lib().cl_multi_solve_device_start(self._m, cnt, arr(d_u), arr(d_alpha),
+                                                 arr(d_alpha_start), arr(d_iters), arr(d_reg),
+                                                 arr(d_status)),
                lambda: lib().cl_multi_last_error(self._m))
 
     def close(self):
@@ -379,7 +408,7 @@ class Solver:
         _check(lib().cl_get_stats(ctx, C.byref(s)), lambda: lib().cl_last_error(ctx))
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
-                "total_trials": s.total_trials}
+                "total_trials": s.total_trials, "fallbacks": s.fallbacks}
 
     def close(self):
         if self._s:
@@ -401,6 +430,81 @@ def solve_batch_noalloc(angular, options, d_u, d_alpha, count, d_iters=None, d_r
                                         ptr(d_alpha), ptr(d_iters), ptr(d_reg), ptr(d_status),
                                         ptr(stream)),
            lib().cl_noalloc_last_error)
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class MLP:
+    """Learned warm start: n -> width x3 -> n MLP trained and evaluated by the
+    library's kernels (cl_mlp_*)."""
+
+    def __init__(self, n, width, moment_type=CL_MN, delta_ppn=1e-10, seed=1):
+        self._m = C.c_void_p()
+        self.n, self.width = n, width
+        self.dims = [n, width, width, width, n]
+        _check(lib().cl_mlp_create(n, width, moment_type, delta_ppn, seed, C.byref(self._m)),
+               lib().cl_global_error)
+
+    def _err(self):
+        return lib().cl_mlp_last_error(self._m)
+
+    def set_output_scaling(self, mean, std):
+        mean = np.ascontiguousarray(mean, dtype=np.float32)
+        std = np.ascontiguousarray(std, dtype=np.float32)
+        _check(lib().cl_mlp_set_output_scaling(self._m, _fp(mean), _fp(std)), self._err)
+
+    def train(self, d_u, d_alpha, count, steps, batch=4096, lr=1e-3, seed=7, record_loss=True):
+        ptr = lambda t: t.data_ptr() if hasattr(t, "data_ptr") else int(t)
+        losses = np.zeros(max(steps, 1), np.float32)
+        _check(lib().cl_mlp_train(self._m, ptr(d_u), ptr(d_alpha), count, steps, batch, lr, seed,
+                                  _fp(losses) if record_loss else None), self._err)
+        return losses[:steps]
+
+    def predict(self, d_u, d_alpha, count, fallback_kind=1, stream=None):
+        ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+        fb = C.c_int(0)
+        _check(lib().cl_mlp_predict(self._m, ptr(d_u), ptr(d_alpha), count, fallback_kind,
+                                    C.byref(fb), ptr(stream)), self._err)
+        return fb.value
+
+    def _bufs(self, withW=True):
+        W = [np.zeros((self.dims[l], self.dims[l + 1]), np.float32) for l in range(4)]
+        b = [np.zeros(self.dims[l + 1], np.float32) for l in range(4)]
+        PW = (C.POINTER(C.c_float) * 4)(*[_fp(w) for w in W])
+        Pb = (C.POINTER(C.c_float) * 4)(*[_fp(x) for x in b])
+        return W, b, PW, Pb
+
+    def loss_and_grads(self, u, alpha):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        W, b, PW, Pb = self._bufs()
+        loss = C.c_float()
+        _check(lib().cl_mlp_loss_and_grads(self._m, _dp(u), _dp(alpha), u.shape[0], C.byref(loss),
+                                           PW, Pb), self._err)
+        return loss.value, W, b
+
+    def get_params(self):
+        W, b, PW, Pb = self._bufs()
+        _check(lib().cl_mlp_get_params(self._m, PW, Pb), self._err)
+        return W, b
+
+    def set_params(self, W, b):
+        W = [np.ascontiguousarray(w, dtype=np.float32) for w in W]
+        b = [np.ascontiguousarray(x, dtype=np.float32) for x in b]
+        PW = (C.POINTER(C.c_float) * 4)(*[_fp(w) for w in W])
+        Pb = (C.POINTER(C.c_float) * 4)(*[_fp(x) for x in b])
+        _check(lib().cl_mlp_set_params(self._m, PW, Pb), self._err)
+
+    def close(self):
+        if self._m:
+            lib().cl_mlp_destroy(self._m)
+            self._m = C.c_void_p()
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_m", None):
+            self.close()
 
 
 def run_deck(deck_path, out_dir=".", max_steps=-1):

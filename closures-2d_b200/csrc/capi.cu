@@ -20,6 +20,7 @@
 using namespace clb;
 
 static std::atomic<long long> g_launches{0};
+int clb_mlp_reserve_for(cl_mlp *m, size_t rows);
 static thread_local std::string g_global_err;
 
 #define CUDA_TRY(ctx, call)                                                                    \
@@ -267,6 +268,8 @@ struct cl_ctx {
     int *dErr = nullptr;
     int *hErr = nullptr;              // pinned [2]
     int *dIters = nullptr;            // [C] iterations of each cell in the last stage
+    cl_mlp *warm = nullptr;           // learned warm start (null: previous stage's alpha)
+    double *dAlphaPred = nullptr;     // [C][n] predicted starts when warm is set
     NewtonArgs nargs;
     FluxArgs fargs;
     int nCtas = 0;
@@ -489,6 +492,7 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->dErr);
     cudaFreeHost(ctx->hErr);
     cudaFree(ctx->dIters);
+    cudaFree(ctx->dAlphaPred);
     cudaFree(ctx->bU);
     cudaFree(ctx->bA);
     cudaFree(ctx->bR);
@@ -513,12 +517,18 @@ static cudaError_t enqueue_step(cl_ctx *ctx, double dt, double dx, double dy, in
                 return e;
             nk += 2;
         }
+        if (ctx->warm) {
+            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
+                return cudaErrorLaunchFailure;
+            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+        }
         NewtonArgs a = ctx->nargs;
         a.prob[0].count = (int)ctx->C;
         a.prob[0].u = ctx->dMom;
         a.prob[0].alpha = ctx->dAlpha;
         a.prob[0].queue = ctx->dQueue + stage;
         a.prob[0].iters = ctx->dIters;
+        a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
         a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
         if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
             return e;
@@ -607,12 +617,18 @@ int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms)
             e = launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, ctx->stream);
             nk += 2;
         }
+        if (ctx->warm && e == cudaSuccess) {
+            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
+                e = cudaErrorLaunchFailure;
+            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+        }
         NewtonArgs a = ctx->nargs;
         a.prob[0].count = (int)ctx->C;
         a.prob[0].u = ctx->dMom;
         a.prob[0].alpha = ctx->dAlpha;
         a.prob[0].queue = ctx->dQueue + stage;
         a.prob[0].iters = ctx->dIters;
+        a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
         a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
         if (e == cudaSuccess)
             e = launch_newton(a, ctx->nCtas, ctx->stream);
@@ -687,6 +703,35 @@ int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha)
     return CL_OK;
 }
 
+int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    if (m) {
+        int rc = clb_mlp_reserve_for(m, (size_t)ctx->C);
+        if (rc) {
+            ctx->err = "warm-start buffers";
+            return rc;
+        }
+        if (!ctx->dAlphaPred &&
+            cudaMalloc(&ctx->dAlphaPred, (size_t)ctx->C * ctx->n * sizeof(double)) != cudaSuccess) {
+            ctx->err = "warm-start buffers";
+            return CL_ERR_CUDA;
+        }
+    }
+    ctx->warm = m;
+    // the captured step changes: re-capture at the next cl_step
+    if (ctx->exec) {
+        cudaGraphExecDestroy(ctx->exec);
+        ctx->exec = nullptr;
+    }
+    if (ctx->graph) {
+        cudaGraphDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    return CL_OK;
+}
+
 int cl_get_last_iterations(cl_ctx *ctx, int *iters)
 {
     if (!ctx || !iters)
@@ -721,11 +766,18 @@ int cl_get_stats(cl_ctx *ctx, cl_stats *s)
         s->hist_reg[i] = (int64_t)d.hist[i];
     s->iter_mean = d.numSolves ? (double)d.totalIter / (double)d.numSolves : 0.0;
     s->total_trials = (int64_t)d.trials;
+    s->fallbacks = (int64_t)d.fallbacks;
     return CL_OK;
 }
 
 int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha, int *d_iters, double *d_reg,
                           int *d_status)
+{
+    return cl_solve_batch_device_start(ctx, count, d_u, d_alpha, nullptr, d_iters, d_reg, d_status);
+}
+
+int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_alpha, const double *d_alpha_start,
+                                int *d_iters, double *d_reg, int *d_status)
 {
     if (!ctx || count < 0 || (count > 0 && (!d_u || !d_alpha)))
         return CL_ERR_ARG;
@@ -738,6 +790,7 @@ int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha, 
     a.prob[0].iters = d_iters;
     a.prob[0].regs = d_reg;
     a.prob[0].status = d_status;
+    a.prob[0].alphaStart = d_alpha_start;
     a.prob[0].queue = ctx->dQueue + 2;
     a.momentsOld = nullptr;
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dQueue + 2, 0, sizeof(unsigned), ctx->stream));
@@ -902,6 +955,13 @@ int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaun
 int cl_multi_solve_device(cl_multi *m, const int *counts, double *const *d_u, double *const *d_alpha,
                           int *const *d_iters, double *const *d_reg, int *const *d_status)
 {
+    return cl_multi_solve_device_start(m, counts, d_u, d_alpha, nullptr, d_iters, d_reg, d_status);
+}
+
+int cl_multi_solve_device_start(cl_multi *m, const int *counts, double *const *d_u, double *const *d_alpha,
+                                double *const *d_alpha_start, int *const *d_iters, double *const *d_reg,
+                                int *const *d_status)
+{
     if (!m || !counts || !d_u || !d_alpha)
         return CL_ERR_ARG;
     NewtonArgs a = m->nargs;
@@ -912,6 +972,7 @@ int cl_multi_solve_device(cl_multi *m, const int *counts, double *const *d_u, do
         a.prob[p].iters = d_iters ? d_iters[p] : nullptr;
         a.prob[p].regs = d_reg ? d_reg[p] : nullptr;
         a.prob[p].status = d_status ? d_status[p] : nullptr;
+        a.prob[p].alphaStart = d_alpha_start ? d_alpha_start[p] : nullptr;
         a.prob[p].queue = m->dQueue + p;
     }
     cudaError_t e = cudaMemsetAsync(m->dQueue, 0, kMaxProblems * sizeof(unsigned), m->stream);

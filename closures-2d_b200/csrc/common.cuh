@@ -76,9 +76,10 @@ struct DevStats {
     unsigned long long totalIter;       // sum of outs.iter
     unsigned long long numSolves;
     unsigned long long trials;          // line-search evaluations
+    unsigned long long fallbacks;       // predicted starts abandoned for the fallback start
     int maxIter;
     int pad;
 };
-constexpr int kStatU64 = kNumReg + 3;
+constexpr int kStatU64 = kNumReg + 4;
 
 }  // namespace clb

@@ -35,7 +35,7 @@ namespace {
 
 enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
 enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_N };
-enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_N };
+enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_N };
 
 constexpr double kSqrtPi = 1.7724538509055160273;
 constexpr double kPi = 3.14159265358979323846;
@@ -258,9 +258,17 @@ __device__ void init_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &
     const int n = pb.n;
     const int cell = L.ints[s * SI_N + SI_CELL];
     double ui = 0.0, ai = 0.0;
+    int pred = 0;
     if (lane < n) {
         ui = pb.u[(size_t)cell * n + lane];
         ai = pb.alpha[(size_t)cell * n + lane];
+    }
+    if (pb.alphaStart != nullptr) {
+        double ap = (lane < n) ? pb.alphaStart[(size_t)cell * n + lane] : 0.0;
+        if (__all_sync(0xffffffffu, isfinite(ap))) {
+            ai = ap;
+            pred = 1;
+        }
     }
     if (a.momentsOld != nullptr && lane < n) {
         int i = cell / a.NY, j = cell % a.NY;
@@ -307,6 +315,7 @@ __device__ void init_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &
         si[SI_TOTAL] = 0;
         si[SI_REG] = 0;
         si[SI_MAXITER] = a.maxIter;
+        si[SI_PRED] = pred;
         si[SI_STATE] = S_NEWTON;
     }
 }
@@ -319,6 +328,30 @@ __device__ void regularize(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     int *si = L.ints + s * SI_N;
     double *sc = L.scal + s * SC_N;
     int reg = si[SI_REG];
+    if (si[SI_PRED] == 1) {
+        // The predicted start failed (the solve would regularise): restart
+        // once from the fallback start with the same u, as plain Newton.
+        const int cell = si[SI_CELL];
+        double af = (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0;
+        const double u0 = sc[SC_U0];
+        if (a.momentType == 0) {
+            if (lane == 0)
+                af = af - sc[SC_ASCALE];
+        } else {
+            af = af / u0;
+        }
+        if (lane < n)
+            L.alpha[s * ldv + lane] = af;
+        __syncwarp();
+        if (lane == 0) {
+            si[SI_PRED] = 2;
+            si[SI_ITER] = 0;
+            sc[SC_T] = 1.0;
+            si[SI_STATE] = S_NEWTON;
+            atomicAdd(&L.stat[kNumReg + 3], 1ull);
+        }
+        return;
+    }
     if (reg >= kNumReg - 1) {
         // opt.cpp:256-261 aborts; report and return the unscaled state.
         double u0 = sc[SC_U0];

@@ -28,7 +28,9 @@ struct NewtonProblem {
     double p0;                  // p[0] = Y_00 (fobj.cpp:305 divides by it)
     int n, nb, K2p, nqp, ldP;
     int count;                  // vectors to solve
-    double *u, *alpha;          // [count][n]
+    double *u, *alpha;          // [count][n]; alpha: start (or fallback start) in, solution out
+    const double *alphaStart;   // nullable [count][n]: predicted start; alpha is then the
+                                // fallback taken (once) before the first regularisation
     int *iters;                 // nullable [count]
     double *regs;               // nullable [count]
     int *status;                // nullable [count]

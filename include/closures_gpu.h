@@ -98,6 +98,7 @@ typedef struct {
     int64_t hist_reg[CL_NUM_REG];   /* c_optStats.histReg */
     int64_t total_iter;             /* sum of iterations (device counter) */
     int64_t total_trials;           /* line-search function evaluations */
+    int64_t fallbacks;              /* predicted starts replaced by the fallback start */
 } cl_stats;
 
 typedef struct cl_ctx cl_ctx;
@@ -148,6 +149,13 @@ int cl_solve_batch(cl_ctx *ctx, int count, double *u, double *alpha,
 /* Same on device pointers (no host copies), on the context's stream. */
 int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
                           int *d_iters, double *d_reg, int *d_status);
+/* Same, starting from d_alpha_start (e.g. cl_mlp_predict's output) where it
+ * is finite; d_alpha is then the fallback start, taken once in place of the
+ * first regularisation step, so a poor prediction costs iterations but does
+ * not change the regularisation the plain start would need. */
+int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
+                                const double *d_alpha_start, int *d_iters, double *d_reg,
+                                int *d_status);
 
 /* Mixed-order batch: a solver context for several moment orders at one
  * quadrature order, so vectors of different N share one persistent launch.
@@ -160,6 +168,10 @@ const char *cl_multi_last_error(const cl_multi *m);
 int cl_multi_solve_device(cl_multi *m, const int *counts, double *const *d_u,
                           double *const *d_alpha, int *const *d_iters,
                           double *const *d_reg, int *const *d_status);
+int cl_multi_solve_device_start(cl_multi *m, const int *counts, double *const *d_u,
+                                double *const *d_alpha, double *const *d_alpha_start,
+                                int *const *d_iters, double *const *d_reg,
+                                int *const *d_status);
 /* ------------------------------------------------------------------------
  * Whole solver behind the reference's Solver interface (solver.h:15-61) for
  * SOLVER momopt on one node: deck parsing (input_deck_reader.cpp), grid and
@@ -201,6 +213,41 @@ int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *opts, int co
                            double *d_u, double *d_alpha, int *d_iters, double *d_reg,
                            int *d_status, void *stream);
 const char *cl_noalloc_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference, which starts every
+ * solve from the previous stage's alpha, momopt_update.cpp:236-238).  An MLP
+ * n -> width -> width -> width -> n (GELU, BF16 weights and activations,
+ * FP32 accumulation on the tensor cores, FP32 Adam) maps u/u0 to the
+ * multipliers of the scaled problem; Newton then runs from the prediction to
+ * the same tolerance, so the network changes iteration counts only.
+ * W_l is [in x out] row-major (y = x W + b); four layers. */
+typedef struct cl_mlp cl_mlp;
+int cl_mlp_create(int n, int width, int moment_type, double delta_ppn, unsigned long long seed, cl_mlp **out);
+void cl_mlp_destroy(cl_mlp *m);
+const char *cl_mlp_last_error(const cl_mlp *m);
+/* Per-component standardisation of the targets: y = (alpha_scaled - mean) / std. */
+int cl_mlp_set_output_scaling(cl_mlp *m, const float *mean, const float *stdv);
+/* Adam (lr, betas 0.9/0.999) on device pairs (u, alpha) [count x n] FP64,
+ * shuffled minibatches; losses[steps] nullable. */
+int cl_mlp_train(cl_mlp *m, const double *d_u, const double *d_alpha, int count, int steps, int batch, float lr,
+                 unsigned long long seed, float *losses);
+/* alpha <- prediction for device u [count x n]; where it is not finite the
+ * given alpha is kept (fallback_kind 0, e.g. the previous stage's) or the
+ * isotropic multiplier is taken (fallback_kind 1).  *fallbacks nullable;
+ * stream null = the network's own stream. */
+int cl_mlp_predict(cl_mlp *m, const double *d_u, double *d_alpha, int count, int fallback_kind, int *fallbacks,
+                   void *stream);
+/* Loss and gradients of one host batch (gradient checks). */
+int cl_mlp_loss_and_grads(cl_mlp *m, const double *u, const double *alpha, int rows, float *loss,
+                          float *const *gW, float *const *gb);
+int cl_mlp_get_params(cl_mlp *m, float *const *W, float *const *b);
+int cl_mlp_set_params(cl_mlp *m, float *const *W, float *const *b);
+/* Grid warm start: before each optimisation stage cl_step predicts alpha for
+ * every cell from its moments (fallback: the previous stage's alpha).  Pass
+ * NULL to return to the reference's plain warm start.  The network must
+ * outlive its use by the context. */
+int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m);
 
 /* Kernel launches issued by the library since load (for the bench). */
 int64_t cl_launch_count(void);
