@@ -400,12 +400,46 @@ def batch_arm(args, world, rank, local):
     dst = [torch.zeros(c, dtype=torch.int32, device=dev) for c in counts]
     opts = cb.make_options(tol=1e-8)
     m = cb.MultiSolver(BATCH_ORDERS, Q, gaunt, opts)
+    nets, dstart = None, None
+    train_s = 0.0
+    if args.newton == "nn":
+        # learned warm start: one network per order, trained on (u, alpha*)
+        # pairs the plain GPU Newton solver produces for fresh samples
+        t0 = time.perf_counter()
+        nets, dstart = [], []
+        sqpi = np.sqrt(np.pi)
+        for k, (a, o) in enumerate(zip(angs, BATCH_ORDERS)):
+            nt = 1 << 18
+            ut, _ = sample_batch_torch(a, nt, gen, dev)
+            at = torch.from_numpy(cb.isotropic_alpha(a.n, nt)).to(dev)
+            stt = torch.zeros(nt, dtype=torch.int32, device=dev)
+            rgt = torch.zeros(nt, dtype=torch.float64, device=dev)
+            ctx = cb.Context.for_batches(a, opts)
+            ctx.solve_batch_device(ut, at, None, rgt, stt, count=nt)
+            torch.cuda.synchronize()
+            ok = (stt == 0) & (rgt == 0)
+            ut, at = ut[ok].contiguous(), at[ok].contiguous()
+            ctx.close()
+            x = ut.cpu().numpy()
+            lin = 2.0 * sqpi * x
+            lin[:, 0] = 2.0 * sqpi * np.log(0.5 / sqpi)
+            resid = at.cpu().numpy() - lin
+            net = cb.MLP(a.n, 256, seed=17 + o)
+            net.set_output_scaling(resid.mean(axis=0), resid.std(axis=0) + 1e-3)
+            net.train(ut, at, ut.shape[0], steps=args.nn_steps, batch=4096, lr=1e-3,
+                      record_loss=False)
+            nets.append(net)
+            dstart.append(torch.empty_like(a_iso[k]))
+        train_s = time.perf_counter() - t0
 
     def one():
         for k in range(len(counts)):
             du[k].copy_(u0[k])
             da[k].copy_(a_iso[k])
-        m.solve_device(counts, du, da, dit, dreg, dst)
+        if nets is not None:
+            for k in range(len(counts)):
+                nets[k].predict(du[k], dstart[k], counts[k], fallback_kind=2)
+        m.solve_device(counts, du, da, dit, dreg, dst, d_alpha_start=dstart)
 
     for _ in range(args.warmup):
         one()
@@ -457,7 +491,11 @@ def batch_arm(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": "batch_2e20", "vectors": total,
                                              "orders": BATCH_ORDERS, "quad_order": Q,
-                                             "use_gaunt": gaunt, "tol": 1e-8, "start": "isotropic"},
+                                             "use_gaunt": gaunt, "tol": 1e-8,
+                                             "newton": args.newton,
+                                             "start": "mlp prediction (isotropic fallback)"
+                                             if nets is not None else "isotropic"},
+            "nn_train_s": train_s if nets is not None else None,
             "per_order": per, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -473,6 +511,9 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--workload", default="m6_800", choices=sorted(WORKLOADS) + ["batch_2e20"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
+                    help="batch workload: start from the isotropic multiplier or a learned prediction")
+    ap.add_argument("--nn-steps", type=int, default=4000)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.workload == "batch_2e20":
