@@ -101,12 +101,12 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
     B.ldP = ldP;
     B.ldPf = B.nb + 4;
     B.p0 = p[0];
-    std::vector<double> P((size_t)B.nqp * ldP, 0.0), W(B.nqp, 0.0);
+    std::vector<double> P((size_t)B.nqp * ldP + B.nqp, 0.0), W(B.nqp, 0.0);
     std::vector<double> Pf((size_t)B.nqp * B.ldPf, 0.0), XI(B.nqp, 0.0), ET(B.nqp, 0.0), CX(B.nqp, 0.0),
         CY(B.nqp, 0.0);
     for (int q = 0; q < nq; q++) {
         const double *pq = p + (size_t)q * n2;
-        double *row = &P[(size_t)q * ldP];
+        double *row = &P[(size_t)basis_row(q, ldP)];
         for (int k = 0; k < n; k++)
             row[k] = pq[k];
         if (useGaunt) {
@@ -119,6 +119,7 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
                     row[B.nb + c++] = pq[i] * pq[j];
         }
         W[q] = w[q];
+        P[(size_t)basis_wgap(q, ldP)] = w[q];
         for (int k = 0; k < n; k++)
             Pf[(size_t)q * B.ldPf + k] = pq[k];
         XI[q] = xi[q];
@@ -554,7 +555,9 @@ static int read_device_error(cl_ctx *ctx)
     if (ctx->hErr[0] != 0) {
         long long cell = ctx->hErr[1];
         char buf[256];
-        if (ctx->NY > 0 && cell < ctx->C)
+        if (cell < 0)
+            snprintf(buf, sizeof(buf), "%s", error_text(ctx->hErr[0]));
+        else if (ctx->NY > 0 && cell < ctx->C)
             snprintf(buf, sizeof(buf), "%s (cell i=%lld j=%lld)", error_text(ctx->hErr[0]), cell / ctx->NY,
                      cell % ctx->NY);
         else
@@ -1128,10 +1131,20 @@ __global__ void exp_check_kernel(const double *x, int n, double *fast, double *r
     for (int i = threadIdx.x; i < 64; i += blockDim.x)
         tab[i] = ex.tab[i];
     __syncthreads();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        fast[i] = fast_exp(x[i], tab, ex.invL, ex.L1, ex.L2);
-        ref[i] = exp(x[i]);
+    // the batched form the kernels use: four consecutive inputs per thread
+    int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (i + 3 < n) {
+        double xv[4] = {x[i], x[i + 1], x[i + 2], x[i + 3]}, yv[4];
+        fast_exp_n<4>(yv, xv, tab, ex.invL, ex.L1, ex.L2);
+        for (int h = 0; h < 4; h++) {
+            fast[i + h] = yv[h];
+            ref[i + h] = exp(xv[h]);
+        }
+    } else {
+        for (; i < n; i++) {
+            fast[i] = fast_exp(x[i], tab, ex.invL, ex.L1, ex.L2);
+            ref[i] = exp(x[i]);
+        }
     }
 }
 }  // namespace
@@ -1148,7 +1161,7 @@ extern "C" int cl_exp_check(const double *x, int n, double *fast, double *ref)
     ExpConsts ex;
     exp_consts_init(ex);
     cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
-    exp_check_kernel<<<(n + 255) / 256, 256>>>(d, n, d + n, d + 2 * (size_t)n, ex);
+    exp_check_kernel<<<((n + 3) / 4 + 255) / 256, 256>>>(d, n, d + n, d + 2 * (size_t)n, ex);
     g_launches += 1;
     cudaMemcpy(fast, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
     cudaError_t e = cudaMemcpy(ref, d + 2 * (size_t)n, sizeof(double) * n, cudaMemcpyDeviceToHost);

@@ -25,11 +25,10 @@ struct ExpConsts {
 // Host: fills the constants (long double arithmetic for the table tails).
 void exp_consts_init(ExpConsts &c);
 
-__device__ __forceinline__ double fast_exp(double x, const double *__restrict__ tab, double invL, double L1,
-                                           double L2)
+// Table method for |x| <= 700 (no range check).
+__device__ __forceinline__ double fast_exp_core(double x, const double *__restrict__ tab, double invL,
+                                                double L1, double L2)
 {
-    if (!(fabs(x) <= 700.0))
-        return exp(x);
     const double shifter = 6755399441055744.0;      // 1.5 * 2^52: rounds to integer in the low bits
     double t = fma(x, invL, shifter);
     long long N = __double_as_longlong(t) - __double_as_longlong(shifter);
@@ -50,6 +49,35 @@ __device__ __forceinline__ double fast_exp(double x, const double *__restrict__ 
     // multiply by 2^m (|m| <= 1011 here, so the scale is a normal number)
     double scale = __longlong_as_double((m + 1023) << 52);
     return y * scale;
+}
+
+__device__ __forceinline__ double fast_exp(double x, const double *__restrict__ tab, double invL, double L1,
+                                           double L2)
+{
+    if (!(fabs(x) <= 700.0))
+        return exp(x);
+    return fast_exp_core(x, tab, invL, L1, L2);
+}
+
+// K exponentials as straight-line code (independent evaluations interleave;
+// a range branch per value would serialise them), then one branch that
+// sends inputs outside [-700, 700] and NaN to the CUDA library exp.
+template <int K>
+__device__ __forceinline__ void fast_exp_n(double (&y)[K], const double (&x)[K], const double *__restrict__ tab,
+                                           double invL, double L1, double L2)
+{
+    bool out = false;
+#pragma unroll
+    for (int h = 0; h < K; h++) {
+        y[h] = fast_exp_core(fmin(fmax(x[h], -700.0), 700.0), tab, invL, L1, L2);
+        out |= !(fabs(x[h]) <= 700.0);
+    }
+    if (out) {
+#pragma unroll
+        for (int h = 0; h < K; h++)
+            if (!(fabs(x[h]) <= 700.0))
+                y[h] = exp(x[h]);
+    }
 }
 
 }  // namespace clb

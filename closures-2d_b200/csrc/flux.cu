@@ -121,22 +121,25 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
             for (int k0 = 0; k0 < nb; k0 += 8)
                 dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
                            B[k0 + t4 + 4]);
+            double v[4];
+            if (f.momentType == 0) {
+                fast_exp_n<4>(v, cs, sExp, f.ex.invL, f.ex.L1, f.ex.L2);
+            } else {
+                const double dl = f.deltaPPn;
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const double kin = cs[h];
+                    if (kin > 0)
+                        v[h] = 0.5 * kin + 0.5 * sqrt(kin * kin + 4 * dl);
+                    else
+                        v[h] = -dl / (0.5 * kin - 0.5 * sqrt(kin * kin + 4 * dl));
+                }
+            }
 #pragma unroll
             for (int h = 0; h < 4; h++) {
-                double kin = cs[h];
-                double v;
-                if (f.momentType == 0) {
-                    v = fast_exp(kin, sExp, f.ex.invL, f.ex.L1, f.ex.L2);
-                } else {
-                    double dl = f.deltaPPn;
-                    if (kin > 0)
-                        v = 0.5 * kin + 0.5 * sqrt(kin * kin + 4 * dl);
-                    else
-                        v = -dl / (0.5 * kin - 0.5 * sqrt(kin * kin + 4 * dl));
-                }
                 int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
                 int q = nt * 8 + 2 * t4 + (h & 1);
-                sA[q * ldA + cell] = v;
+                sA[q * ldA + cell] = v[h];
             }
         }
         __syncthreads();

@@ -53,63 +53,77 @@ __device__ __forceinline__ void record_error(int *err, int code, int idx)
 
 // Cholesky of the symmetric matrix whose row `lane` is h[] (registers), in
 // the dot-product (Crout) form by columns: lane i >= j forms
-// L_ij = (H_ij - sum_k<j L_ik L_jk) / L_jj with row j of L broadcast from
-// lane j.  On return h[k] = L_lane,k for k <= lane and rdiag = 1/L_lane,lane.
-// LAPACK-style info: 0, or j+1 at the first non-positive or NaN pivot
-// (dpotrf semantics).
-__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], double &rdiag, int n, int lane)
+// L_ij = (H_ij - sum_k<j L_ik L_jk) / L_jj.  Row j of L is read back from the
+// warp's shared-memory matrix Ls (stride ldl, even) with 16-byte broadcast
+// loads: lane i writes L_ij there at step j, and 1/L_jj on the diagonal.
+// On return h[k] = L_lane,k for k <= lane.  LAPACK-style info: 0, or j+1 at
+// the first non-positive or NaN pivot (dpotrf semantics).
+__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], double *Ls, int ldl, int n, int lane)
 {
 #pragma unroll
     for (int j = 0; j < kMaxN; j++) {
         if (j < n) {
-            double s0 = h[j], s1 = 0.0;
+            const double *Lj = Ls + j * ldl;
+            double s0 = h[j], s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-            for (int k = 0; k < j; k++) {
-                double ljk = __shfl_sync(0xffffffffu, h[k], j);
-                if (k & 1)
-                    s1 = fma(-h[k], ljk, s1);
-                else
-                    s0 = fma(-h[k], ljk, s0);
+            for (int k = 0; k + 1 < j; k += 2) {
+                const double2 l = *reinterpret_cast<const double2 *>(Lj + k);
+                if (k & 2) {
+                    s2 = fma(-h[k], l.x, s2);
+                    s3 = fma(-h[k + 1], l.y, s3);
+                } else {
+                    s0 = fma(-h[k], l.x, s0);
+                    s1 = fma(-h[k + 1], l.y, s1);
+                }
             }
-            double s = s0 + s1;
-            double djj = __shfl_sync(0xffffffffu, s, j);
+            if (j & 1)
+                s1 = fma(-h[j - 1], Lj[j - 1], s1);
+            const double s = (s0 + s1) + (s2 + s3);
+            const double djj = __shfl_sync(0xffffffffu, s, j);
             if (!(djj > 0.0))
                 return j + 1;
-            double r = rsqrt(djj);
+            const double r = rsqrt(djj);
             if (lane == j) {
                 h[j] = djj * r;
-                rdiag = r;
-            } else if (lane > j) {
+                Ls[j * ldl + j] = r;
+            } else if (lane > j && lane < n) {
                 h[j] = s * r;
+                Ls[lane * ldl + j] = h[j];
             }
+            __syncwarp();
         }
     }
     return 0;
 }
 
-// Column `lane` of L^-1 into v[] from the factor rows in h[] (lane i holds
-// row i): Linv_ic = -(sum_{k=c}^{i-1} L_ik Linv_kc) / L_ii, rows in order.
-__device__ __forceinline__ void invert_regs(const double (&h)[kMaxN], double rdiag, double (&v)[kMaxN], int n,
-                                            int lane)
+// Column `lane` of L^-1 into v[]: Linv_ic = -(sum_{k=c}^{i-1} L_ik Linv_kc) / L_ii,
+// rows in order, row i of L and 1/L_ii read from Ls as left by chol_regs.
+__device__ __forceinline__ void invert_regs(const double *Ls, int ldl, double (&v)[kMaxN], int n, int lane)
 {
 #pragma unroll
     for (int i = 0; i < kMaxN; i++) {
         v[i] = 0.0;
         if (i < n) {
-            double a0 = 0.0, a1 = 0.0;
+            const double *Li = Ls + i * ldl;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
-            for (int k = 0; k < i; k++) {
-                double lik = __shfl_sync(0xffffffffu, h[k], i);
-                if (k & 1)
-                    a1 = fma(lik, v[k], a1);
-                else
-                    a0 = fma(lik, v[k], a0);
+            for (int k = 0; k + 1 < i; k += 2) {
+                const double2 l = *reinterpret_cast<const double2 *>(Li + k);
+                if (k & 2) {
+                    a2 = fma(l.x, v[k], a2);
+                    a3 = fma(l.y, v[k + 1], a3);
+                } else {
+                    a0 = fma(l.x, v[k], a0);
+                    a1 = fma(l.y, v[k + 1], a1);
+                }
             }
-            double rinv = __shfl_sync(0xffffffffu, rdiag, i);
+            if (i & 1)
+                a1 = fma(Li[i - 1], v[i - 1], a1);
+            const double rinv = Li[i];
             if (lane == i)
                 v[i] = rinv;
             else if (lane < i)
-                v[i] = -(a0 + a1) * rinv;
+                v[i] = -((a0 + a1) + (a2 + a3)) * rinv;
         }
     }
 }
@@ -193,6 +207,7 @@ struct Layout {
     unsigned short *ellIdx, *ellPair;
     int *ellOff;
     double *exptab;
+    unsigned long long *bar;   // three mbarriers of the staged basis chunks
 };
 
 __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
@@ -217,6 +232,7 @@ __device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
     L.ellPair = (unsigned short *)(sm + a.offEllPair);
     L.ellOff = (int *)(sm + a.offEllOff);
     L.exptab = sm + a.offExp;
+    L.bar = (unsigned long long *)(sm + a.offBar);
     return L;
 }
 
@@ -418,9 +434,23 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     // H from the contraction results (fobj.cpp:129-155)
     if (a.useGaunt) {
         for (int c = 0; c < pb.ellChunks; c++) {
-            unsigned short pr = L.ellPair[c * 32 + lane];
+            const unsigned short pr = L.ellPair[c * 32 + lane];
+            const int e1 = L.ellOff[c + 1];
+            int e = L.ellOff[c];
             double v = 0.0;
-            for (int e = L.ellOff[c]; e < L.ellOff[c + 1]; e++)
+            // loads of four entries issued ahead of their (in-order) sum
+            for (; e + 4 <= e1; e += 4) {
+                const int i0 = L.ellIdx[e * 32 + lane], i1 = L.ellIdx[(e + 1) * 32 + lane];
+                const int i2 = L.ellIdx[(e + 2) * 32 + lane], i3 = L.ellIdx[(e + 3) * 32 + lane];
+                const double w0 = L.ellVal[e * 32 + lane], w1 = L.ellVal[(e + 1) * 32 + lane];
+                const double w2 = L.ellVal[(e + 2) * 32 + lane], w3 = L.ellVal[(e + 3) * 32 + lane];
+                const double g0 = Gs[i0], g1 = Gs[i1], g2 = Gs[i2], g3 = Gs[i3];
+                v += w0 * g0;
+                v += w1 * g1;
+                v += w2 * g2;
+                v += w3 * g3;
+            }
+            for (; e < e1; e++)
                 v += L.ellVal[e * 32 + lane] * Gs[L.ellIdx[e * 32 + lane]];
             if (pr != 0xFFFF) {
                 int i = pr >> 8, j = pr & 255;
@@ -499,12 +529,12 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         rowsum += fabs(h[k]);
     }
     const double anorm = warp_max(rowsum);
-    double rdiag = 1.0;
-    int info = chol_regs(h, rdiag, n, lane);
+    __syncwarp();
+    int info = chol_regs(h, Hs, ldh, n, lane);
     double condest = 0.0;
     if (info == 0) {
         // column `lane` of L^-1 in v[], rows of L^-1 in Hs
-        invert_regs(h, rdiag, v, n, lane);
+        invert_regs(Hs, ldh, v, n, lane);
         __syncwarp();
         double colsum = 0.0;
 #pragma unroll
@@ -541,12 +571,18 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     if (act)
         for (int c = 0; c <= lane; c++)
             y = fma(Hs[lane * ldh + c], vec[c], y);
+    __syncwarp();
+    vec[32 + lane] = y;
+    __syncwarp();
     double z = 0.0;
 #pragma unroll
-    for (int i = 0; i < kMaxN; i++) {
-        double yi = __shfl_sync(0xffffffffu, y, i);
-        if (i < n)
-            z = fma(v[i], yi, z);
+    for (int i = 0; i < kMaxN; i += 2) {
+        if (i < n) {
+            const double2 yi = *reinterpret_cast<const double2 *>(vec + 32 + i);
+            z = fma(v[i], yi.x, z);
+            if (i + 1 < n)
+                z = fma(v[i + 1], yi.y, z);
+        }
     }
     const double di = act ? -z : 0.0;
     const double err = sqrt(warp_sum(gi * gi));
@@ -604,7 +640,201 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     regularize(a, pb, L, s, lane, ldv, ui, ai);
 }
 
-template <int TPW>
+// Fused evaluation contractions (used when every problem's G has at most NTF
+// column tiles of 8).  Warp w owns slot rows mt = w % 2 (16 slots) and the
+// q-group qg = w / 2 (8 of the chunk's 32 quadrature rows): it forms
+// S = alpha . P^T for its 16 x 8 block,
+// the weights E = w exp(S) in the accumulator layout, and uses them directly
+// as the A operand of G += E . Phess.  The A fragment's k-slots t and t+4 are
+// taken as quadrature rows 2t and 2t+1 (the rows the accumulator of S gives
+// this lane), and the B fragment is read from the same two rows, so E never
+// goes through shared memory.  Chunks keep the basis_row layout of the
+// global array, under which both fragment patterns (rows g, and rows 2t,
+// 2t + 1) are free of bank conflicts.  The four q-group
+// partial sums of G are added in q-group order at the end.  Three chunk
+// buffers keep one chunk in flight while two are read.
+constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on any wait for a staged chunk
+
+template <int NTF, int PPN>
+__device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int tid,
+                                              int lane, int warp, unsigned &mbPhase)
+{
+    const int g = lane >> 2, t4 = lane & 3;
+    const int kq = a.kq, ldv = a.ldv, ldG = a.ldG;
+    const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
+    const int NTH = K2p / 8;
+    const int NT2 = NTH + (a.momentType == 1 ? nb / 8 : 0);
+    const int nchunks = pb.nqp / kq;
+    const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
+    const int mt = warp & 1, qg = warp >> 1;
+    const int r0 = mt * 16 + g, r1 = r0 + 8;
+    const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
+    const double *A0 = L.alpha + r0 * ldv + t4, *A1 = L.alpha + r1 * ldv + t4;
+    double acc[NTF][4];
+#pragma unroll
+    for (int j = 0; j < NTF; j++)
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+    double facc0 = 0.0, facc1 = 0.0;
+    const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
+
+    // Chunk c into buffer `buf`: one bulk copy of the contiguous block
+    // (chunkDoubles is even, the block starts 16-byte aligned), issued by
+    // thread 0 with its byte count expected on the buffer's mbarrier.
+    const unsigned chunkBytes = (unsigned)chunkDoubles * 8u;
+    unsigned pending = 0;   // buffers with a copy issued and not yet waited for
+    auto load_chunk = [&](int c, int buf) {
+        if (tid == 0) {
+            mbar_expect_tx(&L.bar[buf], chunkBytes);
+            bulk_copy_g2s(L.P + buf * chunkDoubles, pb.P + (size_t)c * chunkDoubles, chunkBytes, &L.bar[buf]);
+        }
+        pending |= 1u << buf;
+    };
+    auto wait_chunk = [&](int buf) -> bool {
+        const bool ok = mbar_wait_bounded(&L.bar[buf], (mbPhase >> buf) & 1u, kWaitNs);
+        mbPhase ^= 1u << buf;
+        pending &= ~(1u << buf);
+        return ok;
+    };
+    // after a timeout: wait (bounded) for the copies still in flight so that
+    // none lands in shared memory after the CTA has exited
+    auto abandon = [&]() {
+        if (tid == 0)
+            record_error(a.err, -5, -1);
+        for (int b = 0; b < 3; b++)
+            if (pending & (1u << b))
+                wait_chunk(b);
+        return false;
+    };
+    const int qa = qg * 8 + g;                 // GEMM1 B rows
+    const int qb = qg * 8 + 2 * t4;            // GEMM2 B rows qb, qb + 1
+    const int offA = basis_row(qa, ldP);
+    const int wOff = basis_wgap(qb, ldP);   // weights of rows qb, qb + 1
+    const int offB = basis_row(qb, ldP) + g;   // rows qb and qb + 1 share the gap
+
+    // S block of chunk c (the staged copy at Pb)
+    auto gemm1 = [&](const double *Pb, double (&cs)[4]) {
+        cs[0] = cs[1] = cs[2] = cs[3] = 0.0;
+        const double *B1 = Pb + offA;
+#pragma unroll
+        for (int ks = 0; ks < 4; ks++)
+            if (ks * 8 < nb)
+                dmma16x8x8(cs, A0[ks * 8], A1[ks * 8], A0[ks * 8 + 4], A1[ks * 8 + 4], B1[ks * 8 + t4],
+                           B1[ks * 8 + t4 + 4]);
+    };
+    // e[h]: Hessian weights, eg[h]: PPn gradient weights; h = 0..3 is
+    // (slot r0, row qb), (r0, qb + 1), (r1, qb), (r1, qb + 1) of chunk c
+    auto weights = [&](const double *Pc, const double (&cs)[4], double (&e)[4], double (&eg)[4]) {
+        const double w0 = Pc[wOff], w1 = Pc[wOff + 1];   // staged with the chunk
+        if constexpr (PPN == 0) {
+            fast_exp_n<4>(e, cs, L.exptab, invL, L1, L2);
+            e[0] *= w0;
+            e[1] *= w1;
+            e[2] *= w0;
+            e[3] *= w1;
+            facc0 += e[0] + e[1];
+            facc1 += e[2] + e[3];
+            eg[0] = eg[1] = eg[2] = eg[3] = 0.0;
+        } else {
+            // fobj.cpp:408-434 and :196-210 (PPn)
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const double dl = (h < 2) ? dl0 : dl1;
+                const double ww = (h & 1) ? w1 : w0;
+                const double k = 0.5 * cs[h];
+                const double s2 = sqrt(k * k + dl);
+                double G = k + s2;
+                if (k < 0)
+                    G = -dl / (k - sqrt(k * k + dl));
+                e[h] = 0.5 * ww * (G / s2);
+                eg[h] = ww * G;
+                const double ft = ww * (k * G - 0.5 * dl + dl * log(G));
+                if (h < 2)
+                    facc0 += ft;
+                else
+                    facc1 += ft;
+            }
+        }
+    };
+
+    // Software pipeline over three staged chunks: iteration c accumulates
+    // G with chunk c's weights while it forms S and the weights of chunk
+    // c + 1, and the copy of chunk c + 2 is in flight.
+    load_chunk(0, 0);
+    if (nchunks > 1)
+        load_chunk(1, 1);
+    if (__syncthreads_or(!wait_chunk(0)))
+        return abandon();
+    double e[4], eg[4];
+    {
+        double cs[4];
+        gemm1(L.P, cs);
+        weights(L.P, cs, e, eg);
+    }
+    int bc = 0;   // buffer of chunk c
+    for (int c = 0; c < nchunks; c++) {
+        const int bn = (bc == 2) ? 0 : bc + 1, bf = (bn == 2) ? 0 : bn + 1;
+        const bool okWait = (c + 1 < nchunks) ? wait_chunk(bn) : true;
+        // chunk c + 1 visible to all; every warp is done with chunk c - 1 (buffer bf)
+        if (__syncthreads_or(!okWait))
+            return abandon();
+        if (c + 2 < nchunks)
+            load_chunk(c + 2, bf);
+        const bool more = c + 1 < nchunks;
+        double cs[4];
+        if (more)
+            gemm1(L.P + bn * chunkDoubles, cs);
+        const double *B2 = L.P + bc * chunkDoubles + offB;
+#pragma unroll
+        for (int nt = 0; nt < NTF; nt++) {
+            if (nt < NT2) {
+                const bool hess = (PPN == 0) || nt < NTH;
+                const int col = hess ? nb + nt * 8 : (nt - NTH) * 8;
+                const double x0 = hess ? e[0] : eg[0], x1 = hess ? e[1] : eg[1];
+                const double x2 = hess ? e[2] : eg[2], x3 = hess ? e[3] : eg[3];
+                dmma16x8x8(acc[nt], x0, x2, x1, x3, B2[col], B2[col + ldP]);
+            }
+        }
+        if (more)
+            weights(L.P + bn * chunkDoubles, cs, e, eg);
+        bc = bn;
+    }
+    __syncthreads();   // the G region overlaps the staged basis
+#pragma unroll 1
+    for (int step = 0; step < 4; step++) {
+        if (qg == step) {
+#pragma unroll
+            for (int nt = 0; nt < NTF; nt++) {
+                if (nt < NT2) {
+                    double *G0 = L.G + r0 * ldG + nt * 8 + 2 * t4;
+                    if (step == 0) {
+                        G0[0] = acc[nt][0];
+                        G0[1] = acc[nt][1];
+                        G0[8 * ldG] = acc[nt][2];
+                        G0[8 * ldG + 1] = acc[nt][3];
+                    } else {
+                        G0[0] += acc[nt][0];
+                        G0[1] += acc[nt][1];
+                        G0[8 * ldG] += acc[nt][2];
+                        G0[8 * ldG + 1] += acc[nt][3];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    facc0 += __shfl_xor_sync(0xffffffffu, facc0, 1);
+    facc0 += __shfl_xor_sync(0xffffffffu, facc0, 2);
+    facc1 += __shfl_xor_sync(0xffffffffu, facc1, 1);
+    facc1 += __shfl_xor_sync(0xffffffffu, facc1, 2);
+    if (t4 == 0) {
+        L.fpart[r0 * a.ntq + qg] = facc0;
+        L.fpart[r1 * a.ntq + qg] = facc1;
+    }
+    __syncthreads();
+    return true;
+}
+
+template <int TPW, int NTF, int PPN>
 __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
 {
     extern __shared__ __align__(16) double sm[];
@@ -629,8 +859,14 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         ctl[1] = 0;
         ctl[2] = 0;
     }
+    if (tid == 0) {
+        for (int b = 0; b < 3; b++)
+            mbar_init(&L.bar[b], 1);
+        mbar_init_fence();
+    }
     __syncthreads();
     int loadedProb = -1;
+    unsigned mbPhase = 0;   // parity of the next phase of each chunk mbarrier
 
     for (;;) {
         // ---- refill idle slots from the work counter of the current problem
@@ -701,12 +937,16 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         __syncthreads();
 
         // ---- phase A: evaluation contractions over the quadrature
+        if constexpr (NTF > 0) {
+            if (!phase_a_fused<NTF, PPN>(a, pb, L, tid, lane, warp, mbPhase))
+                return;   // a staged chunk never arrived (error recorded)
+        } else {
         const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
         const int NTH = K2p / 8;
         const int NT2 = NTH + (a.momentType == 1 ? nb / 8 : 0);
         const int ntiles2 = MT * NT2;
         const int nchunks = pb.nqp / kq;
-        const int chunkDoubles = kq * ldP;
+        const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
         const int mt1 = warp % MT, ntq = warp / MT;
         double acc[TPW][4];
 #pragma unroll
@@ -744,7 +984,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
             {
                 double cs[4] = {0.0, 0.0, 0.0, 0.0};
                 const double *A0 = L.alpha + r0 * ldv, *A1 = L.alpha + r1 * ldv;
-                const double *B = Pb + (ntq * 8 + g) * ldP;
+                const double *B = Pb + basis_row(ntq * 8 + g, ldP);
                 for (int k0 = 0; k0 < nb; k0 += 8)
                     dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4],
                                B[k0 + t4], B[k0 + t4 + 4]);
@@ -753,10 +993,9 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                 const double w0 = __ldg(&pb.w[qg]), w1 = __ldg(&pb.w[qg + 1]);
                 if (a.momentType == 0) {
                     const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
-                    double e0 = w0 * fast_exp(cs[0], L.exptab, invL, L1, L2);
-                    double e1 = w1 * fast_exp(cs[1], L.exptab, invL, L1, L2);
-                    double e2 = w0 * fast_exp(cs[2], L.exptab, invL, L1, L2);
-                    double e3 = w1 * fast_exp(cs[3], L.exptab, invL, L1, L2);
+                    double ex4[4];
+                    fast_exp_n<4>(ex4, cs, L.exptab, invL, L1, L2);
+                    double e0 = w0 * ex4[0], e1 = w1 * ex4[1], e2 = w0 * ex4[2], e3 = w1 * ex4[3];
                     L.E[r0 * ldE + ql] = e0;
                     L.E[r0 * ldE + ql + 1] = e1;
                     L.E[r1 * ldE + ql] = e2;
@@ -800,8 +1039,9 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                         int col = (nt2 < NTH) ? nb + nt2 * 8 : (nt2 - NTH) * 8;
                         const double *A0 = Ab + (mt2 * 16 + g) * ldE + k0 + t4;
                         const double *A1 = A0 + 8 * ldE;
-                        const double *B0 = Pb + (k0 + t4) * ldP + col + g;
-                        dmma16x8x8(acc[j], A0[0], A1[0], A0[4], A1[4], B0[0], B0[4 * ldP]);
+                        const double *B0 = Pb + basis_row(k0 + t4, ldP) + col + g;
+                        // row k0 + t4 + 4 is 4 * ldP + 4 doubles further (one gap)
+                        dmma16x8x8(acc[j], A0[0], A1[0], A0[4], A1[4], B0[0], B0[4 * ldP + 4]);
                     }
                 }
             }
@@ -829,6 +1069,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
             L.fpart[r1 * a.ntq + ntq] = facc1;
         }
         __syncthreads();
+        }
 
         // ---- phase B: per-slot Newton logic, one warp per slot
         for (int s = warp; s < T; s += kWarps) {
@@ -836,6 +1077,8 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
             if (st == S_NEWTON || st == S_TRIAL)
                 slot_logic(a, pb, L, s, lane, warp);
         }
+        if constexpr (NTF > 0)
+            fence_proxy_async_smem();   // this round's shared-memory writes before the next bulk copies
         __syncthreads();
     }
 
@@ -870,7 +1113,7 @@ int plan_newton(NewtonArgs &a)
     a.ldv = nbMax + 4;
     a.ldE = a.kq + 4;
     a.ldG = K2tot + 4;
-    a.ldh = (nMax % 2 == 0) ? nMax + 1 : nMax;
+    a.ldh = (nMax | 1) + 1;   // even: 16-byte row pairs for the broadcast loads
     const int T = a.T;
     int off = 0;
     auto take = [&](int ndoubles) {
@@ -891,10 +1134,15 @@ int plan_newton(NewtonArgs &a)
     a.offEllPair = take((ellChunks * 32 + 3) / 4);
     a.offEllOff = take((ellChunks + 2) / 2);
     a.offExp = take(64);
+    a.offBar = take(4);
     exp_consts_init(a.ex);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
     a.tpw = (ntiles2 + kWarps - 1) / kWarps;
+    // fused contractions when every problem's G fits in 16 column tiles
+    // (one warp per 16 slots x 8 quadrature rows of a 32-row chunk)
+    const int nt2 = K2tot / 8;
+    a.ntf = (nt2 <= 16) ? ((nt2 + 3) / 4) * 4 : 0;
     // phase-B region
     int offG = unionBase;
     int offH = offG + ((T * a.ldG + 1) & ~1);
@@ -902,9 +1150,24 @@ int plan_newton(NewtonArgs &a)
     int endB = offVec + kWarps * 64;
     // phase-A region
     const int maxDoubles = (232448 - 1024) / 8;   // opt-in limit minus static shared
+    if (a.ntf > 0) {
+        const int endA = unionBase + 3 * (a.kq * ldPMax + a.kq);   // three chunks
+        const int end = endA > endB ? endA : endB;
+        if (end <= maxDoubles) {
+            a.doubleBuffer = 1;
+            a.offP = unionBase;
+            a.offE = a.offEg = 0;
+            a.offG = offG;
+            a.offH = offH;
+            a.offVec = offVec;
+            a.smemBytes = end * 8;
+            return 0;
+        }
+        a.ntf = 0;
+    }
     for (int db = 1; db >= 0; db--) {
         int offP = unionBase;
-        int offE = offP + (db ? 2 : 1) * a.kq * ldPMax;
+        int offE = offP + (db ? 2 : 1) * (a.kq * ldPMax + a.kq);
         int offEg = offE + T * a.ldE;
         int endA = offEg + T * a.ldE;
         int end = endA > endB ? endA : endB;
@@ -923,59 +1186,79 @@ int plan_newton(NewtonArgs &a)
     return -1;
 }
 
-template <int TPW>
+template <int TPW, int NTF, int PPN>
 static cudaError_t launch_t(const NewtonArgs &a, int grid, cudaStream_t stream, bool prepare)
 {
     if (prepare)
-        return cudaFuncSetAttribute(newton_kernel<TPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(newton_kernel<TPW, NTF, PPN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     a.smemBytes);
-    newton_kernel<TPW><<<grid, kThreads, a.smemBytes, stream>>>(a);
+    newton_kernel<TPW, NTF, PPN><<<grid, kThreads, a.smemBytes, stream>>>(a);
     return cudaGetLastError();
 }
 
-static cudaError_t dispatch(const NewtonArgs &a, int grid, cudaStream_t stream, bool prepare)
-{
-    if (a.tpw <= 1)
-        return launch_t<1>(a, grid, stream, prepare);
-    if (a.tpw <= 2)
-        return launch_t<2>(a, grid, stream, prepare);
-    if (a.tpw <= 4)
-        return launch_t<4>(a, grid, stream, prepare);
-    if (a.tpw <= 8)
-        return launch_t<8>(a, grid, stream, prepare);
-    if (a.tpw <= 16)
-        return launch_t<16>(a, grid, stream, prepare);
-    return cudaErrorInvalidValue;
-}
-
-cudaError_t prepare_newton(const NewtonArgs &a) { return dispatch(a, 0, nullptr, true); }
-
-cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream)
-{
-    return dispatch(a, grid, stream, false);
-}
-
-template <int TPW>
+template <int TPW, int NTF, int PPN>
 static int occupancy_t(const NewtonArgs &a)
 {
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, newton_kernel<TPW>, kThreads, a.smemBytes) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, newton_kernel<TPW, NTF, PPN>, kThreads,
+                                                      a.smemBytes) != cudaSuccess)
         return 1;
     return blocks < 1 ? 1 : blocks;
 }
 
-int newton_ctas_per_sm(const NewtonArgs &a)
+// Calls op.template run<TPW, NTF, PPN>() for the kernel instance of `a`.
+template <class Op>
+static auto with_instance(const NewtonArgs &a, Op op)
 {
+    if (a.ntf > 0) {
+        const bool ppn = a.momentType == 1;
+        if (a.ntf <= 4)
+            return ppn ? op.template run<1, 4, 1>() : op.template run<1, 4, 0>();
+        if (a.ntf <= 8)
+            return ppn ? op.template run<1, 8, 1>() : op.template run<1, 8, 0>();
+        if (a.ntf <= 12)
+            return ppn ? op.template run<1, 12, 1>() : op.template run<1, 12, 0>();
+        return ppn ? op.template run<1, 16, 1>() : op.template run<1, 16, 0>();
+    }
     if (a.tpw <= 1)
-        return occupancy_t<1>(a);
+        return op.template run<1, 0, 0>();
     if (a.tpw <= 2)
-        return occupancy_t<2>(a);
+        return op.template run<2, 0, 0>();
     if (a.tpw <= 4)
-        return occupancy_t<4>(a);
+        return op.template run<4, 0, 0>();
     if (a.tpw <= 8)
-        return occupancy_t<8>(a);
-    return occupancy_t<16>(a);
+        return op.template run<8, 0, 0>();
+    return op.template run<16, 0, 0>();
 }
+
+struct LaunchOp {
+    const NewtonArgs &a;
+    int grid;
+    cudaStream_t stream;
+    bool prepare;
+    template <int TPW, int NTF, int PPN>
+    cudaError_t run() const { return launch_t<TPW, NTF, PPN>(a, grid, stream, prepare); }
+};
+struct OccupancyOp {
+    const NewtonArgs &a;
+    template <int TPW, int NTF, int PPN>
+    int run() const { return occupancy_t<TPW, NTF, PPN>(a); }
+};
+
+cudaError_t prepare_newton(const NewtonArgs &a)
+{
+    if (a.ntf == 0 && a.tpw > 16)
+        return cudaErrorInvalidValue;
+    return with_instance(a, LaunchOp{a, 0, nullptr, true});
+}
+
+cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream)
+{
+    if (a.ntf == 0 && a.tpw > 16)
+        return cudaErrorInvalidValue;
+    return with_instance(a, LaunchOp{a, grid, stream, false});
+}
+
+int newton_ctas_per_sm(const NewtonArgs &a) { return with_instance(a, OccupancyOp{a}); }
 
 }  // namespace clb

@@ -11,7 +11,18 @@ namespace clb {
 //   [0, nb)              basis p_k, k < n (zero for n <= k < nb)
 //   [nb, nb + K2p)       Hessian columns: extended basis (Gaunt) or the
 //                        products p_i p_j, j <= i, at column i(i+1)/2 + j
-// with row stride ldP (ldP % 16 == 4 doubles, conflict-free fragments).
+// with row q at basis_row(q, ldP) = q * ldP + 4 * (q / 4): ldP % 16 == 4
+// doubles and a gap of 4 doubles after every 4 rows make both MMA fragment
+// patterns bank-conflict free, and a chunk of rows is one contiguous block
+// (copied to shared memory as is).  The gap after rows 4k..4k+3 holds their
+// quadrature weights w[4k..4k+3] (basis_wgap), so a staged chunk carries its
+// weights.  The array holds nqp * ldP + nqp doubles.
+__host__ __device__ __forceinline__ int basis_row(int q, int ldP) { return q * ldP + 4 * (q >> 2); }
+__host__ __device__ __forceinline__ int basis_wgap(int q, int ldP)
+{
+    return ((q >> 2) * 4 + 4) * ldP + 4 * (q >> 2) + (q & 3);
+}
+
 struct NewtonProblem {
     const double *P;
     const double *w;            // [nqp], zero on padded rows
@@ -52,10 +63,11 @@ struct NewtonArgs {
     int T, kq, ldv, ldE, ldG, ldh, ntq, doubleBuffer;
     int offAlpha, offAold, offD, offU, offScal, offInt, offFpart, offStat;
     int offP, offE, offEg, offG, offH, offVec;
-    int offEllVal, offEllIdx, offEllPair, offEllOff, offExp;
+    int offEllVal, offEllIdx, offEllPair, offEllOff, offExp, offBar;
     ExpConsts ex;               // table-driven exp constants (staged in shared memory)
     int smemBytes;
-    int tpw;
+    int tpw;                    // column tiles per warp (general contractions)
+    int ntf;                    // > 0: fused contractions with this many tiles per warp
 };
 
 // Fills the layout fields from the problems' sizes; returns 0 or -1 when

@@ -79,7 +79,7 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     const int nnz = gaunt ? ang->gaunt_nnz : 0;
     size_t off = kHeaderBytes;
     const size_t offP = off;
-    off = align_up(off + sizeof(double) * (size_t)nqp * ldP, 256);
+    off = align_up(off + sizeof(double) * ((size_t)nqp * ldP + nqp), 256);
     const size_t offW = off;
     off = align_up(off + sizeof(double) * (size_t)nqp, 256);
     const size_t offPairs = off;
@@ -135,7 +135,7 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     double *W = (double *)(g_stage + offW);
     for (int q = 0; q < nq; q++) {
         const double *pq = ang->p + (size_t)q * n2;
-        double *row = P + (size_t)q * ldP;
+        double *row = P + (size_t)basis_row(q, ldP);
         for (int k = 0; k < n; k++)
             row[k] = pq[k];
         if (gaunt) {
@@ -148,6 +148,7 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
                     row[nb + c++] = pq[i] * pq[j];
         }
         W[q] = ang->w[q];
+        P[(size_t)basis_wgap(q, ldP)] = ang->w[q];
     }
     unsigned short *pairs = (unsigned short *)(g_stage + offPairs);
     int c = 0;
