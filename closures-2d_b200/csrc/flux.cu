@@ -27,17 +27,18 @@ constexpr int IC = TX * TY;                // 256 interior cells (16 m16 tiles)
 constexpr int kFluxThreads = 512;          // 16 warps: one interior m-tile each
 constexpr int kFluxWarps = kFluxThreads / 32;
 constexpr int kQ = 16;                     // directions per chunk
+static_assert(kFluxWarps == kQ && TX == 16 && TY == 16, "stencil mapping: one warp per direction, 16 x 16 tile");
 constexpr double kSqrtPi = 1.7724538509055160273;
 
 __device__ __forceinline__ double minmod(double x, double y)
 {
-    // SIGN(1.0,x)*MAX(0.0, MIN(fabs(x), y*SIGN(1.0,x)))
-    double s = (x >= 0.0) ? 1.0 : -1.0;
-    double m = fabs(x);
-    double ys = y * s;
-    double mn = (m < ys) ? m : ys;
-    double mx = (0.0 > mn) ? 0.0 : mn;
-    return s * mx;
+    // SIGN(1.0,x)*MAX(0.0, MIN(fabs(x), y*SIGN(1.0,x))): the product by +-1
+    // is exact, so it is a sign select (the result carries the sign of x;
+    // only a zero result may differ in the sign of zero)
+    const bool pos = x >= 0.0;
+    const double ys = pos ? y : -y;
+    const double mx = fmax(0.0, fmin(fabs(x), ys));
+    return pos ? mx : -mx;
 }
 
 __device__ __forceinline__ double slopefit(double l, double c, double r, double th)
@@ -143,38 +144,62 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
             }
         }
         __syncthreads();
-        // 2. limited upwind stencil, one q per warp-item (uniform branches)
-        for (int item = warp; item < kq * (IC / 32); item += kFluxWarps) {
-            int q = item / (IC / 32), cg = item % (IC / 32);
-            int ic = cg * 32 + lane;
-            int ti = ic / TY, tj = ic % TY;
-            int h = (ti + 2) * HY + (tj + 2);
-            const double *a = sA + q * ldA;
+        // 2. limited upwind stencil.  Thread (q = warp, column j = lane % 16)
+        //    sweeps interior rows ib..ib+7 (ib = 8 * (lane / 16)) down its
+        //    column: the x-direction slopefit of a cell is formed once and
+        //    serves the cell's own face and its neighbour's, in the
+        //    reference's expression ((k3 +- sf/2) - k2) -+ sf'/2 (:145-188).
+        //    The 1/dx, 1/dy of F are folded into xi w / dx and eta w / dy.
+        {
+            const int q = warp;
+            const int j = lane & 15, ib = (lane >> 4) * 8;
+            const double *col = sA + q * ldA + (j + 2) + 2 * HY;   // col[i * HY] = ansatz of interior row i
             const double xi = Qb[q], eta = Qb[kq + q];
-            const double cx = Qb[2 * kq + q], cy = Qb[3 * kq + q];
+            const double cxd = Qb[2 * kq + q] / f.dx, cyd = Qb[3 * kq + q] / f.dy;
             const double th = f.theta;
-            double flux1 = 0, flux2 = 0, flux3 = 0, flux4 = 0;
+            double fx[8];
             if (xi > 0) {
-                double k1 = a[h - 2 * HY], k2 = a[h - HY], k3 = a[h], k4 = a[h + HY];
-                flux1 = k3 + 0.5 * slopefit(k2, k3, k4, th) - k2 - 0.5 * slopefit(k1, k2, k3, th);
-                flux1 = flux1 * cx;
+                // flux1(i) = ((k_i + sf_i / 2) - k_{i-1}) - sf_{i-1} / 2,
+                // sf_i = slopefit(k_{i-1}, k_i, k_{i+1})
+                double km1 = col[(ib - 1) * HY], k0 = col[ib * HY];
+                double sprev = slopefit(col[(ib - 2) * HY], km1, k0, th);
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    const double kp1 = col[(ib + r + 1) * HY];
+                    const double sc = slopefit(km1, k0, kp1, th);
+                    fx[r] = (((k0 + 0.5 * sc) - km1) - 0.5 * sprev) * cxd;
+                    sprev = sc;
+                    km1 = k0;
+                    k0 = kp1;
+                }
+            } else {
+                // flux2(i) = ((k_{i+1} - sf_{i+1} / 2) - k_i) + sf_i / 2
+                double k0 = col[ib * HY], kp1 = col[(ib + 1) * HY];
+                double scur = slopefit(col[(ib - 1) * HY], k0, kp1, th);
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    const double kp2 = col[(ib + r + 2) * HY];
+                    const double sn = slopefit(k0, kp1, kp2, th);
+                    fx[r] = (((kp1 - 0.5 * sn) - k0) + 0.5 * scur) * cxd;
+                    scur = sn;
+                    k0 = kp1;
+                    kp1 = kp2;
+                }
             }
-            if (xi < 0) {
-                double k1 = a[h - HY], k2 = a[h], k3 = a[h + HY], k4 = a[h + 2 * HY];
-                flux2 = k3 - 0.5 * slopefit(k2, k3, k4, th) - k2 + 0.5 * slopefit(k1, k2, k3, th);
-                flux2 = flux2 * cx;
+            double *out = sF + q * ldF + ib * TY + j;
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const double *row = col + (ib + r) * HY;
+                double fy;
+                if (eta > 0) {
+                    const double k1 = row[-2], k2 = row[-1], k3 = row[0], k4 = row[1];
+                    fy = ((k3 + 0.5 * slopefit(k2, k3, k4, th)) - k2) - 0.5 * slopefit(k1, k2, k3, th);
+                } else {
+                    const double k1 = row[-1], k2 = row[0], k3 = row[1], k4 = row[2];
+                    fy = ((k3 - 0.5 * slopefit(k2, k3, k4, th)) - k2) + 0.5 * slopefit(k1, k2, k3, th);
+                }
+                out[r * TY] = fx[r] + fy * cyd;
             }
-            if (eta > 0) {
-                double k1 = a[h - 2], k2 = a[h - 1], k3 = a[h], k4 = a[h + 1];
-                flux3 = k3 + 0.5 * slopefit(k2, k3, k4, th) - k2 - 0.5 * slopefit(k1, k2, k3, th);
-                flux3 = flux3 * cy;
-            }
-            if (eta < 0) {
-                double k1 = a[h - 1], k2 = a[h], k3 = a[h + 1], k4 = a[h + 2];
-                flux4 = k3 - 0.5 * slopefit(k2, k3, k4, th) - k2 + 0.5 * slopefit(k1, k2, k3, th);
-                flux4 = flux4 * cy;
-            }
-            sF[q * ldF + ic] = (flux1 + flux2) / f.dx + (flux3 + flux4) / f.dy;
         }
         __syncthreads();
         // 3. projection on the basis: flux[ic][k] += F[ic][q] p[q][k]
