@@ -30,20 +30,22 @@ constexpr int kQ = 16;                     // directions per chunk
 static_assert(kFluxWarps == kQ && TX == 16 && TY == 16, "stencil mapping: one warp per direction, 16 x 16 tile");
 constexpr double kSqrtPi = 1.7724538509055160273;
 
-__device__ __forceinline__ double minmod(double x, double y)
+// slopefit(l, c, r, theta) = minmod(theta (r - c), minmod((r - l) / 2,
+// theta (c - l))) with minmod(x, y) = SIGN(1,x) MAX(0, MIN(|x|, y SIGN(1,x)))
+// (momopt_update.cpp:77-90).  The nested form equals, exactly, sign(a)
+// min(|a|, |b|, |c|) when a, b, c share one sign and 0 otherwise (only the
+// sign of a zero result can differ); the sign test runs on the integer
+// high words.
+__device__ __forceinline__ double minmod3(double a, double b, double c)
 {
-    // SIGN(1.0,x)*MAX(0.0, MIN(fabs(x), y*SIGN(1.0,x))): the product by +-1
-    // is exact, so it is a sign select (the result carries the sign of x;
-    // only a zero result may differ in the sign of zero)
-    const bool pos = x >= 0.0;
-    const double ys = pos ? y : -y;
-    const double mx = fmax(0.0, fmin(fabs(x), ys));
-    return pos ? mx : -mx;
+    const double m = fmin(fabs(a), fmin(fabs(b), fabs(c)));
+    const int ha = __double2hiint(a), hb = __double2hiint(b), hc = __double2hiint(c);
+    return (((ha ^ hb) | (ha ^ hc)) >= 0) ? copysign(m, a) : 0.0;
 }
 
 __device__ __forceinline__ double slopefit(double l, double c, double r, double th)
 {
-    return minmod(th * (r - c), minmod(0.5 * (r - l), th * (c - l)));
+    return minmod3(th * (r - c), 0.5 * (r - l), th * (c - l));
 }
 
 __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_constant__ FluxArgs f)
@@ -146,9 +148,10 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         __syncthreads();
         // 2. limited upwind stencil.  Thread (q = warp, column j = lane % 16)
         //    sweeps interior rows ib..ib+7 (ib = 8 * (lane / 16)) down its
-        //    column: the x-direction slopefit of a cell is formed once and
-        //    serves the cell's own face and its neighbour's, in the
-        //    reference's expression ((k3 +- sf/2) - k2) -+ sf'/2 (:145-188).
+        //    column: each slopefit of a cell is formed once and serves the
+        //    cell's own face and its neighbour's (x: down the sweep, y: by a
+        //    lane shuffle), in the reference's expression
+        //    ((k3 +- sf/2) - k2) -+ sf'/2 (:145-188).
         //    The 1/dx, 1/dy of F are folded into xi w / dx and eta w / dy.
         {
             const int q = warp;
@@ -186,17 +189,33 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                     kp1 = kp2;
                 }
             }
+            // y direction: lane j forms sf_j of its row and takes sf_{j-1}
+            // (eta > 0) or sf_{j+1} (eta < 0) from its neighbour lane; the
+            // tile-edge ones (column -1 or 16) of rows ib..ib+7 are formed
+            // by lanes 0..7 of each half in one step
+            double edge = 0.0;
+            if (j < 8) {
+                const double *hr = sA + q * ldA + (ib + j + 2) * HY;   // halo row, column c at hr[c + 2]
+                edge = (eta > 0) ? slopefit(hr[0], hr[1], hr[2], th) : slopefit(hr[17], hr[18], hr[19], th);
+            }
             double *out = sF + q * ldF + ib * TY + j;
 #pragma unroll
             for (int r = 0; r < 8; r++) {
                 const double *row = col + (ib + r) * HY;
+                const double km = row[-1], k0 = row[0], kp = row[1];
+                const double sc = slopefit(km, k0, kp, th);
+                const double se = __shfl_sync(0xffffffffu, edge, r, 16);
                 double fy;
                 if (eta > 0) {
-                    const double k1 = row[-2], k2 = row[-1], k3 = row[0], k4 = row[1];
-                    fy = ((k3 + 0.5 * slopefit(k2, k3, k4, th)) - k2) - 0.5 * slopefit(k1, k2, k3, th);
+                    double sl = __shfl_up_sync(0xffffffffu, sc, 1, 16);
+                    if (j == 0)
+                        sl = se;
+                    fy = ((k0 + 0.5 * sc) - km) - 0.5 * sl;
                 } else {
-                    const double k1 = row[-1], k2 = row[0], k3 = row[1], k4 = row[2];
-                    fy = ((k3 - 0.5 * slopefit(k2, k3, k4, th)) - k2) + 0.5 * slopefit(k1, k2, k3, th);
+                    double sr = __shfl_down_sync(0xffffffffu, sc, 1, 16);
+                    if (j == 15)
+                        sr = se;
+                    fy = ((kp - 0.5 * sr) - k0) + 0.5 * sc;
                 }
                 out[r * TY] = fx[r] + fy * cyd;
             }
