@@ -105,13 +105,10 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
     load_chunk(0, 0);
     for (int c = 0; c < nchunks; c++) {
         const int buf = c & 1;
-        if (c + 1 < nchunks) {
-            load_chunk(c + 1, buf ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
+        cp_async_wait<0>();
+        __syncthreads();   // chunk c visible; every warp is done with chunk c - 1
+        if (c + 1 < nchunks)
+            load_chunk(c + 1, buf ^ 1);   // into the buffer chunk c - 1 used
         const double *Pb = sP + buf * kq * ldPf;
         const double *Qb = sQ + buf * 4 * kq;
         // 1. ansatz on the halo tile
@@ -233,7 +230,6 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 }
             }
         }
-        __syncthreads();
     }
 
     // epilogue: Euler + collision + source (+ Heun average)
