@@ -128,6 +128,32 @@ __device__ __forceinline__ void invert_regs(const double *Ls, int ldl, double (&
     }
 }
 
+// Rigorous upper bound of ||L^-1||_inf ||L^-1||_1 from the comparison matrix
+// M(L) (|L_ii| on the diagonal, -|L_ik| below): |L^-1| <= M(L)^-1 entrywise,
+// so ||L^-1||_inf <= ||M(L)^-1 e||_inf and ||L^-1||_1 <= ||M(L)^-T e||_inf.
+// The two substitutions (nonnegative terms only) run interleaved; factor rows
+// come from h[] (lane i: L_ik) and Ls (1/L_kk on the diagonal, as left by
+// chol_regs).  Used where it is tight: Hessians of smooth cells.
+__device__ __forceinline__ double cmp_bound(const double (&h)[kMaxN], const double *Ls, int ldl, int n, int lane)
+{
+    const double rl = (lane < n) ? Ls[lane * ldl + lane] : 0.0;
+    double accF = 0.0, accB = 0.0;
+#pragma unroll
+    for (int s = 0; s < kMaxN; s++) {
+        if (s < n) {
+            const int kf = s, kb = n - 1 - s;
+            const double xf = __shfl_sync(0xffffffffu, (1.0 + accF) * rl, kf);
+            const double xb = __shfl_sync(0xffffffffu, (1.0 + accB) * rl, kb);
+            if (lane > kf)   // h[k] holds L_lane,k only for k <= lane
+                accF = fma(fabs(h[s]), xf, accF);
+            if (lane < kb)
+                accB = fma(fabs(Ls[kb * ldl + lane]), xb, accB);
+        }
+    }
+    const double x = (lane < n) ? (1.0 + accF) * rl : 0.0, y = (lane < n) ? (1.0 + accB) * rl : 0.0;
+    return warp_max(x) * warp_max(y);
+}
+
 // z = (L L^T)^-1 x with Linv in Hs; x, z held one element per lane.
 __device__ double apply_inv(const double *Hs, int n, int ldh, double *vec, double x, int lane)
 {
@@ -417,6 +443,30 @@ __device__ double modcfl(double di, int n, int lane, int momentType)
     return momentType == 0 ? exp(2.0 * da1 * minf) : 1.0 + 2.0 * da1 * minf;
 }
 
+// Converged (opt.cpp:293-306): Mn write-back of the realised moments, then
+// opt()'s rescaling (:107-109, :133-138), and the slot is finished.
+__device__ void converge(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, double ui, double ai,
+                         double gi, int lane)
+{
+    const double *sc = L.scal + s * SC_N;
+    double uo = ui, ao = ai;
+    const double u0 = sc[SC_U0];
+    if (a.momentType == 0) {
+        double u0w = __shfl_sync(0xffffffffu, ui + gi, 0);
+        uo = (ui + gi) / u0w;
+        if (lane == 0)
+            ao = ai - log(u0w) * 2.0 * kSqrtPi;
+        uo = uo * u0;
+        if (lane == 0)
+            ao = ao + sc[SC_ASCALE];
+    } else {
+        ao = ai * u0;
+        uo = ui * u0;
+    }
+    __syncwarp();
+    finish_slot(a, pb, L, s, uo, ao, 0, lane);
+}
+
 // Newton logic for one slot after its evaluation (warp-wide).
 __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
                            int warp)
@@ -529,8 +579,33 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         rowsum += fabs(h[k]);
     }
     const double anorm = warp_max(rowsum);
+    // Converged at this evaluation with no regularisation due (most cells of
+    // a time step, which start at the previous step's multipliers).  The
+    // reference still factors H and estimates its condition number before
+    // its stopping test; a rigorous bound that shows cond <= MOMOPT_COND_H_MAX
+    // (factor-2 margin for rounding) fixes the same outcome, and neither the
+    // inverse nor the direction is needed (without the gamma test).
+    //  tier 0: H strictly diagonally dominant with positive diagonal:
+    //          ||H^-1||_1 = ||H^-1||_inf <= 1 / min_i (H_ii - sum_j!=i |H_ij|)
+    //          (Varah 1975); such H is SPD and its Cholesky factorisation
+    //          cannot break down, so the factorisation is not needed either;
+    //  tier 1: after the factorisation, the comparison-matrix bound.
+    const double err = sqrt(warp_sum(gi * gi));
+    const bool convTest = err <= sc[SC_RTOL] && !(a.tolGamma > 0.0) && iter < si[SI_MAXITER] && sc[SC_T] != 0.0;
+    if (convTest) {
+        const double dom = act ? 2.0 * Hs[lane * ldh + lane] - rowsum : DBL_MAX;
+        const double delta = -warp_max(-dom);
+        if (delta > 0.0 && anorm <= 0.5 * a.condHMax * delta) {
+            converge(a, pb, L, s, ui, ai, gi, lane);
+            return;
+        }
+    }
     __syncwarp();
     int info = chol_regs(h, Hs, ldh, n, lane);
+    if (info == 0 && convTest && anorm * cmp_bound(h, Hs, ldh, n, lane) <= 0.5 * a.condHMax) {
+        converge(a, pb, L, s, ui, ai, gi, lane);
+        return;
+    }
     double condest = 0.0;
     if (info == 0) {
         // column `lane` of L^-1 in v[], rows of L^-1 in Hs
@@ -585,28 +660,11 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         }
     }
     const double di = act ? -z : 0.0;
-    const double err = sqrt(warp_sum(gi * gi));
     bool gammaOk = true;
     if (a.tolGamma > 0.0)
         gammaOk = modcfl(di, n, lane, a.momentType) <= a.tolGamma;
     if (err <= sc[SC_RTOL] && gammaOk) {
-        // converged (opt.cpp:293-306), then opt()'s rescaling (:107-109, :133-138)
-        double uo = ui, ao = ai;
-        const double u0 = sc[SC_U0];
-        if (a.momentType == 0) {
-            double u0w = __shfl_sync(0xffffffffu, ui + gi, 0);
-            uo = (ui + gi) / u0w;
-            if (lane == 0)
-                ao = ai - log(u0w) * 2.0 * kSqrtPi;
-            uo = uo * u0;
-            if (lane == 0)
-                ao = ao + sc[SC_ASCALE];
-        } else {
-            ao = ai * u0;
-            uo = ui * u0;
-        }
-        __syncwarp();
-        finish_slot(a, pb, L, s, uo, ao, 0, lane);
+        converge(a, pb, L, s, ui, ai, gi, lane);
         return;
     }
     // line search set-up (linesearch.cpp:21-52)
