@@ -1,1156 +1,11 @@
-// newton.cu -- persistent dual-Newton kernel for the Mn / PPn entropy closure.
-//
-// One launch solves, for every vector u of every problem, the dual problem of
-// opt() (src/momopt/opt/opt.cpp:82-343): minimise <eta*(alpha.m)> - alpha.u by
-// Newton's method with the Armijo backtracking line search of
-// linesearch.cpp:21-99 and the isotropic-restart regularisation ladder
-// r in {0, 1e-3, 1e-2, 1e-1, 0.5} (opt.h:39-40, opt.cpp:244-274).
-//
-// B200 mapping.  A CTA owns T "slots" (cells in flight).  Each round every
-// slot needs one evaluation of f, g and H at its current alpha; the rounds are
-// batched contractions over the quadrature on the FP64 tensor cores (DMMA
-// m16n8k8):
-//   S[T x kq]  = alpha[T x nb] . P[kq x nb]^T            (alpha.m per q)
-//   E          = w * exp(S)          (Mn)   or the PPn weights
-//   G[T x K]  += E[T x kq] . Phess[kq x K]               (Hessian columns)
-// with the basis streamed through shared memory in q-chunks by cp.async.
-// Then one warp per slot finishes the Newton logic in FP64: H from G (the
-// Gaunt contraction of fobj.cpp:130-144 or the packed products), Cholesky,
-// Hager/Higham 1-norm condition estimate (the quantity dpocon returns),
-// direction, stopping test, line-search bookkeeping and the ladder.
-// Converged slots write u, alpha back and are refilled from a global work
-// counter, so vectors needing 1 or 40 iterations share the launch.
-//
-// Every line-search trial evaluation also carries H: when the trial is
-// accepted (the usual case) it is reused as the next Newton iteration's
-// evaluation, which the reference recomputes at the same alpha.
+// newton.cu -- launch planning and instance selection of the persistent
+// dual-Newton kernel (device code in newton_kernel.cuh).
 #include "newton.cuh"
 
 #include <cfloat>
 #include <cmath>
 
 namespace clb {
-
-namespace {
-
-enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
-enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_N };
-enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_N };
-
-constexpr double kSqrtPi = 1.7724538509055160273;
-constexpr double kPi = 3.14159265358979323846;
-
-struct Ctx {
-    double *sm;
-    int lane, warp, g, t4;
-};
-
-__device__ __forceinline__ void record_error(int *err, int code, int idx)
-{
-    if (atomicCAS(&err[0], 0, code) == 0)
-        err[1] = idx;
-}
-
-// Cholesky of the symmetric matrix whose row `lane` is h[] (registers), in
-// the dot-product (Crout) form by columns: lane i >= j forms
-// L_ij = (H_ij - sum_k<j L_ik L_jk) / L_jj.  Row j of L is read back from the
-// warp's shared-memory matrix Ls (stride ldl, even) with 16-byte broadcast
-// loads: lane i writes L_ij there at step j, and 1/L_jj on the diagonal.
-// On return h[k] = L_lane,k for k <= lane.  LAPACK-style info: 0, or j+1 at
-// the first non-positive or NaN pivot (dpotrf semantics).
-__device__ __forceinline__ int chol_regs(double (&h)[kMaxN], double *Ls, int ldl, int n, int lane)
-{
-#pragma unroll
-    for (int j = 0; j < kMaxN; j++) {
-        if (j < n) {
-            const double *Lj = Ls + j * ldl;
-            double s0 = h[j], s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll
-            for (int k = 0; k + 1 < j; k += 2) {
-                const double2 l = *reinterpret_cast<const double2 *>(Lj + k);
-                if (k & 2) {
-                    s2 = fma(-h[k], l.x, s2);
-                    s3 = fma(-h[k + 1], l.y, s3);
-                } else {
-                    s0 = fma(-h[k], l.x, s0);
-                    s1 = fma(-h[k + 1], l.y, s1);
-                }
-            }
-            if (j & 1)
-                s1 = fma(-h[j - 1], Lj[j - 1], s1);
-            const double s = (s0 + s1) + (s2 + s3);
-            const double djj = __shfl_sync(0xffffffffu, s, j);
-            if (!(djj > 0.0))
-                return j + 1;
-            const double r = rsqrt(djj);
-            if (lane == j) {
-                h[j] = djj * r;
-                Ls[j * ldl + j] = r;
-            } else if (lane > j && lane < n) {
-                h[j] = s * r;
-                Ls[lane * ldl + j] = h[j];
-            }
-            __syncwarp();
-        }
-    }
-    return 0;
-}
-
-// Column `lane` of L^-1 into v[]: Linv_ic = -(sum_{k=c}^{i-1} L_ik Linv_kc) / L_ii,
-// rows in order, row i of L and 1/L_ii read from Ls as left by chol_regs.
-__device__ __forceinline__ void invert_regs(const double *Ls, int ldl, double (&v)[kMaxN], int n, int lane)
-{
-#pragma unroll
-    for (int i = 0; i < kMaxN; i++) {
-        v[i] = 0.0;
-        if (i < n) {
-            const double *Li = Ls + i * ldl;
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll
-            for (int k = 0; k + 1 < i; k += 2) {
-                const double2 l = *reinterpret_cast<const double2 *>(Li + k);
-                if (k & 2) {
-                    a2 = fma(l.x, v[k], a2);
-                    a3 = fma(l.y, v[k + 1], a3);
-                } else {
-                    a0 = fma(l.x, v[k], a0);
-                    a1 = fma(l.y, v[k + 1], a1);
-                }
-            }
-            if (i & 1)
-                a1 = fma(Li[i - 1], v[i - 1], a1);
-            const double rinv = Li[i];
-            if (lane == i)
-                v[i] = rinv;
-            else if (lane < i)
-                v[i] = -((a0 + a1) + (a2 + a3)) * rinv;
-        }
-    }
-}
-
-// Rigorous upper bound of ||L^-1||_inf ||L^-1||_1 from the comparison matrix
-// M(L) (|L_ii| on the diagonal, -|L_ik| below): |L^-1| <= M(L)^-1 entrywise,
-// so ||L^-1||_inf <= ||M(L)^-1 e||_inf and ||L^-1||_1 <= ||M(L)^-T e||_inf.
-// The two substitutions (nonnegative terms only) run interleaved; factor rows
-// come from h[] (lane i: L_ik) and Ls (1/L_kk on the diagonal, as left by
-// chol_regs).  Used where it is tight: Hessians of smooth cells.
-__device__ __forceinline__ double cmp_bound(const double (&h)[kMaxN], const double *Ls, int ldl, int n, int lane)
-{
-    const double rl = (lane < n) ? Ls[lane * ldl + lane] : 0.0;
-    double accF = 0.0, accB = 0.0;
-#pragma unroll
-    for (int s = 0; s < kMaxN; s++) {
-        if (s < n) {
-            const int kf = s, kb = n - 1 - s;
-            const double xf = __shfl_sync(0xffffffffu, (1.0 + accF) * rl, kf);
-            const double xb = __shfl_sync(0xffffffffu, (1.0 + accB) * rl, kb);
-            if (lane > kf)   // h[k] holds L_lane,k only for k <= lane
-                accF = fma(fabs(h[s]), xf, accF);
-            if (lane < kb)
-                accB = fma(fabs(Ls[kb * ldl + lane]), xb, accB);
-        }
-    }
-    const double x = (lane < n) ? (1.0 + accF) * rl : 0.0, y = (lane < n) ? (1.0 + accB) * rl : 0.0;
-    return warp_max(x) * warp_max(y);
-}
-
-// z = (L L^T)^-1 x with Linv in Hs; x, z held one element per lane.
-__device__ double apply_inv(const double *Hs, int n, int ldh, double *vec, double x, int lane)
-{
-    __syncwarp();
-    vec[lane] = x;
-    __syncwarp();
-    double y = 0.0;
-    if (lane < n)
-        for (int k = 0; k <= lane; k++)
-            y = fma(Hs[lane * ldh + k], vec[k], y);
-    __syncwarp();
-    vec[lane] = y;
-    __syncwarp();
-    double z = 0.0;
-    if (lane < n)
-        for (int k = lane; k < n; k++)
-            z = fma(Hs[k * ldh + lane], vec[k], z);
-    return z;
-}
-
-__device__ __forceinline__ double sgn1(double x) { return x >= 0.0 ? 1.0 : -1.0; }
-
-// Estimate of ||A^-1||_1 for A = L L^T (Higham 1988, Alg. 4.1, the estimator
-// behind LAPACK dlacn2/dpocon); returns rcond = (1/est)/anorm.
-__device__ double rcond_warp(const double *Hs, int n, int ldh, double *vec, double anorm, int lane)
-{
-    const bool act = lane < n;
-    if (anorm == 0.0)
-        return 0.0;
-    double x = act ? 1.0 / n : 0.0;
-    x = apply_inv(Hs, n, ldh, vec, x, lane);
-    double est;
-    if (n == 1) {
-        est = fabs(__shfl_sync(0xffffffffu, x, 0));
-    } else {
-        est = warp_sum(act ? fabs(x) : 0.0);
-        double isgn = act ? sgn1(x) : 0.0;
-        x = apply_inv(Hs, n, ldh, vec, isgn, lane);
-        int j = warp_argmax_first(act ? fabs(x) : -1.0, lane);
-        int iter = 2;
-        for (;;) {
-            x = (lane == j) ? 1.0 : 0.0;
-            x = apply_inv(Hs, n, ldh, vec, x, lane);
-            double estold = est;
-            est = warp_sum(act ? fabs(x) : 0.0);
-            bool same = __all_sync(0xffffffffu, !act || sgn1(x) == isgn);
-            if (same || est <= estold)
-                break;
-            isgn = act ? sgn1(x) : 0.0;
-            x = apply_inv(Hs, n, ldh, vec, isgn, lane);
-            int jlast = j;
-            j = warp_argmax_first(act ? fabs(x) : -1.0, lane);
-            double xjlast = __shfl_sync(0xffffffffu, x, jlast);
-            double xj = __shfl_sync(0xffffffffu, x, j);
-            if (xjlast != fabs(xj) && iter < 5) {
-                iter++;
-                continue;
-            }
-            break;
-        }
-        double alt = act ? ((lane & 1) ? -1.0 : 1.0) * (1.0 + (double)lane / (double)(n - 1)) : 0.0;
-        alt = apply_inv(Hs, n, ldh, vec, alt, lane);
-        double temp = 2.0 * (warp_sum(act ? fabs(alt) : 0.0) / (3.0 * n));
-        if (temp > est)
-            est = temp;
-    }
-    if (est != 0.0)
-        return (1.0 / est) / anorm;
-    return 0.0;
-}
-
-struct Layout {
-    double *alpha, *aold, *d, *u, *scal, *fpart, *P, *E, *Eg, *G, *H, *vec;
-    int *ints;
-    unsigned long long *stat;
-    double *ellVal;
-    unsigned short *ellIdx, *ellPair;
-    int *ellOff;
-    double *exptab;
-    unsigned long long *bar;   // three mbarriers of the staged basis chunks
-};
-
-__device__ __forceinline__ Layout make_layout(double *sm, const NewtonArgs &a)
-{
-    Layout L;
-    L.alpha = sm + a.offAlpha;
-    L.aold = sm + a.offAold;
-    L.d = sm + a.offD;
-    L.u = sm + a.offU;
-    L.scal = sm + a.offScal;
-    L.ints = (int *)(sm + a.offInt);
-    L.fpart = sm + a.offFpart;
-    L.stat = (unsigned long long *)(sm + a.offStat);
-    L.P = sm + a.offP;
-    L.E = sm + a.offE;
-    L.Eg = sm + a.offEg;
-    L.G = sm + a.offG;
-    L.H = sm + a.offH;
-    L.vec = sm + a.offVec;
-    L.ellVal = sm + a.offEllVal;
-    L.ellIdx = (unsigned short *)(sm + a.offEllIdx);
-    L.ellPair = (unsigned short *)(sm + a.offEllPair);
-    L.ellOff = (int *)(sm + a.offEllOff);
-    L.exptab = sm + a.offExp;
-    L.bar = (unsigned long long *)(sm + a.offBar);
-    return L;
-}
-
-// Writes the finished slot's results (scaled back) and updates CTA stats.
-__device__ void finish_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s,
-                            double ui, double ai, int status, int lane)
-{
-    int cell = L.ints[s * SI_N + SI_CELL];
-    int n = pb.n;
-    if (lane < n) {
-        pb.u[(size_t)cell * n + lane] = ui;
-        pb.alpha[(size_t)cell * n + lane] = ai;
-    }
-    if (lane == 0) {
-        int total = L.ints[s * SI_N + SI_TOTAL];
-        int reg = L.ints[s * SI_N + SI_REG];
-        if (pb.iters)
-            pb.iters[cell] = total;
-        if (pb.regs)
-            pb.regs[cell] = kRegularizations[reg];
-        if (pb.status)
-            pb.status[cell] = status;
-        if (status == 0) {
-            atomicAdd(&L.stat[reg], 1ull);
-            atomicAdd(&L.stat[kNumReg], (unsigned long long)total);
-            atomicAdd(&L.stat[kNumReg + 1], 1ull);
-            atomicMax((int *)&L.stat[kStatU64], total);
-        } else {
-            record_error(a.err, status, cell);
-        }
-        L.ints[s * SI_N + SI_STATE] = S_IDLE;
-    }
-}
-
-// Loads and scales a newly assigned vector (opt.cpp:82-148 entry half).
-__device__ void init_slot(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
-                          int ldv)
-{
-    const int n = pb.n;
-    const int cell = L.ints[s * SI_N + SI_CELL];
-    double ui = 0.0, ai = 0.0;
-    int pred = 0;
-    if (lane < n) {
-        ui = pb.u[(size_t)cell * n + lane];
-        ai = pb.alpha[(size_t)cell * n + lane];
-    }
-    if (pb.alphaStart != nullptr) {
-        double ap = (lane < n) ? pb.alphaStart[(size_t)cell * n + lane] : 0.0;
-        if (__all_sync(0xffffffffu, isfinite(ap))) {
-            ai = ap;
-            pred = 1;
-        }
-    }
-    if (a.momentsOld != nullptr && lane < n) {
-        int i = cell / a.NY, j = cell % a.NY;
-        if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
-            a.momentsOld[(size_t)cell * n + lane] = ui;
-    }
-    const double u0 = __shfl_sync(0xffffffffu, ui, 0);
-    if (!(u0 > 0.0)) {
-        // opt.cpp:97-101 aborts; leave the vector untouched and report.
-        if (lane == 0) {
-            L.ints[s * SI_N + SI_TOTAL] = 0;
-            L.ints[s * SI_N + SI_REG] = 0;
-        }
-        __syncwarp();
-        finish_slot(a, pb, L, s, ui, ai, -3, lane);
-        return;
-    }
-    double *sc = L.scal + s * SC_N;
-    double delta = a.deltaPPn;
-    if (a.momentType == 0) {
-        double ascale = log(u0) * 2.0 * kSqrtPi;
-        if (lane == 0)
-            ai = ai - ascale;
-        ui = ui / u0;
-        if (lane == 0)
-            sc[SC_ASCALE] = ascale;
-    } else {
-        ai = ai / u0;
-        ui = ui / u0;
-        delta = delta / (u0 * u0);
-    }
-    if (lane < ldv) {
-        L.u[s * ldv + lane] = (lane < n) ? ui : 0.0;
-        L.alpha[s * ldv + lane] = (lane < n) ? ai : 0.0;
-    }
-    double rtol = sqrt(warp_sum(ui * ui)) * a.tolRel;
-    if (lane == 0) {
-        sc[SC_T] = 1.0;
-        sc[SC_RTOL] = rtol;
-        sc[SC_U0] = u0;
-        sc[SC_DELTA] = delta;
-        int *si = L.ints + s * SI_N;
-        si[SI_ITER] = 0;
-        si[SI_TOTAL] = 0;
-        si[SI_REG] = 0;
-        si[SI_MAXITER] = a.maxIter;
-        si[SI_PRED] = pred;
-        si[SI_STATE] = S_NEWTON;
-    }
-}
-
-// Isotropic restart with the next regularisation (opt.cpp:244-274).
-__device__ void regularize(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
-                           int ldv, double ui, double ai)
-{
-    const int n = pb.n;
-    int *si = L.ints + s * SI_N;
-    double *sc = L.scal + s * SC_N;
-    int reg = si[SI_REG];
-    if (si[SI_PRED] == 1) {
-        // The predicted start failed (the solve would regularise): restart
-        // once from the fallback start with the same u, as plain Newton.
-        const int cell = si[SI_CELL];
-        double af = (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0;
-        const double u0 = sc[SC_U0];
-        if (a.momentType == 0) {
-            if (lane == 0)
-                af = af - sc[SC_ASCALE];
-        } else {
-            af = af / u0;
-        }
-        if (lane < n)
-            L.alpha[s * ldv + lane] = af;
-        __syncwarp();
-        if (lane == 0) {
-            si[SI_PRED] = 2;
-            si[SI_ITER] = 0;
-            sc[SC_T] = 1.0;
-            si[SI_STATE] = S_NEWTON;
-            atomicAdd(&L.stat[kNumReg + 3], 1ull);
-        }
-        return;
-    }
-    if (reg >= kNumReg - 1) {
-        // opt.cpp:256-261 aborts; report and return the unscaled state.
-        double u0 = sc[SC_U0];
-        if (a.momentType == 0) {
-            ui *= u0;
-            if (lane == 0)
-                ai += sc[SC_ASCALE];
-        } else {
-            ui *= u0;
-            ai *= u0;
-        }
-        __syncwarp();
-        finish_slot(a, pb, L, s, ui, ai, -4, lane);
-        return;
-    }
-    reg++;
-    const double r = kRegularizations[reg];
-    const int cell = si[SI_CELL];
-    const double u0 = sc[SC_U0];
-    double unew = 0.0;
-    if (lane < n) {
-        double uorig = pb.u[(size_t)cell * n + lane] / u0;   // scaled original (unchanged in memory)
-        unew = (lane == 0) ? 1.0 : uorig * (1.0 - r);
-        L.u[s * ldv + lane] = unew;
-        double a0 = (a.momentType == 0) ? 2.0 * kSqrtPi * log(0.5 / kSqrtPi)
-                                        : 1.0 - 4.0 * sc[SC_DELTA] * kPi;
-        L.alpha[s * ldv + lane] = (lane == 0) ? a0 : 0.0;
-    }
-    double rtol = sqrt(warp_sum(unew * unew)) * a.tolRel;
-    __syncwarp();
-    if (lane == 0) {
-        si[SI_REG] = reg;
-        si[SI_ITER] = 0;
-        sc[SC_T] = 1.0;
-        sc[SC_RTOL] = rtol;
-        if (reg == kNumReg - 1)
-            si[SI_MAXITER] = 10 * si[SI_MAXITER];
-        si[SI_STATE] = S_NEWTON;
-    }
-}
-
-__device__ double modcfl(double di, int n, int lane, int momentType)
-{
-    double da1 = warp_sum(lane < n ? fabs(di) : 0.0);
-    int pnOrder = (int)floor(sqrt((double)n)) + 1;
-    double minf = sqrt((2 * pnOrder + 1) / (2 * kPi));
-    return momentType == 0 ? exp(2.0 * da1 * minf) : 1.0 + 2.0 * da1 * minf;
-}
-
-// Converged (opt.cpp:293-306): Mn write-back of the realised moments, then
-// opt()'s rescaling (:107-109, :133-138), and the slot is finished.
-__device__ void converge(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, double ui, double ai,
-                         double gi, int lane)
-{
-    const double *sc = L.scal + s * SC_N;
-    double uo = ui, ao = ai;
-    const double u0 = sc[SC_U0];
-    if (a.momentType == 0) {
-        double u0w = __shfl_sync(0xffffffffu, ui + gi, 0);
-        uo = (ui + gi) / u0w;
-        if (lane == 0)
-            ao = ai - log(u0w) * 2.0 * kSqrtPi;
-        uo = uo * u0;
-        if (lane == 0)
-            ao = ao + sc[SC_ASCALE];
-    } else {
-        ao = ai * u0;
-        uo = ui * u0;
-    }
-    __syncwarp();
-    finish_slot(a, pb, L, s, uo, ao, 0, lane);
-}
-
-// Newton logic for one slot after its evaluation (warp-wide).
-__device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
-                           int warp)
-{
-    const int n = pb.n;
-    const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
-    const bool act = lane < n;
-    int *si = L.ints + s * SI_N;
-    double *sc = L.scal + s * SC_N;
-    double *Hs = L.H + warp * (kMaxN * ldh);
-    double *vec = L.vec + warp * 64;
-    const double *Gs = L.G + s * ldG;
-    const int npairs = n * (n + 1) / 2;
-
-    // H from the contraction results (fobj.cpp:129-155)
-    if (a.useGaunt) {
-        for (int c = 0; c < pb.ellChunks; c++) {
-            const unsigned short pr = L.ellPair[c * 32 + lane];
-            const int e1 = L.ellOff[c + 1];
-            int e = L.ellOff[c];
-            double v = 0.0;
-            // loads of four entries issued ahead of their (in-order) sum
-            for (; e + 4 <= e1; e += 4) {
-                const int i0 = L.ellIdx[e * 32 + lane], i1 = L.ellIdx[(e + 1) * 32 + lane];
-                const int i2 = L.ellIdx[(e + 2) * 32 + lane], i3 = L.ellIdx[(e + 3) * 32 + lane];
-                const double w0 = L.ellVal[e * 32 + lane], w1 = L.ellVal[(e + 1) * 32 + lane];
-                const double w2 = L.ellVal[(e + 2) * 32 + lane], w3 = L.ellVal[(e + 3) * 32 + lane];
-                const double g0 = Gs[i0], g1 = Gs[i1], g2 = Gs[i2], g3 = Gs[i3];
-                v += w0 * g0;
-                v += w1 * g1;
-                v += w2 * g2;
-                v += w3 * g3;
-            }
-            for (; e < e1; e++)
-                v += L.ellVal[e * 32 + lane] * Gs[L.ellIdx[e * 32 + lane]];
-            if (pr != 0xFFFF) {
-                int i = pr >> 8, j = pr & 255;
-                Hs[i * ldh + j] = v;
-                Hs[j * ldh + i] = v;
-            }
-        }
-    } else {
-        for (int pi = lane; pi < npairs; pi += 32) {
-            unsigned short pr = pb.pairs[pi];
-            int i = pr >> 8, j = pr & 255;
-            double v = Gs[pi];
-            Hs[i * ldh + j] = v;
-            Hs[j * ldh + i] = v;
-        }
-    }
-    __syncwarp();
-
-    const double ui = act ? L.u[s * ldv + lane] : 0.0;
-    const double ai = act ? L.alpha[s * ldv + lane] : 0.0;
-    double gi;
-    if (a.momentType == 0)
-        gi = act ? Hs[lane] / pb.p0 - ui : 0.0;     // fobj.cpp:303-306
-    else
-        gi = act ? Gs[pb.K2p + lane] - ui : 0.0;    // fobj.cpp:427-431 / :445-452
-    const double au = warp_sum(ai * ui);
-    double fpart = 0.0;
-    for (int k = 0; k < a.ntq; k++)
-        fpart += L.fpart[s * a.ntq + k];
-    const double fsum = fpart - au;                  // no-Hessian f (linesearch's fobj)
-    const double fH = (a.momentType == 0) ? Hs[0] / (pb.p0 * pb.p0) - au : fsum;
-
-    int state = si[SI_STATE];
-    if (state == S_TRIAL) {
-        if (lane == 0)
-            atomicAdd(&L.stat[kNumReg + 2], 1ull);
-        double t = sc[SC_T];
-        if (!(fsum <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD])) {
-            t = 0.5 * t;
-            double ao = act ? L.aold[s * ldv + lane] : 0.0;
-            if (t * sc[SC_MAXF] > DBL_EPSILON / 2) {
-                if (act)
-                    L.alpha[s * ldv + lane] = ao + t * L.d[s * ldv + lane];
-                __syncwarp();
-                if (lane == 0)
-                    sc[SC_T] = t;
-                return;
-            }
-            // backtracked all the way (linesearch.cpp:84-98): alpha restored,
-            // the next iteration regularises because t == 0.
-            __syncwarp();
-            if (lane == 0) {
-                si[SI_ITER] += 1;
-                si[SI_TOTAL] += 1;
-            }
-            __syncwarp();
-            regularize(a, pb, L, s, lane, ldv, ui, ao);
-            return;
-        }
-        // accepted: this evaluation is the next Newton iteration's (opt.cpp:262-274)
-    }
-
-    // one Newton iteration (opt.cpp:258-368)
-    const int iter = si[SI_ITER] + 1;
-    __syncwarp();
-    if (lane == 0) {
-        si[SI_ITER] = iter;
-        si[SI_TOTAL] += 1;
-    }
-    // row `lane` of H in registers; utils_norm1 = max absolute row sum
-    double h[kMaxN], v[kMaxN];
-    double rowsum = 0.0;
-#pragma unroll
-    for (int k = 0; k < kMaxN; k++) {
-        h[k] = (act && k < n) ? Hs[lane * ldh + k] : 0.0;
-        rowsum += fabs(h[k]);
-    }
-    const double anorm = warp_max(rowsum);
-    // Converged at this evaluation with no regularisation due (most cells of
-    // a time step, which start at the previous step's multipliers).  The
-    // reference still factors H and estimates its condition number before
-    // its stopping test; a rigorous bound that shows cond <= MOMOPT_COND_H_MAX
-    // (factor-2 margin for rounding) fixes the same outcome, and neither the
-    // inverse nor the direction is needed (without the gamma test).
-    //  tier 0: H strictly diagonally dominant with positive diagonal:
-    //          ||H^-1||_1 = ||H^-1||_inf <= 1 / min_i (H_ii - sum_j!=i |H_ij|)
-    //          (Varah 1975); such H is SPD and its Cholesky factorisation
-    //          cannot break down, so the factorisation is not needed either;
-    //  tier 1: after the factorisation, the comparison-matrix bound.
-    const double err = sqrt(warp_sum(gi * gi));
-    const bool convTest = err <= sc[SC_RTOL] && !(a.tolGamma > 0.0) && iter < si[SI_MAXITER] && sc[SC_T] != 0.0;
-    if (convTest) {
-        const double dom = act ? 2.0 * Hs[lane * ldh + lane] - rowsum : DBL_MAX;
-        const double delta = -warp_max(-dom);
-        if (delta > 0.0 && anorm <= 0.5 * a.condHMax * delta) {
-            converge(a, pb, L, s, ui, ai, gi, lane);
-            return;
-        }
-    }
-    __syncwarp();
-    int info = chol_regs(h, Hs, ldh, n, lane);
-    if (info == 0 && convTest && anorm * cmp_bound(h, Hs, ldh, n, lane) <= 0.5 * a.condHMax) {
-        converge(a, pb, L, s, ui, ai, gi, lane);
-        return;
-    }
-    double condest = 0.0;
-    if (info == 0) {
-        // column `lane` of L^-1 in v[], rows of L^-1 in Hs
-        invert_regs(Hs, ldh, v, n, lane);
-        __syncwarp();
-        double colsum = 0.0;
-#pragma unroll
-        for (int i = 0; i < kMaxN; i++) {
-            if (i < n && act)
-                Hs[i * ldh + lane] = v[i];
-            colsum += fabs(v[i]);
-        }
-        __syncwarp();
-        double rs = 0.0;
-        if (act)
-            for (int c = 0; c <= lane; c++)
-                rs += fabs(Hs[lane * ldh + c]);
-        // ||A^-1||_1 <= ||L^-1||_1 ||L^-1||_inf, and the Higham estimate never
-        // exceeds ||A^-1||_1: when the bound already shows cond <= COND_H_MAX
-        // (with a factor-2 margin for rounding) the estimate cannot trigger
-        // regularisation and is not needed.
-        const double bound = anorm * warp_max(colsum) * warp_max(rs);
-        if (!(bound <= 0.5 * a.condHMax)) {
-            double rc = rcond_warp(Hs, n, ldh, vec, anorm, lane);
-            condest = 1.0 / rc;
-        }
-    }
-    if (iter >= si[SI_MAXITER] || info != 0 || sc[SC_T] == 0.0 || condest > a.condHMax) {
-        __syncwarp();
-        regularize(a, pb, L, s, lane, ldv, ui, ai);
-        return;
-    }
-    // d = -L^-T (L^-1 g): rows of L^-1 from Hs, columns from registers
-    __syncwarp();
-    vec[lane] = gi;
-    __syncwarp();
-    double y = 0.0;
-    if (act)
-        for (int c = 0; c <= lane; c++)
-            y = fma(Hs[lane * ldh + c], vec[c], y);
-    __syncwarp();
-    vec[32 + lane] = y;
-    __syncwarp();
-    double z = 0.0;
-#pragma unroll
-    for (int i = 0; i < kMaxN; i += 2) {
-        if (i < n) {
-            const double2 yi = *reinterpret_cast<const double2 *>(vec + 32 + i);
-            z = fma(v[i], yi.x, z);
-            if (i + 1 < n)
-                z = fma(v[i + 1], yi.y, z);
-        }
-    }
-    const double di = act ? -z : 0.0;
-    bool gammaOk = true;
-    if (a.tolGamma > 0.0)
-        gammaOk = modcfl(di, n, lane, a.momentType) <= a.tolGamma;
-    if (err <= sc[SC_RTOL] && gammaOk) {
-        converge(a, pb, L, s, ui, ai, gi, lane);
-        return;
-    }
-    // line search set-up (linesearch.cpp:21-52)
-    const double gd = warp_sum(gi * di);
-    const double maxf = warp_max(act ? fabs(di) / (fabs(ai) + 1e-100) : 0.0);
-    if (act) {
-        L.aold[s * ldv + lane] = ai;
-        L.d[s * ldv + lane] = di;
-    }
-    if (1.0 * maxf > DBL_EPSILON / 2) {
-        if (act)
-            L.alpha[s * ldv + lane] = ai + 1.0 * di;
-        __syncwarp();
-        if (lane == 0) {
-            sc[SC_T] = 1.0;
-            sc[SC_FREF] = fH;
-            sc[SC_GD] = gd;
-            sc[SC_MAXF] = maxf;
-            si[SI_STATE] = S_TRIAL;
-        }
-        return;
-    }
-    // zero-length search: linesearch returns 0 without evaluating
-    __syncwarp();
-    if (lane == 0) {
-        sc[SC_T] = 0.0;
-        si[SI_ITER] += 1;
-        si[SI_TOTAL] += 1;
-    }
-    __syncwarp();
-    regularize(a, pb, L, s, lane, ldv, ui, ai);
-}
-
-// Fused evaluation contractions (used when every problem's G has at most NTF
-// column tiles of 8).  Warp w owns slot rows mt = w % 2 (16 slots) and the
-// q-group qg = w / 2 (8 of the chunk's 32 quadrature rows): it forms
-// S = alpha . P^T for its 16 x 8 block,
-// the weights E = w exp(S) in the accumulator layout, and uses them directly
-// as the A operand of G += E . Phess.  The A fragment's k-slots t and t+4 are
-// taken as quadrature rows 2t and 2t+1 (the rows the accumulator of S gives
-// this lane), and the B fragment is read from the same two rows, so E never
-// goes through shared memory.  Chunks keep the basis_row layout of the
-// global array, under which both fragment patterns (rows g, and rows 2t,
-// 2t + 1) are free of bank conflicts.  The four q-group
-// partial sums of G are added in q-group order at the end.  Three chunk
-// buffers keep one chunk in flight while two are read.
-constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on any wait for a staged chunk
-
-template <int NTF, int PPN>
-__device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int tid,
-                                              int lane, int warp, unsigned &mbPhase)
-{
-    const int g = lane >> 2, t4 = lane & 3;
-    const int kq = a.kq, ldv = a.ldv, ldG = a.ldG;
-    const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
-    const int NTH = K2p / 8;
-    const int NT2 = NTH + (a.momentType == 1 ? nb / 8 : 0);
-    const int nchunks = pb.nqp / kq;
-    const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
-    const int mt = warp & 1, qg = warp >> 1;
-    const int r0 = mt * 16 + g, r1 = r0 + 8;
-    const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
-    const double *A0 = L.alpha + r0 * ldv + t4, *A1 = L.alpha + r1 * ldv + t4;
-    double acc[NTF][4];
-#pragma unroll
-    for (int j = 0; j < NTF; j++)
-        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
-    double facc0 = 0.0, facc1 = 0.0;
-    const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
-
-    // Chunk c into buffer `buf`: one bulk copy of the contiguous block
-    // (chunkDoubles is even, the block starts 16-byte aligned), issued by
-    // thread 0 with its byte count expected on the buffer's mbarrier.
-    const unsigned chunkBytes = (unsigned)chunkDoubles * 8u;
-    unsigned pending = 0;   // buffers with a copy issued and not yet waited for
-    auto load_chunk = [&](int c, int buf) {
-        if (tid == 0) {
-            mbar_expect_tx(&L.bar[buf], chunkBytes);
-            bulk_copy_g2s(L.P + buf * chunkDoubles, pb.P + (size_t)c * chunkDoubles, chunkBytes, &L.bar[buf]);
-        }
-        pending |= 1u << buf;
-    };
-    auto wait_chunk = [&](int buf) -> bool {
-        const bool ok = mbar_wait_bounded(&L.bar[buf], (mbPhase >> buf) & 1u, kWaitNs);
-        mbPhase ^= 1u << buf;
-        pending &= ~(1u << buf);
-        return ok;
-    };
-    // after a timeout: wait (bounded) for the copies still in flight so that
-    // none lands in shared memory after the CTA has exited
-    auto abandon = [&]() {
-        if (tid == 0)
-            record_error(a.err, -5, -1);
-        for (int b = 0; b < 3; b++)
-            if (pending & (1u << b))
-                wait_chunk(b);
-        return false;
-    };
-    const int qa = qg * 8 + g;                 // GEMM1 B rows
-    const int qb = qg * 8 + 2 * t4;            // GEMM2 B rows qb, qb + 1
-    const int offA = basis_row(qa, ldP);
-    const int wOff = basis_wgap(qb, ldP);   // weights of rows qb, qb + 1
-    const int offB = basis_row(qb, ldP) + g;   // rows qb and qb + 1 share the gap
-
-    // S block of chunk c (the staged copy at Pb)
-    auto gemm1 = [&](const double *Pb, double (&cs)[4]) {
-        cs[0] = cs[1] = cs[2] = cs[3] = 0.0;
-        const double *B1 = Pb + offA;
-#pragma unroll
-        for (int ks = 0; ks < 4; ks++)
-            if (ks * 8 < nb)
-                dmma16x8x8(cs, A0[ks * 8], A1[ks * 8], A0[ks * 8 + 4], A1[ks * 8 + 4], B1[ks * 8 + t4],
-                           B1[ks * 8 + t4 + 4]);
-    };
-    // e[h]: Hessian weights, eg[h]: PPn gradient weights; h = 0..3 is
-    // (slot r0, row qb), (r0, qb + 1), (r1, qb), (r1, qb + 1) of chunk c
-    auto weights = [&](const double *Pc, const double (&cs)[4], double (&e)[4], double (&eg)[4]) {
-        const double w0 = Pc[wOff], w1 = Pc[wOff + 1];   // staged with the chunk
-        if constexpr (PPN == 0) {
-            fast_exp_n<4>(e, cs, L.exptab, invL, L1, L2);
-            e[0] *= w0;
-            e[1] *= w1;
-            e[2] *= w0;
-            e[3] *= w1;
-            facc0 += e[0] + e[1];
-            facc1 += e[2] + e[3];
-            eg[0] = eg[1] = eg[2] = eg[3] = 0.0;
-        } else {
-            // fobj.cpp:408-434 and :196-210 (PPn)
-#pragma unroll
-            for (int h = 0; h < 4; h++) {
-                const double dl = (h < 2) ? dl0 : dl1;
-                const double ww = (h & 1) ? w1 : w0;
-                const double k = 0.5 * cs[h];
-                const double s2 = sqrt(k * k + dl);
-                double G = k + s2;
-                if (k < 0)
-                    G = -dl / (k - sqrt(k * k + dl));
-                e[h] = 0.5 * ww * (G / s2);
-                eg[h] = ww * G;
-                const double ft = ww * (k * G - 0.5 * dl + dl * log(G));
-                if (h < 2)
-                    facc0 += ft;
-                else
-                    facc1 += ft;
-            }
-        }
-    };
-
-    // Software pipeline over three staged chunks: iteration c accumulates
-    // G with chunk c's weights while it forms S and the weights of chunk
-    // c + 1, and the copy of chunk c + 2 is in flight.
-    load_chunk(0, 0);
-    if (nchunks > 1)
-        load_chunk(1, 1);
-    if (__syncthreads_or(!wait_chunk(0)))
-        return abandon();
-    double e[4], eg[4];
-    {
-        double cs[4];
-        gemm1(L.P, cs);
-        weights(L.P, cs, e, eg);
-    }
-    int bc = 0;   // buffer of chunk c
-    for (int c = 0; c < nchunks; c++) {
-        const int bn = (bc == 2) ? 0 : bc + 1, bf = (bn == 2) ? 0 : bn + 1;
-        const bool okWait = (c + 1 < nchunks) ? wait_chunk(bn) : true;
-        // chunk c + 1 visible to all; every warp is done with chunk c - 1 (buffer bf)
-        if (__syncthreads_or(!okWait))
-            return abandon();
-        if (c + 2 < nchunks)
-            load_chunk(c + 2, bf);
-        const bool more = c + 1 < nchunks;
-        double cs[4];
-        if (more)
-            gemm1(L.P + bn * chunkDoubles, cs);
-        const double *B2 = L.P + bc * chunkDoubles + offB;
-#pragma unroll
-        for (int nt = 0; nt < NTF; nt++) {
-            if (nt < NT2) {
-                const bool hess = (PPN == 0) || nt < NTH;
-                const int col = hess ? nb + nt * 8 : (nt - NTH) * 8;
-                const double x0 = hess ? e[0] : eg[0], x1 = hess ? e[1] : eg[1];
-                const double x2 = hess ? e[2] : eg[2], x3 = hess ? e[3] : eg[3];
-                dmma16x8x8(acc[nt], x0, x2, x1, x3, B2[col], B2[col + ldP]);
-            }
-        }
-        if (more)
-            weights(L.P + bn * chunkDoubles, cs, e, eg);
-        bc = bn;
-    }
-    __syncthreads();   // the G region overlaps the staged basis
-#pragma unroll 1
-    for (int step = 0; step < 4; step++) {
-        if (qg == step) {
-#pragma unroll
-            for (int nt = 0; nt < NTF; nt++) {
-                if (nt < NT2) {
-                    double *G0 = L.G + r0 * ldG + nt * 8 + 2 * t4;
-                    if (step == 0) {
-                        G0[0] = acc[nt][0];
-                        G0[1] = acc[nt][1];
-                        G0[8 * ldG] = acc[nt][2];
-                        G0[8 * ldG + 1] = acc[nt][3];
-                    } else {
-                        G0[0] += acc[nt][0];
-                        G0[1] += acc[nt][1];
-                        G0[8 * ldG] += acc[nt][2];
-                        G0[8 * ldG + 1] += acc[nt][3];
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    facc0 += __shfl_xor_sync(0xffffffffu, facc0, 1);
-    facc0 += __shfl_xor_sync(0xffffffffu, facc0, 2);
-    facc1 += __shfl_xor_sync(0xffffffffu, facc1, 1);
-    facc1 += __shfl_xor_sync(0xffffffffu, facc1, 2);
-    if (t4 == 0) {
-        L.fpart[r0 * a.ntq + qg] = facc0;
-        L.fpart[r1 * a.ntq + qg] = facc1;
-    }
-    __syncthreads();
-    return true;
-}
-
-template <int TPW, int NTF, int PPN>
-__global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
-{
-    extern __shared__ __align__(16) double sm[];
-    __shared__ int ctl[4];   // [0] problem, [1] done, [2] exhausted
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t4 = lane & 3;
-    const int T = a.T, MT = a.T / 16, kq = a.kq, ldv = a.ldv, ldE = a.ldE, ldG = a.ldG;
-    Layout L = make_layout(sm, a);
-
-    for (int i = tid; i < 4 * T * ldv; i += kThreads)
-        L.alpha[i] = 0.0;   // alpha, aold, d, u are contiguous
-    for (int i = tid; i < T * SI_N; i += kThreads)
-        L.ints[i] = (i % SI_N == SI_STATE) ? S_IDLE : 0;
-    for (int i = tid; i <= kStatU64; i += kThreads)
-        L.stat[i] = 0ull;
-    for (int i = tid; i < 64; i += kThreads)
-        L.exptab[i] = a.ex.tab[i];
-    for (int i = tid; i < T * SC_N; i += kThreads)
-        L.scal[i] = 0.0;
-    if (tid == 0) {
-        ctl[0] = 0;
-        ctl[1] = 0;
-        ctl[2] = 0;
-    }
-    if (tid == 0) {
-        for (int b = 0; b < 3; b++)
-            mbar_init(&L.bar[b], 1);
-        mbar_init_fence();
-    }
-    __syncthreads();
-    int loadedProb = -1;
-    unsigned mbPhase = 0;   // parity of the next phase of each chunk mbarrier
-
-    for (;;) {
-        // ---- refill idle slots from the work counter of the current problem
-        if (tid == 0) {
-            int p = ctl[0];
-            int nIdle = 0, nActive = 0;
-            for (int s = 0; s < T; s++) {
-                if (L.ints[s * SI_N + SI_STATE] == S_IDLE)
-                    nIdle++;
-                else
-                    nActive++;
-            }
-            bool exhausted = ctl[2] != 0;
-            while (nIdle > 0) {
-                if (exhausted) {
-                    if (nActive == 0 && p + 1 < a.nprob) {
-                        p++;
-                        exhausted = false;
-                        continue;
-                    }
-                    break;
-                }
-                const NewtonProblem &pb = a.prob[p];
-                unsigned base = atomicAdd(pb.queue, (unsigned)nIdle);
-                if (base >= (unsigned)pb.count) {
-                    exhausted = true;
-                    continue;
-                }
-                int take = min(nIdle, pb.count - (int)base);
-                int c = 0;
-                for (int s = 0; s < T && c < take; s++) {
-                    if (L.ints[s * SI_N + SI_STATE] == S_IDLE) {
-                        L.ints[s * SI_N + SI_CELL] = (int)base + c;
-                        L.ints[s * SI_N + SI_STATE] = S_NEW;
-                        c++;
-                    }
-                }
-                nIdle -= take;
-                nActive += take;
-                if (nIdle > 0)
-                    exhausted = true;
-            }
-            ctl[0] = p;
-            ctl[2] = exhausted ? 1 : 0;
-            ctl[1] = (nActive == 0) ? 1 : 0;
-        }
-        __syncthreads();
-        if (ctl[1])
-            break;
-        const NewtonProblem &pb = a.prob[ctl[0]];
-        if (ctl[0] != loadedProb) {
-            // stage this order's Gaunt contraction table in shared memory
-            loadedProb = ctl[0];
-            if (a.useGaunt) {
-                for (int i = tid; i < pb.ellRows * 32; i += kThreads) {
-                    L.ellVal[i] = pb.ellVal[i];
-                    L.ellIdx[i] = pb.ellIdx[i];
-                }
-                for (int i = tid; i < pb.ellChunks * 32; i += kThreads)
-                    L.ellPair[i] = pb.ellPair[i];
-                for (int i = tid; i <= pb.ellChunks; i += kThreads)
-                    L.ellOff[i] = pb.ellOff[i];
-            }
-        }
-        for (int s = warp; s < T; s += kWarps)
-            if (L.ints[s * SI_N + SI_STATE] == S_NEW)
-                init_slot(a, pb, L, s, lane, ldv);
-        __syncthreads();
-
-        // ---- phase A: evaluation contractions over the quadrature
-        if constexpr (NTF > 0) {
-            if (!phase_a_fused<NTF, PPN>(a, pb, L, tid, lane, warp, mbPhase))
-                return;   // a staged chunk never arrived (error recorded)
-        } else {
-        const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
-        const int NTH = K2p / 8;
-        const int NT2 = NTH + (a.momentType == 1 ? nb / 8 : 0);
-        const int ntiles2 = MT * NT2;
-        const int nchunks = pb.nqp / kq;
-        const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
-        const int mt1 = warp % MT, ntq = warp / MT;
-        double acc[TPW][4];
-#pragma unroll
-        for (int j = 0; j < TPW; j++)
-            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
-        double facc0 = 0.0, facc1 = 0.0;
-        const int r0 = mt1 * 16 + g, r1 = r0 + 8;
-        const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
-
-        auto load_chunk = [&](int c, int buf) {
-            const double *src = pb.P + (size_t)c * chunkDoubles;
-            double *dst = L.P + buf * chunkDoubles;
-            for (int i = tid; i < chunkDoubles / 2; i += kThreads)
-                cp_async16(dst + 2 * i, src + 2 * i);
-            cp_async_commit();
-        };
-        if (a.doubleBuffer)
-            load_chunk(0, 0);
-        for (int c = 0; c < nchunks; c++) {
-            int buf = a.doubleBuffer ? (c & 1) : 0;
-            if (a.doubleBuffer) {
-                if (c + 1 < nchunks) {
-                    load_chunk(c + 1, buf ^ 1);
-                    cp_async_wait<1>();
-                } else {
-                    cp_async_wait<0>();
-                }
-            } else {
-                load_chunk(c, 0);
-                cp_async_wait<0>();
-            }
-            __syncthreads();
-            const double *Pb = L.P + buf * chunkDoubles;
-            // GEMM1: S = alpha . P^T for this warp's 16 x 8 tile
-            {
-                double cs[4] = {0.0, 0.0, 0.0, 0.0};
-                const double *A0 = L.alpha + r0 * ldv, *A1 = L.alpha + r1 * ldv;
-                const double *B = Pb + basis_row(ntq * 8 + g, ldP);
-                for (int k0 = 0; k0 < nb; k0 += 8)
-                    dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4],
-                               B[k0 + t4], B[k0 + t4 + 4]);
-                const int ql = ntq * 8 + 2 * t4;
-                const int qg = c * kq + ql;
-                const double w0 = __ldg(&pb.w[qg]), w1 = __ldg(&pb.w[qg + 1]);
-                if (a.momentType == 0) {
-                    const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
-                    double ex4[4];
-                    fast_exp_n<4>(ex4, cs, L.exptab, invL, L1, L2);
-                    double e0 = w0 * ex4[0], e1 = w1 * ex4[1], e2 = w0 * ex4[2], e3 = w1 * ex4[3];
-                    L.E[r0 * ldE + ql] = e0;
-                    L.E[r0 * ldE + ql + 1] = e1;
-                    L.E[r1 * ldE + ql] = e2;
-                    L.E[r1 * ldE + ql + 1] = e3;
-                    facc0 += e0 + e1;
-                    facc1 += e2 + e3;
-                } else {
-                    // fobj.cpp:408-434 and :196-210 (PPn)
-                    double wv[2] = {w0, w1};
-#pragma unroll
-                    for (int h = 0; h < 4; h++) {
-                        double dl = (h < 2) ? dl0 : dl1;
-                        double ww = wv[h & 1];
-                        double k = 0.5 * cs[h];
-                        double s2 = sqrt(k * k + dl);
-                        double G = k + s2;
-                        if (k < 0)
-                            G = -dl / (k - sqrt(k * k + dl));
-                        double eh = 0.5 * ww * (G / s2);
-                        double eg = ww * G;
-                        double ft = ww * (k * G - 0.5 * dl + dl * log(G));
-                        int row = (h < 2) ? r0 : r1;
-                        L.E[row * ldE + ql + (h & 1)] = eh;
-                        L.Eg[row * ldE + ql + (h & 1)] = eg;
-                        if (h < 2)
-                            facc0 += ft;
-                        else
-                            facc1 += ft;
-                    }
-                }
-            }
-            __syncthreads();
-            // GEMM2: G += E . Phess (and Eg . P for the PPn gradient)
-            for (int k0 = 0; k0 < kq; k0 += 8) {
-#pragma unroll
-                for (int j = 0; j < TPW; j++) {
-                    int ti = warp + kWarps * j;
-                    if (ti < ntiles2) {
-                        int mt2 = ti % MT, nt2 = ti / MT;
-                        const double *Ab = (nt2 < NTH) ? L.E : L.Eg;
-                        int col = (nt2 < NTH) ? nb + nt2 * 8 : (nt2 - NTH) * 8;
-                        const double *A0 = Ab + (mt2 * 16 + g) * ldE + k0 + t4;
-                        const double *A1 = A0 + 8 * ldE;
-                        const double *B0 = Pb + basis_row(k0 + t4, ldP) + col + g;
-                        // row k0 + t4 + 4 is 4 * ldP + 4 doubles further (one gap)
-                        dmma16x8x8(acc[j], A0[0], A1[0], A0[4], A1[4], B0[0], B0[4 * ldP + 4]);
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        // dump accumulators and f partial sums
-#pragma unroll
-        for (int j = 0; j < TPW; j++) {
-            int ti = warp + kWarps * j;
-            if (ti < ntiles2) {
-                int mt2 = ti % MT, nt2 = ti / MT;
-                double *G0 = L.G + (mt2 * 16 + g) * ldG + nt2 * 8 + 2 * t4;
-                G0[0] = acc[j][0];
-                G0[1] = acc[j][1];
-                G0[8 * ldG] = acc[j][2];
-                G0[8 * ldG + 1] = acc[j][3];
-            }
-        }
-        facc0 += __shfl_xor_sync(0xffffffffu, facc0, 1);
-        facc0 += __shfl_xor_sync(0xffffffffu, facc0, 2);
-        facc1 += __shfl_xor_sync(0xffffffffu, facc1, 1);
-        facc1 += __shfl_xor_sync(0xffffffffu, facc1, 2);
-        if (t4 == 0) {
-            L.fpart[r0 * a.ntq + ntq] = facc0;
-            L.fpart[r1 * a.ntq + ntq] = facc1;
-        }
-        __syncthreads();
-        }
-
-        // ---- phase B: per-slot Newton logic, one warp per slot
-        for (int s = warp; s < T; s += kWarps) {
-            int st = L.ints[s * SI_N + SI_STATE];
-            if (st == S_NEWTON || st == S_TRIAL)
-                slot_logic(a, pb, L, s, lane, warp);
-        }
-        if constexpr (NTF > 0)
-            fence_proxy_async_smem();   // this round's shared-memory writes before the next bulk copies
-        __syncthreads();
-    }
-
-    // flush CTA statistics (hist, totalIter, numSolves, trials are contiguous)
-    if (tid < kStatU64) {
-        unsigned long long v = L.stat[tid];
-        if (v)
-            atomicAdd(&a.stats->hist[0] + tid, v);
-    } else if (tid == kStatU64) {
-        atomicMax(&a.stats->maxIter, *(int *)&L.stat[kStatU64]);
-    }
-}
-
-}  // namespace
 
 int plan_newton(NewtonArgs &a)
 {
@@ -1200,7 +55,9 @@ int plan_newton(NewtonArgs &a)
     // fused contractions when every problem's G fits in 16 column tiles
     // (one warp per 16 slots x 8 quadrature rows of a 32-row chunk)
     const int nt2 = K2tot / 8;
-    a.ntf = (nt2 <= 16) ? ((nt2 + 3) / 4) * 4 : 0;
+    a.ntf = (nt2 <= 16) ? ((nt2 + 7) / 8) * 8 : 0;
+    a.ntExact = (a.ntf > 0 && a.nprob == 1) ? nt2 : 0;
+    a.nbk = (a.ntf > 0 && a.nprob == 1) ? a.prob[0].nb / 8 : 0;
     // phase-B region
     int offG = unionBase;
     int offH = offG + ((T * a.ldG + 1) & ~1);
@@ -1222,6 +79,7 @@ int plan_newton(NewtonArgs &a)
             return 0;
         }
         a.ntf = 0;
+        a.ntExact = a.nbk = 0;
     }
     for (int db = 1; db >= 0; db--) {
         int offP = unionBase;
@@ -1244,79 +102,38 @@ int plan_newton(NewtonArgs &a)
     return -1;
 }
 
-template <int TPW, int NTF, int PPN>
-static cudaError_t launch_t(const NewtonArgs &a, int grid, cudaStream_t stream, bool prepare)
+// Instance selection: a single-problem launch on the fused path runs the
+// kernel specialised to its exact column-tile and k-step counts; mixed
+// orders run the fused instance with runtime counts; the rest the general
+// contractions.  mode: 0 launch, 1 shared-memory attribute, 2 occupancy.
+static cudaError_t run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
 {
-    if (prepare)
-        return cudaFuncSetAttribute(newton_kernel<TPW, NTF, PPN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    a.smemBytes);
-    newton_kernel<TPW, NTF, PPN><<<grid, kThreads, a.smemBytes, stream>>>(a);
-    return cudaGetLastError();
-}
-
-template <int TPW, int NTF, int PPN>
-static int occupancy_t(const NewtonArgs &a)
-{
-    int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, newton_kernel<TPW, NTF, PPN>, kThreads,
-                                                      a.smemBytes) != cudaSuccess)
-        return 1;
-    return blocks < 1 ? 1 : blocks;
-}
-
-// Calls op.template run<TPW, NTF, PPN>() for the kernel instance of `a`.
-template <class Op>
-static auto with_instance(const NewtonArgs &a, Op op)
-{
-    if (a.ntf > 0) {
-        const bool ppn = a.momentType == 1;
-        if (a.ntf <= 4)
-            return ppn ? op.template run<1, 4, 1>() : op.template run<1, 4, 0>();
-        if (a.ntf <= 8)
-            return ppn ? op.template run<1, 8, 1>() : op.template run<1, 8, 0>();
-        if (a.ntf <= 12)
-            return ppn ? op.template run<1, 12, 1>() : op.template run<1, 12, 0>();
-        return ppn ? op.template run<1, 16, 1>() : op.template run<1, 16, 0>();
+    cudaError_t e = cudaErrorInvalidValue;
+    if (a.ntf > 0 && a.ntExact > 0) {
+        if (newton_run_exact_mn_a(a, grid, stream, mode, occ, &e) ||
+            newton_run_exact_mn_b(a, grid, stream, mode, occ, &e) ||
+            newton_run_exact_ppn_a(a, grid, stream, mode, occ, &e) ||
+            newton_run_exact_ppn_b(a, grid, stream, mode, occ, &e))
+            return e;
     }
-    if (a.tpw <= 1)
-        return op.template run<1, 0, 0>();
-    if (a.tpw <= 2)
-        return op.template run<2, 0, 0>();
-    if (a.tpw <= 4)
-        return op.template run<4, 0, 0>();
-    if (a.tpw <= 8)
-        return op.template run<8, 0, 0>();
-    return op.template run<16, 0, 0>();
+    if (newton_run_generic(a, grid, stream, mode, occ, &e))
+        return e;
+    return cudaErrorInvalidValue;
 }
 
-struct LaunchOp {
-    const NewtonArgs &a;
-    int grid;
-    cudaStream_t stream;
-    bool prepare;
-    template <int TPW, int NTF, int PPN>
-    cudaError_t run() const { return launch_t<TPW, NTF, PPN>(a, grid, stream, prepare); }
-};
-struct OccupancyOp {
-    const NewtonArgs &a;
-    template <int TPW, int NTF, int PPN>
-    int run() const { return occupancy_t<TPW, NTF, PPN>(a); }
-};
-
-cudaError_t prepare_newton(const NewtonArgs &a)
-{
-    if (a.ntf == 0 && a.tpw > 16)
-        return cudaErrorInvalidValue;
-    return with_instance(a, LaunchOp{a, 0, nullptr, true});
-}
+cudaError_t prepare_newton(const NewtonArgs &a) { return run(a, 0, nullptr, 1, nullptr); }
 
 cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream)
 {
-    if (a.ntf == 0 && a.tpw > 16)
-        return cudaErrorInvalidValue;
-    return with_instance(a, LaunchOp{a, grid, stream, false});
+    return run(a, grid, stream, 0, nullptr);
 }
 
-int newton_ctas_per_sm(const NewtonArgs &a) { return with_instance(a, OccupancyOp{a}); }
+int newton_ctas_per_sm(const NewtonArgs &a)
+{
+    int occ = 1;
+    if (run(a, 0, nullptr, 2, &occ) != cudaSuccess)
+        return 1;
+    return occ;
+}
 
 }  // namespace clb

@@ -48,6 +48,11 @@ struct NewtonProblem {
     unsigned int *queue;        // work counter, zero before the launch
 };
 
+// Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
+enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
+enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_N };
+enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_N };
+
 struct NewtonArgs {
     NewtonProblem prob[kMaxProblems];
     int nprob;
@@ -68,6 +73,8 @@ struct NewtonArgs {
     int smemBytes;
     int tpw;                    // column tiles per warp (general contractions)
     int ntf;                    // > 0: fused contractions with this many tiles per warp
+    int ntExact, nbk;           // single problem on the fused path: its column tiles and
+                                // GEMM1 k-steps (selects a specialised instance), else 0
 };
 
 // Fills the layout fields from the problems' sizes; returns 0 or -1 when
@@ -78,5 +85,14 @@ cudaError_t prepare_newton(const NewtonArgs &a);
 // Launches the persistent kernel on `stream` over `grid` CTAs.
 cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream);
 int newton_ctas_per_sm(const NewtonArgs &a);
+
+// Kernel instances, grouped by translation unit.  Each returns true when it
+// holds the instance `a` selects and then sets *err to the result of
+// running it (mode 0 launch, 1 shared-memory attribute, 2 occupancy).
+bool newton_run_generic(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_mn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_mn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_ppn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_ppn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 
 }  // namespace clb
