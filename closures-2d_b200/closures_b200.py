@@ -315,8 +315,11 @@ class Context:
                                                  ptr(d_status)), self._err)
 
     def set_warm_start(self, mlp):
-        """Predict alpha with `mlp` before every optimisation stage (None: off)."""
+        """Predict alpha with `mlp` before every optimisation stage (None: off).
+        The context borrows the network's device buffers, so it keeps a
+        reference to `mlp` until the warm start is replaced or removed."""
         _check(lib().cl_set_warm_start(self._ctx, mlp._m if mlp is not None else None), self._err)
+        self._warm = mlp
 
     def device_state(self):
         m, a = C.c_void_p(), C.c_void_p()
@@ -382,11 +385,15 @@ class Solver:
         _check(lib().cl_solver_output(self._s, time), self._err)
 
     def context(self):
-        """The device context (shares the solver's state)."""
-        c = Context.__new__(Context)
-        c._ctx = C.c_void_p(lib().cl_solver_context(self._s))
-        c._borrowed = True
-        c.n, c.NX, c.NY = self.n, self.NX, self.NY
+        """The device context (shares the solver's state; one wrapper per
+        solver, so a warm start set through it lives as long as the solver)."""
+        c = getattr(self, "_cctx", None)
+        if c is None:
+            c = Context.__new__(Context)
+            c._ctx = C.c_void_p(lib().cl_solver_context(self._s))
+            c._borrowed = True
+            c.n, c.NX, c.NY = self.n, self.NX, self.NY
+            self._cctx = c
         return c
 
     def context_state(self):
@@ -414,6 +421,7 @@ class Solver:
         if self._s:
             lib().cl_solver_destroy(self._s)
             self._s = C.c_void_p()
+        self._cctx = None   # after the context is gone: drops a borrowed warm-start network
 
     def __del__(self):
         if _lib is not None and getattr(self, "_s", None):

@@ -152,3 +152,66 @@ def test_warm_start_reduces_iterations_same_answer():
     assert err.max() < 1e-6
     m.close()
     ctx.close()
+
+
+def test_grid_warm_start_matches_plain(tmp_path):
+    """cl_set_warm_start on a grid: a network trained on the run's own
+    (u, alpha*) pairs gives the predicted starts (fallback: the previous
+    stage's alpha); the steps reach the same moments as plain steps."""
+    import torch
+    import decks
+
+    # a deck whose decisions rounding does not move (the grid parity test
+    # holds it to 1e-10 against the oracle): both runs must then agree to
+    # the solver tolerance, with the same regularisation steps
+    kw = dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.1, floor=1e-8, moment_order=6,
+              quad_order=40, tol=1e-8, use_gaunt=1)
+    deck = str(tmp_path / "input.deck")
+    decks.write_deck(deck, decks.deck_text(**kw))
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    s1 = cb.Solver(deck, str(tmp_path / "a"))
+    s2 = cb.Solver(deck, str(tmp_path / "b"))
+    for _ in range(3):
+        s1.update(s1.max_dt)
+        s2.update(s2.max_dt)
+    n = s2.n
+    dev = torch.device("cuda", 0)
+    m, al = s2.context_state()
+    du = torch.from_numpy(m.reshape(-1, n).copy()).to(dev)
+    da = torch.from_numpy(al.reshape(-1, n).copy()).to(dev)
+    cnt = du.shape[0]
+    ang = cb.Angular(6, 40, 1)
+    bctx = cb.Context.for_batches(ang, cb.make_options(tol=1e-8))
+    st = torch.zeros(cnt, dtype=torch.int32, device=dev)
+    bctx.solve_batch_device(du, da, None, None, st, count=cnt)
+    torch.cuda.synchronize()
+    bctx.close()
+    assert (st == 0).all()
+    u, a = du.cpu().numpy(), da.cpu().numpy()
+    tgt = a.copy()
+    tgt[:, 0] -= 2.0 * SQRT_PI * np.log(u[:, 0])
+    lin = 2.0 * SQRT_PI * u / u[:, :1]
+    lin[:, 0] = 2.0 * SQRT_PI * np.log(0.5 / SQRT_PI)
+    resid = tgt - lin
+    net = cb.MLP(n, 128, seed=3)
+    net.set_output_scaling(resid.mean(axis=0).astype(np.float32),
+                           (resid.std(axis=0) + 1e-3).astype(np.float32))
+    net.train(du, da, cnt, steps=400, batch=512, lr=1e-3, record_loss=False)
+    s2.context().set_warm_start(net)
+    del net   # the context keeps the network alive
+    f0 = s2.stats()["fallbacks"]
+    for _ in range(3):
+        s1.update(s1.max_dt)
+        s2.update(s2.max_dt)
+    m1, _ = s1.context_state()
+    m2, _ = s2.context_state()
+    st1, st2 = s1.stats(), s2.stats()
+    print("iterations plain %.3f, learned start %.3f, fallback restarts %d"
+          % (st1["iter_mean"], st2["iter_mean"], st2["fallbacks"] - f0))
+    assert st1["hist_reg"] == st2["hist_reg"]
+    err = float(np.max(np.abs(m2 - m1) / np.abs(m1[:, :, :1])))
+    assert err < 1e-6, err
+    s2.context().set_warm_start(None)
+    s1.close()
+    s2.close()
