@@ -137,9 +137,12 @@ def dist_setup():
     return world, rank, local
 
 
-def write_deck(tmpdir, workload):
+def write_deck(tmpdir, workload, precision="fp64"):
     path = os.path.join(tmpdir, "input.deck")
-    decks.write_deck(path, decks.deck_text(**WORKLOADS[workload]))
+    kw = dict(WORKLOADS[workload])
+    if precision == "mixed":
+        kw["extra"] = {"MOMOPT_GPU_PRECISION": "mixed"}
+    decks.write_deck(path, decks.deck_text(**kw))
     return path
 
 
@@ -254,7 +257,7 @@ def native_arm(args, world, rank, local):
                                 device_id=torch.device("cuda", local))
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
-    deck = write_deck(tmp, args.workload)
+    deck = write_deck(tmp, args.workload, args.precision)
     solver = cb.Solver(deck, tmp)
     ctx = solver.context()
     dt, dx, dy = solver.max_dt, solver.dx, solver.dy
@@ -364,13 +367,14 @@ def native_arm(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": "cell-solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": device_ms / args.steps, "steps_per_s": 1e3 * args.steps / device_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f64, Hessian-only tiles split tf32",
             "data": "synthetic",
             "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
                        "moment_order": w["moment_order"], "n": n, "quad_order": w["quad_order"],
                        "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
                        "moment_type": w["moment_type"] if "moment_type" in w else "mn",
-                       "newton": args.newton, "precision": "fp64", "t_start": args.warmup * dt,
+                       "newton": args.newton, "precision": args.precision, "t_start": args.warmup * dt,
                        "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
                        "parallelism": "replicas" if world > 1 else "single"},
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
@@ -569,6 +573,8 @@ def main():
     ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
                     help="batch workload: start from the isotropic multiplier or a learned prediction")
     ap.add_argument("--nn-steps", type=int, default=4000)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="grid workloads: Hessian-only tiles in split TF32 (MOMOPT_GPU_PRECISION mixed)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.workload == "batch_2e20":

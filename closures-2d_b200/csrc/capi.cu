@@ -102,6 +102,8 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
     B.ldPf = B.nb + 4;
     B.p0 = p[0];
     std::vector<double> P((size_t)B.nqp * ldP + B.nqp, 0.0), W(B.nqp, 0.0);
+    std::vector<unsigned short> prod(n * (n + 1) / 2);
+    product_columns(n, prod.data());
     std::vector<double> Pf((size_t)B.nqp * B.ldPf, 0.0), XI(B.nqp, 0.0), ET(B.nqp, 0.0), CX(B.nqp, 0.0),
         CY(B.nqp, 0.0);
     for (int q = 0; q < nq; q++) {
@@ -113,10 +115,8 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
             for (int k = 0; k < n2; k++)
                 row[B.nb + k] = pq[k];
         } else {
-            int c = 0;
-            for (int i = 0; i < n; i++)
-                for (int j = 0; j <= i; j++)
-                    row[B.nb + c++] = pq[i] * pq[j];
+            for (int c = 0; c < n * (n + 1) / 2; c++)
+                row[B.nb + c] = pq[prod[c] >> 8] * pq[prod[c] & 255];
         }
         W[q] = w[q];
         P[(size_t)basis_wgap(q, ldP)] = w[q];
@@ -127,13 +127,7 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         CX[q] = xi[q] * w[q];
         CY[q] = eta[q] * w[q];
     }
-    std::vector<unsigned short> pairs;
-    for (int i = 0; i < n; i++)
-        for (int j = 0; j <= i; j++)
-            pairs.push_back((unsigned short)((i << 8) | j));
-    for (int k = 0; k < n; k++)
-        for (int i = k; i < n; i++)
-            pairs.push_back((unsigned short)((i << 8) | k));
+    std::vector<unsigned short> &pairs = prod;
     cudaError_t e;
     if ((e = upload(&B.P, P)) != cudaSuccess) return e;
     if ((e = upload(&B.w, W)) != cudaSuccess) return e;
@@ -228,6 +222,7 @@ void fill_newton_options(NewtonArgs &a, const cl_options &o, int useGaunt)
     a.tolRel = o.tol;
     a.condHMax = o.cond_h_max;
     a.deltaPPn = o.delta_ppn;
+    a.mixed = o.precision == CL_MIXED;
     a.tolGamma = o.tol_gamma;
 }
 
@@ -423,8 +418,10 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     a.err = ctx->dErr;
     a.NX = ctx->NX;
     a.NY = ctx->NY;
-    if (plan_newton(a) != 0) {
-        ctx->err = "Newton kernel layout does not fit in shared memory";
+    const int pl = plan_newton(a);
+    if (pl != 0) {
+        ctx->err = pl == -2 ? "mixed precision needs a configuration with at most 16 Hessian column tiles"
+                            : "Newton kernel layout does not fit in shared memory";
         return ctx_fail(ctx, CL_ERR_ARG);
     }
     if ((ce = prepare_newton(a)) != cudaSuccess) {
@@ -939,8 +936,10 @@ int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaun
     cudaMemset(m->dErr, 0, 2 * sizeof(int));
     a.stats = m->dStats;
     a.err = m->dErr;
-    if (plan_newton(a) != 0) {
-        g_global_err = "Newton kernel layout does not fit in shared memory";
+    const int pl = plan_newton(a);
+    if (pl != 0) {
+        g_global_err = pl == -2 ? "mixed precision needs a single moment order per launch"
+                                : "Newton kernel layout does not fit in shared memory";
         cl_multi_destroy(m);
         return CL_ERR_ARG;
     }
@@ -1014,7 +1013,58 @@ __global__ void dmma_selftest_kernel(const double *A, const double *B, double *C
     C[(g + 8) * 8 + 2 * t] = c[2];
     C[(g + 8) * 8 + 2 * t + 1] = c[3];
 }
+__global__ void tmma_selftest_kernel(const float *A, const float *B, float *C)
+{
+    // one warp: C[16x8] = A[16x8] . B[8x8] in TF32 (integer-valued inputs: exact)
+    int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float c[4] = {0, 0, 0, 0};
+    tmma16x8x8(c, __float_as_uint(A[g * 8 + t]), __float_as_uint(A[(g + 8) * 8 + t]),
+               __float_as_uint(A[g * 8 + t + 4]), __float_as_uint(A[(g + 8) * 8 + t + 4]),
+               __float_as_uint(B[t * 8 + g]), __float_as_uint(B[(t + 4) * 8 + g]));
+    C[g * 8 + 2 * t] = c[0];
+    C[g * 8 + 2 * t + 1] = c[1];
+    C[(g + 8) * 8 + 2 * t] = c[2];
+    C[(g + 8) * 8 + 2 * t + 1] = c[3];
+}
 }  // namespace
+
+// TF32 fragment layout (the mixed-precision Hessian tiles rely on it).
+static int tmma_selftest()
+{
+    float hA[128], hB[64], hC[128], ref[128];
+    for (int i = 0; i < 128; i++)
+        hA[i] = (float)((i * 7) % 11 - 5);
+    for (int i = 0; i < 64; i++)
+        hB[i] = (float)((i * 5) % 9 - 4);
+    for (int r = 0; r < 16; r++)
+        for (int c = 0; c < 8; c++) {
+            float s = 0;
+            for (int k = 0; k < 8; k++)
+                s += hA[r * 8 + k] * hB[k * 8 + c];
+            ref[r * 8 + c] = s;
+        }
+    float *d = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * 320) != cudaSuccess) {
+        g_global_err = "selftest allocation failed";
+        return CL_ERR_CUDA;
+    }
+    cudaMemcpy(d, hA, sizeof(hA), cudaMemcpyHostToDevice);
+    cudaMemcpy(d + 128, hB, sizeof(hB), cudaMemcpyHostToDevice);
+    tmma_selftest_kernel<<<1, 32>>>(d, d + 128, d + 192);
+    g_launches += 1;
+    cudaError_t e = cudaMemcpy(hC, d + 192, sizeof(hC), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        g_global_err = std::string("selftest: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    for (int i = 0; i < 128; i++)
+        if (hC[i] != ref[i]) {
+            g_global_err = "TF32 fragment layout mismatch";
+            return CL_ERR_STATE;
+        }
+    return CL_OK;
+}
 
 extern "C" int cl_selftest(void)
 {
@@ -1050,7 +1100,7 @@ extern "C" int cl_selftest(void)
             g_global_err = "DMMA fragment layout mismatch";
             return CL_ERR_STATE;
         }
-    return CL_OK;
+    return tmma_selftest();
 }
 
 // Lets the host solver layer report through cl_global_error().

@@ -29,6 +29,27 @@ __device__ __forceinline__ void dmma16x8x8(double (&c)[4], double a0, double a1,
         : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
+// TF32 tensor-core MMA m16n8k8 with FP32 accumulation: the same fragment
+// ownership as dmma16x8x8, 32-bit registers holding TF32 values.
+__device__ __forceinline__ void tmma16x8x8(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                           unsigned b0, unsigned b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// x = hi + lo with hi, lo TF32 (round to nearest): the three products
+// hi.hi + hi.lo + lo.hi of two split operands carry about FP32 accuracy.
+__device__ __forceinline__ void tf32_split(float x, unsigned &hi, unsigned &lo)
+{
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(hi) : "f"(x));
+    const float r = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(lo) : "f"(r));
+}
+
 // 16-byte global->shared asynchronous copy (L2 only) and its group fences.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {

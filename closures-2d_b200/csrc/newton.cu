@@ -58,6 +58,8 @@ int plan_newton(NewtonArgs &a)
     a.ntf = (nt2 <= 16) ? ((nt2 + 7) / 8) * 8 : 0;
     a.ntExact = (a.ntf > 0 && a.nprob == 1) ? nt2 : 0;
     a.nbk = (a.ntf > 0 && a.nprob == 1) ? a.prob[0].nb / 8 : 0;
+    if (a.mixed && a.ntExact == 0)
+        return -2;
     // phase-B region
     int offG = unionBase;
     int offH = offG + ((T * a.ldG + 1) & ~1);
@@ -80,6 +82,8 @@ int plan_newton(NewtonArgs &a)
         }
         a.ntf = 0;
         a.ntExact = a.nbk = 0;
+        if (a.mixed)
+            return -2;
     }
     for (int db = 1; db >= 0; db--) {
         int offP = unionBase;
@@ -109,6 +113,11 @@ int plan_newton(NewtonArgs &a)
 static cudaError_t run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
 {
     cudaError_t e = cudaErrorInvalidValue;
+    if (a.mixed) {
+        if (newton_run_mixed_mn(a, grid, stream, mode, occ, &e) || newton_run_mixed_ppn(a, grid, stream, mode, occ, &e))
+            return e;
+        return cudaErrorInvalidValue;
+    }
     if (a.ntf > 0 && a.ntExact > 0) {
         if (newton_run_exact_mn_a(a, grid, stream, mode, occ, &e) ||
             newton_run_exact_mn_b(a, grid, stream, mode, occ, &e) ||

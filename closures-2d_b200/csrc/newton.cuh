@@ -75,10 +75,12 @@ struct NewtonArgs {
     int ntf;                    // > 0: fused contractions with this many tiles per warp
     int ntExact, nbk;           // single problem on the fused path: its column tiles and
                                 // GEMM1 k-steps (selects a specialised instance), else 0
+    int mixed;                  // Hessian-only tiles by split TF32 (CL_MIXED); needs ntExact
 };
 
-// Fills the layout fields from the problems' sizes; returns 0 or -1 when
-// the configuration does not fit in shared memory.
+// Fills the layout fields from the problems' sizes; returns 0, -1 when the
+// configuration does not fit in shared memory, -2 when mixed precision is
+// asked for a configuration without a specialised instance.
 int plan_newton(NewtonArgs &a);
 // Sets the kernel's shared-memory attribute (call once, outside capture).
 cudaError_t prepare_newton(const NewtonArgs &a);
@@ -94,5 +96,7 @@ bool newton_run_exact_mn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mo
 bool newton_run_exact_mn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_mixed_mn(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_mixed_ppn(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 
 }  // namespace clb

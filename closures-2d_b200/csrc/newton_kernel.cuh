@@ -712,7 +712,7 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
 // buffers keep one chunk in flight while two are read.
 constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on any wait for a staged chunk
 
-template <int NTF, int PPN, int NT, int NBK>
+template <int NTF, int PPN, int NT, int NBK, int MIX>
 __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int tid,
                                               int lane, int warp, unsigned &mbPhase)
 {
@@ -731,10 +731,19 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     const int r0 = mt * 16 + g, r1 = r0 + 8;
     const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
     const double *A0 = L.alpha + r0 * ldv + t4, *A1 = L.alpha + r1 * ldv + t4;
+    // Mixed precision (MIX, exact tile counts only): the Hessian-only tiles
+    // -- Mn: tiles >= NBK (columns past the n that give f and g); PPn: the
+    // Hessian tiles -- accumulate split-TF32 products in FP32; the rest FP64.
+    static_assert(!MIX || NT > 0, "mixed precision runs the exact-count instances");
+    auto lowp = [&](int nt) { return MIX && (PPN ? nt < NTH : nt >= NBK); };
     double acc[NTL][4];
+    float acc32[MIX ? NTL : 1][4];
 #pragma unroll
     for (int j = 0; j < NTL; j++)
         acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+#pragma unroll
+    for (int j = 0; j < (MIX ? NTL : 1); j++)
+        acc32[j][0] = acc32[j][1] = acc32[j][2] = acc32[j][3] = 0.0f;
     double facc0 = 0.0, facc1 = 0.0;
     const double invL = a.ex.invL, L1 = a.ex.L1, L2 = a.ex.L2;
 
@@ -834,14 +843,29 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     // G += E . Phess for the chunk staged at Pc (E: weights held in e, eg)
     auto gemm2 = [&](const double *Pc) {
         const double *B2 = Pc + offB;
+        unsigned ah[4], al[4];   // the Hessian weights split into TF32 head and tail
+        if constexpr (MIX) {
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+                tf32_split((float)e[h], ah[h], al[h]);
+        }
 #pragma unroll
         for (int nt = 0; nt < NTL; nt++) {
             if (NT > 0 || nt < NT2) {
                 const bool hess = (PPN == 0) || nt < NTH;
                 const int col = hess ? nb + nt * 8 : (nt - NTH) * 8;
-                const double x0 = hess ? e[0] : eg[0], x1 = hess ? e[1] : eg[1];
-                const double x2 = hess ? e[2] : eg[2], x3 = hess ? e[3] : eg[3];
-                dmma16x8x8(acc[nt], x0, x2, x1, x3, B2[col], B2[col + ldP]);
+                if (lowp(nt)) {
+                    unsigned bh0, bl0, bh1, bl1;
+                    tf32_split((float)B2[col], bh0, bl0);
+                    tf32_split((float)B2[col + ldP], bh1, bl1);
+                    tmma16x8x8(acc32[nt], al[0], al[2], al[1], al[3], bh0, bh1);
+                    tmma16x8x8(acc32[nt], ah[0], ah[2], ah[1], ah[3], bl0, bl1);
+                    tmma16x8x8(acc32[nt], ah[0], ah[2], ah[1], ah[3], bh0, bh1);
+                } else {
+                    const double x0 = hess ? e[0] : eg[0], x1 = hess ? e[1] : eg[1];
+                    const double x2 = hess ? e[2] : eg[2], x3 = hess ? e[3] : eg[3];
+                    dmma16x8x8(acc[nt], x0, x2, x1, x3, B2[col], B2[col + ldP]);
+                }
             }
         }
     };
@@ -861,6 +885,13 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
         bc = bn;
     }
     gemm2(L.P + bc * chunkDoubles);   // the last chunk (waited for by the last iteration)
+    if constexpr (MIX) {
+#pragma unroll
+        for (int nt = 0; nt < NTL; nt++)
+            if (lowp(nt))
+                for (int h = 0; h < 4; h++)
+                    acc[nt][h] = (double)acc32[nt][h];
+    }
     __syncthreads();   // the G region overlaps the staged basis
 #pragma unroll 1
     for (int step = 0; step < 4; step++) {
@@ -897,7 +928,7 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     return true;
 }
 
-template <int TPW, int NTF, int PPN, int NT, int NBK>
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX>
 __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
 {
     extern __shared__ __align__(16) double sm[];
@@ -1001,7 +1032,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
         // ---- phase A: evaluation contractions over the quadrature
         if constexpr (NTF > 0) {
-            if (!phase_a_fused<NTF, PPN, NT, NBK>(a, pb, L, tid, lane, warp, mbPhase))
+            if (!phase_a_fused<NTF, PPN, NT, NBK, MIX>(a, pb, L, tid, lane, warp, mbPhase))
                 return;   // a staged chunk never arrived (error recorded)
         } else {
         const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
@@ -1157,10 +1188,10 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
 // One kernel instance: mode 0 launches it, 1 sets its shared-memory limit,
 // 2 writes its resident CTAs per SM to *occ.
-template <int TPW, int NTF, int PPN, int NT, int NBK>
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX = 0>
 cudaError_t newton_run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
 {
-    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK>;
+    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK, MIX>;
     if (mode == 1)
         return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smemBytes);
     if (mode == 2) {

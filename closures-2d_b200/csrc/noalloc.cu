@@ -19,6 +19,7 @@
 
 #include "../host/angular.h"
 #include "common.cuh"
+#include "angular.h"
 #include "newton.cuh"
 
 using namespace clb;
@@ -83,7 +84,7 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     const size_t offW = off;
     off = align_up(off + sizeof(double) * (size_t)nqp, 256);
     const size_t offPairs = off;
-    off = align_up(off + sizeof(unsigned short) * 2 * (size_t)npairs, 256);
+    off = align_up(off + sizeof(unsigned short) * (size_t)npairs, 256);
     const size_t offHoff = off;
     off = align_up(off + sizeof(int) * (size_t)(gaunt ? n * n + 1 : 1), 256);
     const size_t offHidx = off;
@@ -133,6 +134,8 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     std::memset(g_stage, 0, off);
     double *P = (double *)(g_stage + offP);
     double *W = (double *)(g_stage + offW);
+    unsigned short *pairs = (unsigned short *)(g_stage + offPairs);
+    product_columns(n, pairs);
     for (int q = 0; q < nq; q++) {
         const double *pq = ang->p + (size_t)q * n2;
         double *row = P + (size_t)basis_row(q, ldP);
@@ -142,22 +145,12 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
             for (int k = 0; k < n2; k++)
                 row[nb + k] = pq[k];
         } else {
-            int c = 0;
-            for (int i = 0; i < n; i++)
-                for (int j = 0; j <= i; j++)
-                    row[nb + c++] = pq[i] * pq[j];
+            for (int c = 0; c < npairs; c++)
+                row[nb + c] = pq[pairs[c] >> 8] * pq[pairs[c] & 255];
         }
         W[q] = ang->w[q];
         P[(size_t)basis_wgap(q, ldP)] = ang->w[q];
     }
-    unsigned short *pairs = (unsigned short *)(g_stage + offPairs);
-    int c = 0;
-    for (int i = 0; i < n; i++)
-        for (int j = 0; j <= i; j++)
-            pairs[c++] = (unsigned short)((i << 8) | j);
-    for (int k = 0; k < n; k++)
-        for (int i = k; i < n; i++)
-            pairs[c++] = (unsigned short)((i << 8) | k);
     int ellRows = 0;
     if (gaunt) {
         std::memcpy(g_stage + offHoff, ang->gaunt_off, sizeof(int) * (n * n + 1));
@@ -214,7 +207,11 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     a.condHMax = opts->cond_h_max;
     a.deltaPPn = opts->delta_ppn;
     a.tolGamma = opts->tol_gamma;
-    if (plan_newton(a) != 0)
+    a.mixed = opts->precision == CL_MIXED;
+    const int pl = plan_newton(a);
+    if (pl == -2)
+        return fail(CL_ERR_ARG, "mixed precision needs a configuration with at most 16 Hessian column tiles");
+    if (pl != 0)
         return fail(CL_ERR_ARG, "Newton kernel layout does not fit in shared memory");
     if ((e = prepare_newton(a)) != cudaSuccess)
         return fail(CL_ERR_CUDA, cudaGetErrorString(e));

@@ -233,6 +233,16 @@ int build_angular(int order, int Q, int useGaunt, Angular &A)
 
 namespace clb {
 
+void product_columns(int n, unsigned short *pairs)
+{
+    int c = 0;
+    for (int i = 0; i < n; i++)
+        pairs[c++] = (unsigned short)(i << 8);
+    for (int i = 1; i < n; i++)
+        for (int j = 1; j <= i; j++)
+            pairs[c++] = (unsigned short)((i << 8) | j);
+}
+
 int build_gaunt_ell(int n, const int *off, const int *idx, const double *val, unsigned short *pair,
                     unsigned short *eidx, double *eval, int *eoff, int maxRows)
 {

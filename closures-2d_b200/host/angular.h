@@ -33,4 +33,10 @@ int build_gaunt_ell(int n, const int *off, const int *idx, const double *val, un
                     unsigned short *eidx, double *eval, int *eoff, int maxRows);
 inline int gaunt_ell_chunks(int n) { return (n * (n + 1) / 2 + 31) / 32; }
 
+// Column order of the packed Hessian products p_i p_j (j <= i) used without
+// the Gaunt table: the n products with p_0 first (they hold the gradient and
+// f, which mixed precision keeps in FP64), then j >= 1 row by row.  Fills
+// pairs[n(n+1)/2] with (i << 8) | j.
+void product_columns(int n, unsigned short *pairs);
+
 }  // namespace clb
