@@ -372,3 +372,277 @@ int orc_opt_batch(const orc_setup *s, orc_options opts, int count, double *u, do
     }
     return worst;
 }
+
+
+/* ---------------------------------------------------------------------- */
+/* Change-of-basis Newton: opt/optcb.cpp (MOMOPT_OPTIMIZATION_TYPE 1).     */
+/* The per-cell basis P2M (lower triangular, row-major here; the reference  */
+/* keeps it column-major for BLAS) and the multipliers alphaP in that basis */
+/* persist between calls.  The BLAS operations optcb.cpp calls are          */
+/* restated as row-major lower-triangular loops below.                      */
+
+/* x <- A^-1 x (dtrsv L,N,N) */
+static void trsv_l(int n, const double *a, double *x)
+{
+    for (int i = 0; i < n; i++) {
+        double s = x[i];
+        for (int k = 0; k < i; k++)
+            s -= a[i * n + k] * x[k];
+        x[i] = s / a[i * n + i];
+    }
+}
+
+/* x <- A^-T x (dtrsv L,T,N) */
+static void trsv_lt(int n, const double *a, double *x)
+{
+    for (int i = n - 1; i >= 0; i--) {
+        double s = x[i];
+        for (int k = i + 1; k < n; k++)
+            s -= a[k * n + i] * x[k];
+        x[i] = s / a[i * n + i];
+    }
+}
+
+/* x <- A x (dtrmv L,N,N) */
+static void trmv_l(int n, const double *a, double *x)
+{
+    for (int i = n - 1; i >= 0; i--) {
+        double s = 0.0;
+        for (int k = 0; k <= i; k++)
+            s += a[i * n + k] * x[k];
+        x[i] = s;
+    }
+}
+
+/* x <- A^T x (dtrmv L,T,N) */
+static void trmv_lt(int n, const double *a, double *x)
+{
+    for (int i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int k = i; k < n; k++)
+            s += a[k * n + i] * x[k];
+        x[i] = s;
+    }
+}
+
+/* B <- B A for lower-triangular B and A (dtrmm R,L,N,N) */
+static void trmm_rl(int n, double *b, const double *a)
+{
+    double row[ORC_NMAX];
+    for (int i = 0; i < n; i++) {
+        for (int j = 0; j <= i; j++) {
+            double s = 0.0;
+            for (int k = j; k <= i; k++)
+                s += b[i * n + k] * a[k * n + j];
+            row[j] = s;
+        }
+        for (int j = 0; j <= i; j++)
+            b[i * n + j] = row[j];
+    }
+}
+
+static void set_identity(int n, double *a)
+{
+    memset(a, 0, sizeof(double) * (size_t)n * (size_t)n);
+    for (int i = 0; i < n; i++)
+        a[i * n + i] = 1.0;
+}
+
+/* pP <- P2M^-1 p for every quadrature point (dtrsm L,L,N,N on the nm x nq
+ * block whose columns are the points' basis vectors); p has row stride np. */
+static void basis_to_p(int nm, int nq, const double *T, const double *p, int np, double *pP)
+{
+    for (int q = 0; q < nq; q++) {
+        double *x = pP + (size_t)q * nm;
+        for (int k = 0; k < nm; k++)
+            x[k] = p[(size_t)q * np + k];
+        trsv_l(nm, T, x);
+    }
+}
+
+/* optcb.cpp:156-415 */
+static int optcb_scaled(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
+                        const double *w, const double *p, int np, orc_options *o, orc_outs *outs)
+{
+    double f = 0.0;
+    double alphaP0[ORC_NMAX], dP[ORC_NMAX], gP[ORC_NMAX], uP[ORC_NMAX], gM[ORC_NMAX];
+    double chol[ORC_NMAX * ORC_NMAX], hP[ORC_NMAX * ORC_NMAX], P2Min[ORC_NMAX * ORC_NMAX];
+    double work[3 * ORC_NMAX];
+    double gExt[ORC_N2MAX];
+    int iwork[ORC_NMAX];
+    double *pP = (double *)malloc(sizeof(double) * (size_t)nq * nm);
+    if (!pP)
+        return ORC_ERR_INPUT;
+    int status = ORC_OK;
+    memcpy(alphaP0, alphaP, sizeof(double) * nm);
+    memcpy(P2Min, P2M, sizeof(double) * (size_t)nm * (size_t)nm);
+    basis_to_p(nm, nq, P2Min, p, np, pP);
+    int maxIter = o->maxIter;
+    const double tolRel = o->tolRel;
+    double r = 0.0;
+    const double condHMax = o->condHMax;
+    int regIndex = 0;
+    memcpy(uP, u, sizeof(double) * nm);
+    trsv_l(nm, P2M, uP);
+    double rtol = orc_nrm2(nm, u) * tolRel;
+    int iter = 0, totalIter = 0;
+    double t = 1.0, err = 0.0;
+    int hitMaxRegularization = 0;
+
+    while (1) {
+        iter = iter + 1;
+        totalIter = totalIter + 1;
+        f = orc_fobj(o->momentType, nm, nm, nq, alphaP, uP, w, pP, o->deltaPPn, gP, hP, 0, NULL,
+                     gExt);
+        memcpy(chol, hP, sizeof(double) * (size_t)nm * (size_t)nm);
+        int error = orc_cholesky(nm, chol);
+        double norm = orc_norm1(nm, hP);
+        double condest = 1.0 / orc_rcond(nm, chol, norm, work, iwork);
+
+        /* a bad Hessian at the very first evaluation: isotropic alpha and the
+         * standard basis (optcb.cpp:247-265) */
+        if (totalIter == 1 && (error != 0 || condest > condHMax)) {
+            isotropic_alpha(nm, alphaP0, o->momentType, o->deltaPPn);
+            set_identity(nm, P2M);
+            set_identity(nm, P2Min);
+            memcpy(alphaP, alphaP0, sizeof(double) * nm);
+            memcpy(uP, u, sizeof(double) * nm);
+            for (int q = 0; q < nq; q++)
+                for (int k = 0; k < nm; k++)
+                    pP[(size_t)q * nm + k] = p[(size_t)q * np + k];
+            rtol = orc_nrm2(nm, u) * tolRel;
+            iter = 0;
+            t = 1.0;
+            continue;
+        }
+
+        /* optcb.cpp:268-318 */
+        if (iter >= maxIter || error != 0 || t == 0 || condest > condHMax) {
+            if (regIndex < ORC_NUM_REG - 1) {
+                regIndex++;
+                r = ORC_REGULARIZATIONS[regIndex];
+                uP[0] = 1.0;
+                for (int i = 1; i < nm; i++)
+                    uP[i] = u[i] * (1.0 - r);
+            } else {
+                if (hitMaxRegularization) {
+                    status = ORC_ERR_MAXREG;   /* "This should never happen." */
+                    break;
+                }
+                isotropic_alpha(nm, alphaP0, o->momentType, o->deltaPPn);
+                set_identity(nm, P2Min);
+                memcpy(uP, u, sizeof(double) * nm);
+                regIndex = 0;   /* r keeps its last value, as optcb.cpp:288-296 */
+                hitMaxRegularization = 1;
+                maxIter = o->maxIter;
+            }
+            rtol = orc_nrm2(nm, uP) * tolRel;
+            memcpy(alphaP, alphaP0, sizeof(double) * nm);
+            memcpy(P2M, P2Min, sizeof(double) * (size_t)nm * (size_t)nm);
+            trsv_l(nm, P2M, uP);
+            basis_to_p(nm, nq, P2Min, p, np, pP);
+            iter = 0;
+            t = 1.0;
+            if (regIndex == ORC_NUM_REG - 1)
+                maxIter = 10 * maxIter;
+            continue;
+        }
+
+        /* change of basis by the Cholesky factor L of hP (optcb.cpp:321-332) */
+        trsv_l(nm, chol, gP);
+        for (int q = 0; q < nq; q++)
+            trsv_l(nm, chol, pP + (size_t)q * nm);
+        trmm_rl(nm, P2M, chol);
+        trmv_lt(nm, chol, alphaP);
+        trsv_l(nm, chol, uP);
+        for (int i = 0; i < nm; i++)
+            dP[i] = -gP[i];
+        /* the gradient in the moment basis measures the error (:340-344) */
+        memcpy(gM, gP, sizeof(double) * nm);
+        trmv_l(nm, P2M, gM);
+        err = orc_nrm2(nm, gM);
+        if (err <= rtol) {
+            memcpy(alphaM, alphaP, sizeof(double) * nm);
+            trsv_lt(nm, P2M, alphaM);
+            u[0] = 1.0;
+            for (int i = 1; i < nm; i++)
+                u[i] = u[i] * (1.0 - r);
+            break;
+        }
+        t = linesearch(nm, nm, nq, alphaP, dP, f, gP, uP, w, pP, o->deltaPPn, o->momentType, gExt);
+    }
+    if (outs != NULL) {
+        outs->iter = totalIter;
+        outs->normG = err;
+        outs->r = r;
+    }
+    free(pP);
+    return status;
+}
+
+/* optcb.cpp:87-153: scaling wrapper */
+int orc_optcb(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
+              orc_options options, const double *w, const double *p, int np, orc_outs *outs)
+{
+    if (nm > ORC_NMAX)
+        return ORC_ERR_INPUT;
+    const double u0 = u[0];
+    if (u0 <= 0)
+        return ORC_ERR_U0;
+    int status;
+    if (options.momentType == ORC_MN) {
+        const double alphaScale = log(u0) * 2.0 * sqrt(M_PI);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] / u0;
+        status = optcb_scaled(nm, nq, u, P2M, alphaP, alphaM, w, p, np, &options, outs);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] * u0;
+        alphaM[0] = alphaM[0] + alphaScale;
+    } else if (options.momentType == ORC_PPN) {
+        options.deltaPPn = options.deltaPPn / (u0 * u0);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] / u0;
+        status = optcb_scaled(nm, nq, u, P2M, alphaP, alphaM, w, p, np, &options, outs);
+        for (int i = 0; i < nm; i++) {
+            alphaM[i] = alphaM[i] * u0;
+            u[i] = u[i] * u0;
+        }
+    } else {
+        return ORC_ERR_INPUT;
+    }
+    return status;
+}
+
+/* momopt_init.cpp:146-157: alphaP isotropic and the P2M block with its first
+ * nm entries (column-major: the first column) set to one -- singular, so a
+ * cell's first solve takes the first-evaluation reset to the standard basis. */
+void orc_optcb_init(int nm, int momentType, double delta, double *P2M, double *alphaP)
+{
+    memset(P2M, 0, sizeof(double) * (size_t)nm * (size_t)nm);
+    for (int k = 0; k < nm; k++)
+        P2M[k * nm + 0] = 1.0;
+    isotropic_alpha(nm, alphaP, momentType, delta);
+}
+
+int orc_optcb_batch(const orc_setup *s, orc_options opts, int count, double *u, double *P2M,
+                    double *alphaP, double *alpha, int *iters, double *regs, int *status)
+{
+    const int n = s->n;
+    int worst = ORC_OK;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < count; c++) {
+        orc_outs outs = {0.0, 0, 0.0};
+        int st = orc_optcb(n, s->nq, u + (size_t)c * n, P2M + (size_t)c * n * n, alphaP + (size_t)c * n,
+                           alpha + (size_t)c * n, opts, s->w, s->p, s->n2, &outs);
+        if (iters)
+            iters[c] = outs.iter;
+        if (regs)
+            regs[c] = outs.r;
+        status[c] = st;
+        if (st != ORC_OK) {
+#pragma omp critical
+            worst = st;
+        }
+    }
+    return worst;
+}

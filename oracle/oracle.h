@@ -97,6 +97,17 @@ int orc_opt(int n, int n2, int nq, double *u, double *alpha, orc_options opts,
 int orc_opt_batch(const orc_setup *s, orc_options opts, int count,
                   double *u, double *alpha, int *iters, double *regs, int *status);
 
+/* Change-of-basis Newton, opt/optcb.cpp (MOMOPT_OPTIMIZATION_TYPE 1).  P2M
+ * (nm x nm lower triangular, row-major) and alphaP persist per cell and are
+ * updated in place; alphaM receives the multipliers in the moment basis.  p
+ * is the basis with row stride np (the setup's n2). */
+int orc_optcb(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
+              orc_options opts, const double *w, const double *p, int np, orc_outs *outs);
+/* momopt_init.cpp:146-157 initial state of a cell (see opt.c). */
+void orc_optcb_init(int nm, int momentType, double delta, double *P2M, double *alphaP);
+int orc_optcb_batch(const orc_setup *s, orc_options opts, int count, double *u, double *P2M,
+                    double *alphaP, double *alpha, int *iters, double *regs, int *status);
+
 /* f,g,H evaluation (fobj.cpp); g and h may be NULL as in the reference. */
 double orc_fobj(int momentType, int n, int n2, int nq, const double *alpha,
                 const double *u, const double *w, const double *p, double delta,
@@ -131,6 +142,7 @@ typedef struct {
     double dx, dy, maxDt;
     double *initialGrid, *sigmaT, *sigmaS;   /* [NX*NY] */
     double *moments, *alpha, *flux, *momentsOld, *ansatzGrid;
+    double *alphaP, *P2M;   /* change-of-basis state per cell (optType 1) */
     orc_stats stats;
     int *lastIters;         /* per-cell iterations of the last stage */
     int status;             /* first error code seen */

@@ -28,6 +28,35 @@ int orc_batch(int order, int Q, int useGaunt, int momentType, int maxIter, doubl
     return st;
 }
 
+/* Batched change-of-basis opt (optcb.cpp) with per-vector P2M and alphaP
+ * state, in place. */
+int orc_batch_cb(int order, int Q, int momentType, int maxIter, double tol, double condHMax,
+                 double deltaPPn, int count, double *u, double *P2M, double *alphaP, double *alpha,
+                 int *iters, double *regs, int *status)
+{
+    orc_setup s;
+    int st = orc_setup_create(order, Q, 0, &s);
+    if (st)
+        return st;
+    orc_options o;
+    memset(&o, 0, sizeof(o));
+    o.momentType = momentType;
+    o.maxIter = maxIter;
+    o.tolRel = tol;
+    o.condHMax = condHMax;
+    o.deltaPPn = deltaPPn;
+    st = orc_optcb_batch(&s, o, count, u, P2M, alphaP, alpha, iters, regs, status);
+    orc_setup_free(&s);
+    return st;
+}
+
+/* The reference's initial change-of-basis state for count cells. */
+void orc_cb_init(int n, int momentType, double delta, int count, double *P2M, double *alphaP)
+{
+    for (int c = 0; c < count; c++)
+        orc_optcb_init(n, momentType, delta, P2M + (size_t)c * n * n, alphaP + (size_t)c * n);
+}
+
 /* Angular set-up copied into caller buffers (sizes from orc_setup_dims). */
 int orc_setup_dims(int order, int Q, int useGaunt, int *n, int *n2, int *nq, int *nnz)
 {

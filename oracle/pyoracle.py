@@ -61,6 +61,10 @@ def _bind(L):
         L.orc_solver_stats.argtypes = [vp, ip, dp, C.POINTER(C.c_longlong), ip]
         L.orc_solver_close.argtypes = [vp]
         L.orc_solver_last_iters.argtypes = [vp, ip]
+        L.orc_batch_cb.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                   C.c_double, C.c_int, dp, dp, dp, dp, ip, dp, ip]
+        L.orc_cb_init.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, dp, dp]
+        L.orc_cb_init.restype = None
     return L
 
 
@@ -98,6 +102,28 @@ def opt_batch(order, Q, use_gaunt, u, alpha, moment_type=0, max_iter=100, tol=1e
     status = np.zeros(count, np.int32)
     lib(fma).orc_batch(order, Q, int(use_gaunt), moment_type, max_iter, tol, cond_h_max, delta_ppn,
                     tol_gamma, count, _dp(u), _dp(alpha), _ip(iters), _dp(regs), _ip(status))
+    return iters, regs, status
+
+
+def cb_init(n, count, moment_type=0, delta_ppn=1e-10):
+    """The reference's initial change-of-basis state (P2M [count][n][n]
+    row-major lower triangular, alphaP [count][n])."""
+    P2M = np.zeros((count, n, n))
+    alphaP = np.zeros((count, n))
+    lib().orc_cb_init(n, moment_type, delta_ppn, count, _dp(P2M), _dp(alphaP))
+    return P2M, alphaP
+
+
+def optcb_batch(order, Q, u, P2M, alphaP, alpha, moment_type=0, max_iter=100, tol=1e-8,
+                cond_h_max=1e10, delta_ppn=1e-10, fma=False):
+    """Change-of-basis opt (optcb.cpp) on each row in place: u, P2M, alphaP
+    updated, alpha receives the multipliers.  Returns iters, regs, status."""
+    count = u.shape[0]
+    iters = np.zeros(count, np.int32)
+    regs = np.zeros(count)
+    status = np.zeros(count, np.int32)
+    lib(fma).orc_batch_cb(order, Q, moment_type, max_iter, tol, cond_h_max, delta_ppn, count, _dp(u),
+                          _dp(P2M), _dp(alphaP), _dp(alpha), _ip(iters), _dp(regs), _ip(status))
     return iters, regs, status
 
 

@@ -165,7 +165,7 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
 {
     memset(s, 0, sizeof(*s));
     s->deck = *d;
-    if (d->optType != 0 || (d->momentType != ORC_MN && d->momentType != ORC_PPN))
+    if ((d->optType != 0 && d->optType != 1) || (d->momentType != ORC_MN && d->momentType != ORC_PPN))
         return ORC_ERR_INPUT;
     const int ng = 2;
     int sizeX = d->numCellsX, sizeY = d->numCellsY;
@@ -247,6 +247,13 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
     s->momentsOld = (double *)calloc(C * n, sizeof(double));
     s->ansatzGrid = (double *)malloc(sizeof(double) * C);
     s->lastIters = (int *)calloc(C, sizeof(int));
+    if (d->optType == 1) {
+        /* momopt_init.cpp:114-157 */
+        s->alphaP = (double *)malloc(sizeof(double) * C * n);
+        s->P2M = (double *)malloc(sizeof(double) * C * n * n);
+        for (size_t c = 0; c < C; c++)
+            orc_optcb_init(n, d->momentType, d->deltaPPn, s->P2M + c * n * n, s->alphaP + c * n);
+    }
     /* momopt_init.cpp:120-143 */
     for (int i = s->gX[0]; i <= s->gX[3]; i++)
         for (int j = s->gY[0]; j <= s->gY[3]; j++) {
@@ -279,6 +286,8 @@ void orc_solver_free(orc_solver *s)
     free(s->momentsOld);
     free(s->ansatzGrid);
     free(s->lastIters);
+    free(s->alphaP);
+    free(s->P2M);
     orc_setup_free(&s->set);
     memset(s, 0, sizeof(*s));
 }
@@ -320,7 +329,13 @@ static void solve_optimization(orc_solver *s)
 #pragma omp parallel for schedule(dynamic, 1)
     for (long index = 0; index < (long)C; index++) {
         orc_outs outs = {0.0, 0, 0.0};
-        int st = orc_opt(n, s->set.n2, s->set.nq, &s->moments[(size_t)index * n],
+        int st;
+        if (d->optType == 1)
+            st = orc_optcb(n, s->set.nq, &s->moments[(size_t)index * n], &s->P2M[(size_t)index * n * n],
+                           &s->alphaP[(size_t)index * n], &s->alpha[(size_t)index * n], o, s->set.w,
+                           s->set.p, s->set.n2, &outs);
+        else
+            st = orc_opt(n, s->set.n2, s->set.nq, &s->moments[(size_t)index * n],
                          &s->alpha[(size_t)index * n], o, s->set.w, s->set.p, &s->set.gaunt, &outs);
         s->lastIters[index] = outs.iter;
 #pragma omp critical
