@@ -91,6 +91,7 @@ def lib():
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
             "cl_solve_batch_device_start": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp]),
+            "cl_solve_batch_cb_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]),
             "cl_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
             "cl_multi_create": (C.c_int, [C.c_int, ip, C.c_int, C.c_int, C.POINTER(cl_options),
                                           C.POINTER(vp)]),
@@ -313,6 +314,15 @@ class Context:
         _check(lib().cl_solve_batch_device_start(self._ctx, count, ptr(d_u), ptr(d_alpha),
                                                  ptr(d_alpha_start), ptr(d_iters), ptr(d_reg),
                                                  ptr(d_status)), self._err)
+
+    def solve_batch_cb_device(self, d_u, d_P2M, d_alphaP, d_alpha, d_iters=None, d_reg=None,
+                              d_status=None, count=None):
+        """Change-of-basis solve (opt_type 1 contexts): per-vector basis and
+        alphaP state in/out, alpha out (moment basis)."""
+        ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
+        _check(lib().cl_solve_batch_cb_device(self._ctx, count, ptr(d_u), ptr(d_P2M), ptr(d_alphaP),
+                                              ptr(d_alpha), ptr(d_iters), ptr(d_reg), ptr(d_status)),
+               self._err)
 
     def set_warm_start(self, mlp):
         """Predict alpha with `mlp` before every optimisation stage (None: off).

@@ -194,9 +194,9 @@ int check_options(const cl_options *o, std::string &err)
         err = "null options";
         return CL_ERR_ARG;
     }
-    if (o->opt_type != 0) {
+    if (o->opt_type != 0 && o->opt_type != 1) {
         err = "MOMOPT_OPTIMIZATION_TYPE " + std::to_string(o->opt_type) +
-              " (change of basis / BFGS) is not provided by the B200 path";
+              " (BFGS) is not provided by the B200 path";
         return CL_ERR_ARG;
     }
     if (o->moment_type != CL_MN && o->moment_type != CL_PPN) {
@@ -223,6 +223,7 @@ void fill_newton_options(NewtonArgs &a, const cl_options &o, int useGaunt)
     a.condHMax = o.cond_h_max;
     a.deltaPPn = o.delta_ppn;
     a.mixed = o.precision == CL_MIXED;
+    a.optType = o.opt_type;
     a.tolGamma = o.tol_gamma;
 }
 
@@ -266,6 +267,8 @@ struct cl_ctx {
     int *dIters = nullptr;            // [C] iterations of each cell in the last stage
     cl_mlp *warm = nullptr;           // learned warm start (null: previous stage's alpha)
     double *dAlphaPred = nullptr;     // [C][n] predicted starts when warm is set
+    double *dP2M = nullptr, *dAlphaP = nullptr;   // change-of-basis state per cell (opt type 1)
+    double *dCbScratch = nullptr;     // working basis per Newton slot (opt type 1)
     NewtonArgs nargs;
     FluxArgs fargs;
     int nCtas = 0;
@@ -384,7 +387,10 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     ctx->C = (long long)ctx->NX * ctx->NY;
     const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
     CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, ang->use_gaunt, ang->w, ang->xi,
+    // the change-of-basis solve forms its Hessians from the basis products
+    // (optcb.cpp calls fobj without the Gaunt table)
+    const int gauntNewton = (opts->opt_type == 1) ? 0 : ang->use_gaunt;
+    cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi,
                                         ang->eta, ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
                                         ang->gaunt_nnz);
     if (ce != cudaSuccess) {
@@ -413,11 +419,31 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     memset(&a, 0, sizeof(a));
     a.nprob = 1;
     a.prob[0] = make_problem(ctx->B);
-    fill_newton_options(a, *opts, ang->use_gaunt);
+    fill_newton_options(a, *opts, gauntNewton);
     a.stats = ctx->dStats;
     a.err = ctx->dErr;
     a.NX = ctx->NX;
     a.NY = ctx->NY;
+    if (opts->opt_type == 1) {
+        // momopt_init.cpp:146-157: alphaP isotropic, and the first n entries
+        // of each P2M block (its first column, as the reference stores it
+        // column-major) set to one -- singular, so each cell's first solve
+        // takes the first-evaluation reset to the standard basis
+        std::vector<double> hP2M(C * n * n, 0.0), hAP(C * n, 0.0);
+        const double a0 = (opts->moment_type == CL_MN) ? 2.0 * std::sqrt(M_PI) * std::log(0.5 / std::sqrt(M_PI))
+                                                       : 1.0 - 4.0 * opts->delta_ppn * M_PI;
+        for (size_t c = 0; c < C; c++) {
+            for (size_t k = 0; k < n; k++)
+                hP2M[c * n * n + k * n] = 1.0;
+            hAP[c * n] = a0;
+        }
+        if (upload(&ctx->dP2M, hP2M) != cudaSuccess || upload(&ctx->dAlphaP, hAP) != cudaSuccess) {
+            ctx->err = "device allocation failed";
+            return ctx_fail(ctx, CL_ERR_CUDA);
+        }
+        a.prob[0].P2M = ctx->dP2M;
+        a.prob[0].alphaP = ctx->dAlphaP;
+    }
     const int pl = plan_newton(a);
     if (pl != 0) {
         ctx->err = pl == -2 ? "mixed precision needs a configuration with at most 16 Hessian column tiles"
@@ -429,6 +455,13 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
     ctx->nCtas = sm_count() * newton_ctas_per_sm(a);
+    if (opts->opt_type == 1) {
+        if (cudaMalloc(&ctx->dCbScratch, (size_t)ctx->nCtas * a.T * kCbSlotDoubles * sizeof(double)) != cudaSuccess) {
+            ctx->err = "device allocation failed";
+            return ctx_fail(ctx, CL_ERR_CUDA);
+        }
+        a.cbScratch = ctx->dCbScratch;
+    }
 
     FluxArgs &f = ctx->fargs;
     memset(&f, 0, sizeof(f));
@@ -491,6 +524,9 @@ void cl_destroy(cl_ctx *ctx)
     cudaFreeHost(ctx->hErr);
     cudaFree(ctx->dIters);
     cudaFree(ctx->dAlphaPred);
+    cudaFree(ctx->dP2M);
+    cudaFree(ctx->dAlphaP);
+    cudaFree(ctx->dCbScratch);
     cudaFree(ctx->bU);
     cudaFree(ctx->bA);
     cudaFree(ctx->bR);
@@ -781,6 +817,10 @@ int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_a
 {
     if (!ctx || count < 0 || (count > 0 && (!d_u || !d_alpha)))
         return CL_ERR_ARG;
+    if (ctx->nargs.optType == 1) {
+        ctx->err = "change-of-basis contexts solve batches with cl_solve_batch_cb_device";
+        return CL_ERR_STATE;
+    }
     if (count == 0)
         return CL_OK;
     NewtonArgs a = ctx->nargs;
@@ -791,6 +831,35 @@ int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_a
     a.prob[0].regs = d_reg;
     a.prob[0].status = d_status;
     a.prob[0].alphaStart = d_alpha_start;
+    a.prob[0].queue = ctx->dQueue + 2;
+    a.momentsOld = nullptr;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dQueue + 2, 0, sizeof(unsigned), ctx->stream));
+    CUDA_TRY(ctx, launch_newton(a, ctx->nCtas, ctx->stream));
+    g_launches += 1;
+    return CL_OK;
+}
+
+int cl_solve_batch_cb_device(cl_ctx *ctx, int count, double *d_u, double *d_P2M, double *d_alphaP,
+                             double *d_alpha, int *d_iters, double *d_reg, int *d_status)
+{
+    if (!ctx || count < 0 || (count > 0 && (!d_u || !d_P2M || !d_alphaP || !d_alpha)))
+        return CL_ERR_ARG;
+    if (ctx->nargs.optType != 1) {
+        ctx->err = "the context was not created for MOMOPT_OPTIMIZATION_TYPE 1";
+        return CL_ERR_STATE;
+    }
+    if (count == 0)
+        return CL_OK;
+    NewtonArgs a = ctx->nargs;
+    a.prob[0].count = count;
+    a.prob[0].u = d_u;
+    a.prob[0].alpha = d_alpha;
+    a.prob[0].P2M = d_P2M;
+    a.prob[0].alphaP = d_alphaP;
+    a.prob[0].iters = d_iters;
+    a.prob[0].regs = d_reg;
+    a.prob[0].status = d_status;
+    a.prob[0].alphaStart = nullptr;
     a.prob[0].queue = ctx->dQueue + 2;
     a.momentsOld = nullptr;
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dQueue + 2, 0, sizeof(unsigned), ctx->stream));
@@ -891,6 +960,10 @@ int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaun
     if (rc) {
         g_global_err = e;
         return rc;
+    }
+    if (opts->opt_type != 0) {
+        g_global_err = "the change-of-basis solve runs one moment order per context (cl_create)";
+        return CL_ERR_ARG;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {

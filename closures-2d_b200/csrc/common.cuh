@@ -10,6 +10,10 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kMaxN = 32;            // moments per cell handled by one warp (order <= 6)
 constexpr int kMaxProblems = 8;      // moment orders sharing one persistent launch
 constexpr int kNumReg = 5;
+// change-of-basis working state of one Newton slot in global memory: the
+// basis T and the rows of L^-1 ([kMaxN][kMaxN] each), then alphaP, the
+// line-search alphaM and step, and 1/T_ii ([kMaxN] each)
+constexpr int kCbSlotDoubles = 2 * kMaxN * kMaxN + 4 * kMaxN;
 
 // opt/opt.h:39-40
 __device__ __constant__ const double kRegularizations[kNumReg] = {0.0, 1e-3, 1e-2, 1e-1, 5e-1};

@@ -48,6 +48,7 @@ int plan_newton(NewtonArgs &a)
     a.offEllOff = take((ellChunks + 2) / 2);
     a.offExp = take(64);
     a.offBar = take(4);
+
     exp_consts_init(a.ex);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
@@ -65,6 +66,7 @@ int plan_newton(NewtonArgs &a)
     int offH = offG + ((T * a.ldG + 1) & ~1);
     int offVec = offH + ((kWarps * kMaxN * a.ldh + 1) & ~1);
     int endB = offVec + kWarps * 64;
+
     // phase-A region
     const int maxDoubles = (232448 - 1024) / 8;   // opt-in limit minus static shared
     if (a.ntf > 0) {

@@ -42,6 +42,10 @@ struct NewtonProblem {
     double *u, *alpha;          // [count][n]; alpha: start (or fallback start) in, solution out
     const double *alphaStart;   // nullable [count][n]: predicted start; alpha is then the
                                 // fallback taken (once) before the first regularisation
+    // change-of-basis Newton (MOMOPT_OPTIMIZATION_TYPE 1): per-vector basis
+    // P2M [count][n][n] (row-major lower triangular) and alphaP [count][n],
+    // read at the start and written back on convergence; null otherwise
+    double *P2M, *alphaP;
     int *iters;                 // nullable [count]
     double *regs;               // nullable [count]
     int *status;                // nullable [count]
@@ -50,8 +54,8 @@ struct NewtonProblem {
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
 enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
-enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_N };
-enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_N };
+enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_R, SC_N };
+enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_CB, SI_N };
 
 struct NewtonArgs {
     NewtonProblem prob[kMaxProblems];
@@ -76,6 +80,8 @@ struct NewtonArgs {
     int ntExact, nbk;           // single problem on the fused path: its column tiles and
                                 // GEMM1 k-steps (selects a specialised instance), else 0
     int mixed;                  // Hessian-only tiles by split TF32 (CL_MIXED); needs ntExact
+    int optType;                // 0 Newton (opt.cpp), 1 change of basis (optcb.cpp)
+    double *cbScratch;          // optType 1: per-slot working state, [grid][T][kCbSlotDoubles]
 };
 
 // Fills the layout fields from the problems' sizes; returns 0, -1 when the

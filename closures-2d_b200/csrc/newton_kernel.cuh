@@ -697,6 +697,508 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     regularize(a, pb, L, s, lane, ldv, ui, ai);
 }
 
+// ---------------------------------------------------------------------------
+// Change-of-basis Newton (MOMOPT_OPTIMIZATION_TYPE 1, opt/optcb.cpp:156-415).
+// Each vector carries a lower-triangular basis T (P2M) and multipliers alphaP
+// in that basis.  Exponents and f do not depend on the basis (alphaP.pP_q =
+// alphaM.p_q with alphaM = T^-T alphaP), so phase A evaluates at alphaM with
+// the shared basis as for plain Newton; phase B forms the Hessian in the
+// working basis, H_P = T^-1 H_M T^-T, and the gradient g_P = T^-1 g_M by two
+// triangular solves, factors H_P = L L^T, takes the reference's decisions on
+// it (first-evaluation reset, regularisation), and changes the basis
+// T <- T L, alphaP <- L^T alphaP, g_P <- L^-1 g_P, so the Newton step in the
+// new basis is d_P = -g_P (the moment-basis step is (T L)^-T d_P).  The
+// working state of a slot (T, L^-1, alphaP, the line search's alphaM and
+// step) lives in global scratch, L1/L2-resident, so shared memory stays as for
+// plain Newton; the vector's stored basis and alphaP are the start of every
+// regularisation restart and are written back on convergence.
+enum { CB_START_STD = 1, CB_HIT_MAX = 2 };
+
+__device__ __forceinline__ double *cb_slot(const NewtonArgs &a, int s)
+{
+    return a.cbScratch + ((size_t)blockIdx.x * a.T + s) * kCbSlotDoubles;
+}
+__device__ __forceinline__ double *cb_basis(const NewtonArgs &a, int s) { return cb_slot(a, s); }
+__device__ __forceinline__ double *cb_linv(const NewtonArgs &a, int s) { return cb_slot(a, s) + kMaxN * kMaxN; }
+__device__ __forceinline__ double *cb_ap(const NewtonArgs &a, int s) { return cb_slot(a, s) + 2 * kMaxN * kMaxN; }
+__device__ __forceinline__ double *cb_am(const NewtonArgs &a, int s) { return cb_ap(a, s) + kMaxN; }
+__device__ __forceinline__ double *cb_dm(const NewtonArgs &a, int s) { return cb_ap(a, s) + 2 * kMaxN; }
+__device__ __forceinline__ double *cb_rdiag(const NewtonArgs &a, int s) { return cb_ap(a, s) + 3 * kMaxN; }
+
+// x = T^-T y (lane i holds y_i, returns x_i): backward substitution with the
+// reciprocal diagonal, x_i = (y_i - sum_{k>i} T_ki x_k) / T_ii.
+__device__ double cb_solve_t(const double *Tg, double y, int n, int lane)
+{
+    const double rl = (lane < n) ? 1.0 / Tg[lane * kMaxN + lane] : 0.0;
+    double acc = 0.0, x = 0.0;
+    for (int i = n - 1; i >= 0; i--) {
+        const double xi = __shfl_sync(0xffffffffu, (y - acc) * rl, i);
+        if (lane == i)
+            x = xi;
+        if (lane < i)
+            acc = fma(Tg[i * kMaxN + lane], xi, acc);
+    }
+    return (lane < n) ? x : 0.0;
+}
+
+// Columns held per lane (lane j: m[i] = M_ij) replaced by those of T^-1 M:
+// forward substitution by rows, row i of T (stride kMaxN) read by every lane
+// (one broadcast), rd[i] = 1/T_ii.
+__device__ __forceinline__ void cb_trsv_cols(const double *Tg, const double *rd, double (&m)[kMaxN], int n)
+{
+#pragma unroll
+    for (int i = 0; i < kMaxN; i++) {
+        if (i < n) {
+            const double *Ti = Tg + i * kMaxN;
+            double a0 = m[i], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+            for (int k = 0; k + 1 < i; k += 2) {
+                const double2 l = *reinterpret_cast<const double2 *>(Ti + k);
+                if (k & 2) {
+                    a2 = fma(-l.x, m[k], a2);
+                    a3 = fma(-l.y, m[k + 1], a3);
+                } else {
+                    a0 = fma(-l.x, m[k], a0);
+                    a1 = fma(-l.y, m[k + 1], a1);
+                }
+            }
+            if (i & 1)
+                a1 = fma(-Ti[i - 1], m[i - 1], a1);
+            m[i] = ((a0 + a1) + (a2 + a3)) * rd[i];
+        }
+    }
+}
+
+// alphaM = T^-T alphaP for the slot (working basis), into L.alpha.
+__device__ void cb_set_alpha_m(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane)
+{
+    const int n = pb.n, ldv = a.ldv;
+    const double ap = (lane < n) ? cb_ap(a, s)[lane] : 0.0;
+    const double am = cb_solve_t(cb_basis(a, s), ap, n, lane);
+    __syncwarp();
+    if (lane < n)
+        L.alpha[s * ldv + lane] = am;
+    __syncwarp();
+}
+
+// Working basis <- the vector's stored basis, or the identity after a
+// restart in the standard basis; alphaP likewise (optcb.cpp:247-318).
+__device__ void cb_restart_state(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane)
+{
+    const int n = pb.n, ldv = a.ldv;
+    const int cell = L.ints[s * SI_N + SI_CELL];
+    const bool std_ = (L.ints[s * SI_N + SI_CB] & CB_START_STD) != 0;
+    double *Tg = cb_basis(a, s);
+    const double *T0 = pb.P2M + (size_t)cell * n * n;
+    for (int i = 0; i < n; i++)
+        if (lane < n)
+            Tg[i * kMaxN + lane] = std_ ? (i == lane ? 1.0 : 0.0) : T0[i * n + lane];
+    if (lane < n)
+        cb_rdiag(a, s)[lane] = std_ ? 1.0 : 1.0 / T0[lane * n + lane];
+    double ap;
+    if (std_) {
+        const double a0 = (a.momentType == 0) ? 2.0 * kSqrtPi * log(0.5 / kSqrtPi)
+                                              : 1.0 - 4.0 * L.scal[s * SC_N + SC_DELTA] * kPi;
+        ap = (lane == 0) ? a0 : 0.0;
+    } else {
+        ap = (lane < n) ? pb.alphaP[(size_t)cell * n + lane] : 0.0;
+    }
+    if (lane < n)
+        cb_ap(a, s)[lane] = ap;
+    __syncwarp();
+    cb_set_alpha_m(a, pb, L, s, lane);
+}
+
+// Loads a newly assigned vector (optcb.cpp:87-153 entry half, :170-188).
+__device__ void init_slot_cb(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane, int ldv)
+{
+    const int n = pb.n;
+    const int cell = L.ints[s * SI_N + SI_CELL];
+    double ui = (lane < n) ? pb.u[(size_t)cell * n + lane] : 0.0;
+    if (a.momentsOld != nullptr && lane < n) {
+        int i = cell / a.NY, j = cell % a.NY;
+        if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
+            a.momentsOld[(size_t)cell * n + lane] = ui;
+    }
+    const double u0 = __shfl_sync(0xffffffffu, ui, 0);
+    if (!(u0 > 0.0)) {
+        if (lane == 0) {
+            L.ints[s * SI_N + SI_TOTAL] = 0;
+            L.ints[s * SI_N + SI_REG] = 0;
+        }
+        __syncwarp();
+        finish_slot(a, pb, L, s, ui, (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0, -3, lane);
+        return;
+    }
+    double *sc = L.scal + s * SC_N;
+    double delta = a.deltaPPn;
+    if (a.momentType == 0) {
+        if (lane == 0)
+            sc[SC_ASCALE] = log(u0) * 2.0 * kSqrtPi;
+    } else {
+        delta = delta / (u0 * u0);
+    }
+    ui = ui / u0;
+    if (lane < ldv)
+        L.u[s * ldv + lane] = (lane < n) ? ui : 0.0;
+    const double rtol = sqrt(warp_sum(ui * ui)) * a.tolRel;
+    if (lane == 0) {
+        sc[SC_T] = 1.0;
+        sc[SC_RTOL] = rtol;
+        sc[SC_U0] = u0;
+        sc[SC_DELTA] = delta;
+        sc[SC_R] = 0.0;
+        int *si = L.ints + s * SI_N;
+        si[SI_ITER] = 0;
+        si[SI_TOTAL] = 0;
+        si[SI_REG] = 0;
+        si[SI_MAXITER] = a.maxIter;
+        si[SI_PRED] = 0;
+        si[SI_CB] = 0;
+        si[SI_STATE] = S_NEWTON;
+    }
+    __syncwarp();
+    cb_restart_state(a, pb, L, s, lane);
+}
+
+// Regularisation restart of the change-of-basis solve (optcb.cpp:268-318).
+__device__ void cb_regularize(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane)
+{
+    const int n = pb.n, ldv = a.ldv;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    const int cell = si[SI_CELL];
+    const double u0 = sc[SC_U0];
+    int reg = si[SI_REG], flags = si[SI_CB];
+    double r = sc[SC_R];
+    const double us = (lane < n) ? pb.u[(size_t)cell * n + lane] / u0 : 0.0;   // scaled original
+    double unew;
+    int maxIter = si[SI_MAXITER];
+    if (reg < kNumReg - 1) {
+        reg++;
+        r = kRegularizations[reg];
+        unew = (lane == 0) ? 1.0 : us * (1.0 - r);
+    } else {
+        if (flags & CB_HIT_MAX) {
+            // "This should never happen." -- the reference aborts
+            double uo = us * u0, ao = (lane < n) ? L.alpha[s * ldv + lane] : 0.0;
+            if (a.momentType == 0) {
+                if (lane == 0)
+                    ao += sc[SC_ASCALE];
+            } else {
+                ao *= u0;
+            }
+            __syncwarp();
+            finish_slot(a, pb, L, s, uo, ao, -4, lane);
+            return;
+        }
+        flags |= CB_HIT_MAX | CB_START_STD;
+        unew = us;
+        reg = 0;   // r keeps its value (optcb.cpp:288-296)
+        maxIter = a.maxIter;
+    }
+    if (reg == kNumReg - 1)
+        maxIter = 10 * maxIter;
+    if (lane < n)
+        L.u[s * ldv + lane] = unew;
+    const double rtol = sqrt(warp_sum(lane < n ? unew * unew : 0.0)) * a.tolRel;
+    __syncwarp();
+    if (lane == 0) {
+        si[SI_REG] = reg;
+        si[SI_CB] = flags;
+        si[SI_ITER] = 0;
+        si[SI_MAXITER] = maxIter;
+        sc[SC_R] = r;
+        sc[SC_T] = 1.0;
+        sc[SC_RTOL] = rtol;
+        si[SI_STATE] = S_NEWTON;
+    }
+    __syncwarp();
+    cb_restart_state(a, pb, L, s, lane);
+}
+
+// Converged: the regularised input moments and alphaM are returned (no
+// moment write-back, optcb.cpp:347-360 and the wrapper's rescaling), the
+// vector's basis and alphaP are stored.
+__device__ void cb_converge(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane)
+{
+    const int n = pb.n, ldv = a.ldv;
+    int *si = L.ints + s * SI_N;
+    const double *sc = L.scal + s * SC_N;
+    const int cell = si[SI_CELL];
+    const double u0 = sc[SC_U0], r = sc[SC_R];
+    const double us = (lane < n) ? pb.u[(size_t)cell * n + lane] / u0 : 0.0;
+    double uo = ((lane == 0) ? 1.0 : us * (1.0 - r)) * u0;
+    double ao = (lane < n) ? L.alpha[s * ldv + lane] : 0.0;
+    if (a.momentType == 0) {
+        if (lane == 0)
+            ao += sc[SC_ASCALE];
+    } else {
+        ao *= u0;
+    }
+    const double *Tg = cb_basis(a, s);
+    double *T0 = pb.P2M + (size_t)cell * n * n;
+    for (int i = 0; i < n; i++)
+        if (lane < n)
+            T0[i * n + lane] = Tg[i * kMaxN + lane];
+    if (lane < n)
+        pb.alphaP[(size_t)cell * n + lane] = cb_ap(a, s)[lane];
+    // the histogram bin of r (after a restart in the standard basis the
+    // level index is 0 while r keeps its last value, as in the reference)
+    int bin = 0;
+    for (int k = 0; k < kNumReg; k++)
+        if (fabs(r - kRegularizations[k]) < 1e-10)
+            bin = k;
+    __syncwarp();
+    if (lane == 0)
+        si[SI_REG] = bin;
+    __syncwarp();
+    finish_slot(a, pb, L, s, uo, ao, 0, lane);
+}
+
+// Newton logic of one change-of-basis slot after its evaluation.
+__device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane, int warp)
+{
+    const int n = pb.n;
+    const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
+    const bool act = lane < n;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    double *Hs = L.H + warp * (kMaxN * ldh);
+    double *Wi = cb_linv(a, s);   // rows of L^-1, stride kMaxN
+    double *APs = cb_ap(a, s), *AMs = cb_am(a, s), *DMs = cb_dm(a, s);
+    double *vec = L.vec + warp * 64;
+    const double *Gs = L.G + s * ldG;
+    const int npairs = n * (n + 1) / 2;
+
+    // H_M from the product columns (fobj.cpp:37-129)
+    for (int pi = lane; pi < npairs; pi += 32) {
+        const unsigned short pr = pb.pairs[pi];
+        const int i = pr >> 8, j = pr & 255;
+        const double v = Gs[pi];
+        Hs[i * ldh + j] = v;
+        Hs[j * ldh + i] = v;
+    }
+    __syncwarp();
+    const double ui = act ? L.u[s * ldv + lane] : 0.0;
+    const double am = act ? L.alpha[s * ldv + lane] : 0.0;
+    double gi;
+    if (a.momentType == 0)
+        gi = act ? Hs[lane] / pb.p0 - ui : 0.0;
+    else
+        gi = act ? Gs[pb.K2p + lane] - ui : 0.0;
+    const double au = warp_sum(am * ui);
+    double fpart = 0.0;
+    for (int k = 0; k < a.ntq; k++)
+        fpart += L.fpart[s * a.ntq + k];
+    const double fsum = fpart - au;
+    const double fH = (a.momentType == 0) ? Hs[0] / (pb.p0 * pb.p0) - au : fsum;
+
+    if (si[SI_STATE] == S_TRIAL) {
+        if (lane == 0)
+            atomicAdd(&L.stat[kNumReg + 2], 1ull);
+        double t = sc[SC_T];
+        if (!(fsum <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD])) {
+            t = 0.5 * t;
+            if (t * sc[SC_MAXF] > DBL_EPSILON / 2) {
+                if (act)
+                    L.alpha[s * ldv + lane] = AMs[lane] + t * DMs[lane];
+                __syncwarp();
+                if (lane == 0)
+                    sc[SC_T] = t;
+                return;
+            }
+            // backtracked all the way: restored alpha, the next iteration
+            // regularises because t == 0
+            if (act) {
+                APs[lane] = L.aold[s * ldv + lane];
+                L.alpha[s * ldv + lane] = AMs[lane];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                si[SI_ITER] += 1;
+                si[SI_TOTAL] += 1;
+            }
+            __syncwarp();
+            cb_regularize(a, pb, L, s, lane);
+            return;
+        }
+        // accepted: alphaP <- alphaP + t d_P, and this evaluation is the next
+        // iteration's
+        if (act)
+            APs[lane] = L.aold[s * ldv + lane] + t * L.d[s * ldv + lane];
+        __syncwarp();
+    }
+
+    const int iter = si[SI_ITER] + 1;
+    const int total = si[SI_TOTAL] + 1;
+    __syncwarp();
+    if (lane == 0) {
+        si[SI_ITER] = iter;
+        si[SI_TOTAL] = total;
+    }
+    const double err = sqrt(warp_sum(gi * gi));   // the moment-basis gradient (:340-344)
+
+    double *Tg = cb_basis(a, s);
+    const double *rd = cb_rdiag(a, s);
+    vec[lane] = gi;
+    __syncwarp();
+    // X = T^-1 [H_M | g_M]: lane j < n a column of H_M, lane n the gradient
+    double m[kMaxN];
+#pragma unroll
+    for (int k = 0; k < kMaxN; k++)
+        m[k] = (k < n) ? (act ? Hs[lane * ldh + k] : (lane == n ? vec[k] : 0.0)) : 0.0;
+    cb_trsv_cols(Tg, rd, m, n);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kMaxN; k++) {
+        if (k < n) {
+            if (act)
+                Hs[k * ldh + lane] = m[k];
+            else if (lane == n)
+                vec[32 + k] = m[k];   // g_P
+        }
+    }
+    __syncwarp();
+    // H_P = T^-1 X^T: lane j takes row j of X (a column of X^T)
+#pragma unroll
+    for (int k = 0; k < kMaxN; k++)
+        m[k] = (act && k < n) ? Hs[lane * ldh + k] : 0.0;
+    cb_trsv_cols(Tg, rd, m, n);
+    double rowsum = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxN; k++)
+        rowsum += (k < n) ? fabs(m[k]) : 0.0;
+    const double anorm = warp_max(act ? rowsum : 0.0);
+    __syncwarp();
+    int info = chol_regs(m, Hs, ldh, n, lane);
+    double condest = 0.0;
+    double v[kMaxN];
+    if (info == 0) {
+        invert_regs(Hs, ldh, v, n, lane);
+        __syncwarp();
+        double colsum = 0.0;
+#pragma unroll
+        for (int i = 0; i < kMaxN; i++) {
+            if (i < n && act)
+                Wi[i * kMaxN + lane] = v[i];   // rows of L^-1
+            colsum += fabs(v[i]);
+        }
+        __syncwarp();
+        double rs = 0.0;
+        if (act)
+            for (int c = 0; c <= lane; c++)
+                rs += fabs(Wi[lane * kMaxN + c]);
+        const double bound = anorm * warp_max(colsum) * warp_max(rs);
+        if (!(bound <= 0.5 * a.condHMax)) {
+            const double rc = rcond_warp(Wi, n, kMaxN, vec, anorm, lane);
+            condest = 1.0 / rc;
+        }
+    }
+    // a bad Hessian at the very first evaluation: isotropic alpha and the
+    // standard basis (optcb.cpp:247-265)
+    if (total == 1 && (info != 0 || condest > a.condHMax)) {
+        __syncwarp();
+        if (lane == 0) {
+            si[SI_CB] |= CB_START_STD;
+            si[SI_ITER] = 0;
+            sc[SC_T] = 1.0;
+            si[SI_STATE] = S_NEWTON;
+        }
+        __syncwarp();
+        cb_restart_state(a, pb, L, s, lane);
+        return;
+    }
+    if (iter >= si[SI_MAXITER] || info != 0 || sc[SC_T] == 0.0 || condest > a.condHMax) {
+        __syncwarp();
+        cb_regularize(a, pb, L, s, lane);
+        return;
+    }
+
+    // change of basis by L (optcb.cpp:321-332)
+    double gpn = 0.0;   // L^-1 g_P
+    if (act)
+        for (int k = 0; k <= lane; k++)
+            gpn = fma(Wi[lane * kMaxN + k], vec[32 + k], gpn);
+    // alphaP <- L^T alphaP: lane j sums L_kj alphaP_k over k >= j
+    double apn = 0.0;
+    if (act) {
+        apn = (1.0 / Hs[lane * ldh + lane]) * APs[lane];
+        for (int k = lane + 1; k < n; k++)
+            apn = fma(Hs[k * ldh + lane], APs[k], apn);
+    }
+    // T <- T L: lane i forms row i
+    {
+        double t[kMaxN], tn[kMaxN];
+#pragma unroll
+        for (int k = 0; k < kMaxN; k++) {
+            t[k] = (act && k <= lane) ? Tg[lane * kMaxN + k] : 0.0;
+            tn[k] = 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxN; k++) {
+            if (k < n) {
+                const double *Lk = Hs + k * ldh;
+                const double lkk = 1.0 / Lk[k];
+#pragma unroll
+                for (int j = 0; j < kMaxN; j++)
+                    if (j <= k)
+                        tn[j] = fma(t[k], (j == k) ? lkk : Lk[j], tn[j]);
+            }
+        }
+        __syncwarp();
+        double tdiag = 1.0;
+#pragma unroll
+        for (int k = 0; k < kMaxN; k++) {
+            if (act && k <= lane)
+                Tg[lane * kMaxN + k] = tn[k];
+            if (k == lane)
+                tdiag = tn[k];
+        }
+        if (act)
+            cb_rdiag(a, s)[lane] = 1.0 / tdiag;
+    }
+    __syncwarp();
+    if (act)
+        APs[lane] = apn;
+    __syncwarp();
+    if (err <= sc[SC_RTOL]) {
+        cb_converge(a, pb, L, s, lane);
+        return;
+    }
+    // line search set-up in the new basis (linesearch.cpp:21-52 with d_P = -g_P)
+    const double dp = act ? -gpn : 0.0;
+    const double gd = warp_sum(gpn * dp);
+    const double maxf = warp_max(act ? fabs(dp) / (fabs(apn) + 1e-100) : 0.0);
+    if (1.0 * maxf > DBL_EPSILON / 2) {
+        const double dmv = cb_solve_t(Tg, dp, n, lane);   // moment-basis step (T L)^-T d_P
+        if (act) {
+            L.aold[s * ldv + lane] = apn;
+            L.d[s * ldv + lane] = dp;
+            AMs[lane] = am;
+            DMs[lane] = dmv;
+            L.alpha[s * ldv + lane] = am + dmv;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            sc[SC_T] = 1.0;
+            sc[SC_FREF] = fH;
+            sc[SC_GD] = gd;
+            sc[SC_MAXF] = maxf;
+            si[SI_STATE] = S_TRIAL;
+        }
+        return;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        sc[SC_T] = 0.0;
+        si[SI_ITER] += 1;
+        si[SI_TOTAL] += 1;
+    }
+    __syncwarp();
+    cb_regularize(a, pb, L, s, lane);
+}
+
 // Fused evaluation contractions (used when every problem's G has at most NTF
 // column tiles of 8).  Warp w owns slot rows mt = w % 2 (16 slots) and the
 // q-group qg = w / 2 (8 of the chunk's 32 quadrature rows): it forms
@@ -1027,7 +1529,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         }
         for (int s = warp; s < T; s += kWarps)
             if (L.ints[s * SI_N + SI_STATE] == S_NEW)
-                init_slot(a, pb, L, s, lane, ldv);
+                (a.optType == 1) ? init_slot_cb(a, pb, L, s, lane, ldv) : init_slot(a, pb, L, s, lane, ldv);
         __syncthreads();
 
         // ---- phase A: evaluation contractions over the quadrature
@@ -1168,8 +1670,12 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         // ---- phase B: per-slot Newton logic, one warp per slot
         for (int s = warp; s < T; s += kWarps) {
             int st = L.ints[s * SI_N + SI_STATE];
-            if (st == S_NEWTON || st == S_TRIAL)
-                slot_logic(a, pb, L, s, lane, warp);
+            if (st == S_NEWTON || st == S_TRIAL) {
+                if (a.optType == 1)
+                    slot_logic_cb(a, pb, L, s, lane, warp);
+                else
+                    slot_logic(a, pb, L, s, lane, warp);
+            }
         }
         if constexpr (NTF > 0)
             fence_proxy_async_smem();   // this round's shared-memory writes before the next bulk copies

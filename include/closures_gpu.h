@@ -73,7 +73,8 @@ void cl_angular_free(cl_angular *a);
 /* Solver options: the MOMOPT_* deck keys read at momopt_init.cpp:56-68. */
 typedef struct {
     int moment_type;        /* CL_MN or CL_PPN */
-    int opt_type;           /* must be 0 (Newton, opt.cpp); 1 and 2 are rejected */
+    int opt_type;           /* 0 Newton (opt.cpp), 1 change of basis (optcb.cpp);
+                               2 (BFGS, optbfgs.cpp) is rejected */
     int max_iter;           /* MOMOPT_MAX_ITER */
     double tol;             /* MOMOPT_TOL (relative gradient tolerance) */
     double cond_h_max;      /* MOMOPT_COND_H_MAX */
@@ -156,6 +157,17 @@ int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
 int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
                                 const double *d_alpha_start, int *d_iters, double *d_reg,
                                 int *d_status);
+/* Change-of-basis solve (optcb(), optcb.cpp:87-415; replaces the
+ * OPT_TYPE_CHANGE_BASIS branch of momopt_update.cpp:240-244) on device
+ * pointers, for a context created with opt_type 1: each vector carries its
+ * basis d_P2M [count][n][n] (row-major, lower triangular) and multipliers
+ * d_alphaP [count][n] in that basis, read at the start and written back on
+ * convergence; d_alpha receives the multipliers in the moment basis and d_u
+ * the regularised input moments, as the reference returns them.  A grid
+ * context keeps this state per cell by itself (initialised as
+ * momopt_init.cpp:146-157 does). */
+int cl_solve_batch_cb_device(cl_ctx *ctx, int count, double *d_u, double *d_P2M, double *d_alphaP,
+                             double *d_alpha, int *d_iters, double *d_reg, int *d_status);
 
 /* Mixed-order batch: a solver context for several moment orders at one
  * quadrature order, so vectors of different N share one persistent launch.

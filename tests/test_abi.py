@@ -74,15 +74,22 @@ def test_no_cpu_fallback():
     assert e.value.code == cb.CL_ERR_CUDA
 
 
-def test_rejects_change_of_basis_and_bfgs(tmp_path):
-    for opt_type in (1, 2):
-        d = tmp_path / ("deck%d" % opt_type)
-        decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=opt_type,
-                                                  moment_order=1, quad_order=4))
-        with pytest.raises(cb.ClosuresError) as e:
-            cb.Solver(str(d), str(tmp_path))
-        assert e.value.code == cb.CL_ERR_ARG
-        assert "OPTIMIZATION_TYPE" in str(e.value)
+def test_rejects_bfgs_accepts_change_of_basis(tmp_path):
+    """MOMOPT_OPTIMIZATION_TYPE 2 (BFGS) is an input error; type 1 (change of
+    basis) passes validation and, without a GPU, stops at the device."""
+    d = tmp_path / "deck2"
+    decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=2,
+                                              moment_order=1, quad_order=4))
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert e.value.code == cb.CL_ERR_ARG
+    assert "OPTIMIZATION_TYPE" in str(e.value)
+    d = tmp_path / "deck1"
+    decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=1,
+                                              moment_order=1, quad_order=4))
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert e.value.code == cb.CL_ERR_CUDA
 
 
 def test_missing_deck_key_is_an_input_error(tmp_path):
