@@ -137,9 +137,10 @@ def dist_setup():
     return world, rank, local
 
 
-def write_deck(tmpdir, workload, precision="fp64"):
+def write_deck(tmpdir, workload, precision="fp64", opt_type=0):
     path = os.path.join(tmpdir, "input.deck")
     kw = dict(WORKLOADS[workload])
+    kw["opt_type"] = opt_type
     if precision == "mixed":
         kw["extra"] = {"MOMOPT_GPU_PRECISION": "mixed"}
     decks.write_deck(path, decks.deck_text(**kw))
@@ -173,6 +174,39 @@ def run_oracle_steps(deck, max_steps, budget_s):
             break
     g.close()
     return done, t_total, 2 * C * done, threads
+
+
+def run_oracle_cb_sample(deck, w, budget_s):
+    """The reference's change-of-basis solve on the host cores (oracle
+    restatement, OpenMP over the cells): the first stage's cell-solves of the
+    deck from t = 0 (every cell from the reference's initial basis), on a
+    random sample of cells grown until it takes about budget_s.
+    Returns (cells, seconds, threads)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    threads = cpu_threads()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import pyoracle
+    pyoracle.build()
+    g = pyoracle.GridSolver(deck)
+    m, _ = g.state()
+    g.close()
+    order, Q = w["moment_order"], w["quad_order"]
+    moment_type = 0 if w.get("moment_type", "mn") == "mn" else 1
+    u_all = m.reshape(-1, m.shape[-1])
+    rng = np.random.default_rng(0)
+    count = 2 * threads
+    while True:
+        idx = rng.choice(u_all.shape[0], size=min(count, u_all.shape[0]), replace=False)
+        u = u_all[idx].copy()
+        P2M, aP = pyoracle.cb_init(u.shape[1], len(idx), moment_type)
+        al = np.zeros_like(u)
+        t0 = time.perf_counter()
+        pyoracle.optcb_batch(order, Q, u, P2M, aP, al, moment_type=moment_type,
+                             tol=w["tol"])
+        secs = time.perf_counter() - t0
+        if secs >= 0.3 * budget_s or len(idx) == u_all.shape[0]:
+            return len(idx), secs, threads
+        count = int(count * min(8.0, max(2.0, budget_s / max(secs, 1e-3))))
 
 
 def reference_arm(args, world, rank):
@@ -257,7 +291,7 @@ def native_arm(args, world, rank, local):
                                 device_id=torch.device("cuda", local))
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
-    deck = write_deck(tmp, args.workload, args.precision)
+    deck = write_deck(tmp, args.workload, args.precision, args.opt_type)
     solver = cb.Solver(deck, tmp)
     ctx = solver.context()
     dt, dx, dy = solver.max_dt, solver.dx, solver.dy
@@ -320,7 +354,12 @@ def native_arm(args, world, rank, local):
     trials = st1["total_trials"] - st0["total_trials"]
     newton_ms = float(kernel_ms[0] + kernel_ms[2])
     flux_ms = float(kernel_ms[1] + kernel_ms[3])
-    f_newton = iters * flops_per_iteration(n, ang.n2, ang.nq, w["use_gaunt"], nnz) + \
+    per_iter = flops_per_iteration(n, ang.n2, ang.nq, w["use_gaunt"], nnz)
+    if args.opt_type == 1:
+        # the change of basis adds the two triangular solves of
+        # H_P = T^-1 H_M T^-T and the basis update T <- T L (n^3 each)
+        per_iter += 3.0 * n ** 3
+    f_newton = iters * per_iter + \
         trials * flops_per_trial(n, ang.nq)
     f_flux = 2 * args.steps * flops_flux_stage(C, C_int, n, ang.nq)
     ach_newton = f_newton / (newton_ms * 1e-3) / 1e12
@@ -355,12 +394,22 @@ def native_arm(args, world, rank, local):
     state_bytes = 2 * C * n * 8
 
     cpu = None
-    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and rank == 0 and not args.no_cpu_baseline and args.opt_type == 0:
         steps, secs, solves_cpu, threads = run_oracle_steps(deck, 1, budget_s=60.0)
         cpu = {"value": solves_cpu / secs, "unit": "cell-solves/s", "cores": threads,
                "kind": "port",
                "sample": "first RK2 step of the same deck from t=0 on all %d host threads "
                          "(oracle restatement, -O3 -fopenmp)" % threads}
+    elif world == 1 and rank == 0 and not args.no_cpu_baseline:
+        # the oracle's change-of-basis solve transforms the basis rows at
+        # every iteration, so a full step takes minutes on the host: a
+        # sample of the first stage's cells instead
+        cells, secs, threads = run_oracle_cb_sample(deck, w, budget_s=20.0)
+        cpu = {"value": cells / secs, "unit": "cell-solves/s", "cores": threads,
+               "kind": "port",
+               "sample": "%d random cells of the deck's first stage from t=0 (reference initial "
+                         "basis), change-of-basis solve on all %d host threads (oracle "
+                         "restatement, -O3 -fopenmp)" % (cells, threads)}
 
     if rank == 0:
         line = {
@@ -374,7 +423,8 @@ def native_arm(args, world, rank, local):
                        "moment_order": w["moment_order"], "n": n, "quad_order": w["quad_order"],
                        "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
                        "moment_type": w["moment_type"] if "moment_type" in w else "mn",
-                       "newton": args.newton, "precision": args.precision, "t_start": args.warmup * dt,
+                       "newton": args.newton, "precision": args.precision, "opt_type": args.opt_type,
+                       "t_start": args.warmup * dt,
                        "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
                        "parallelism": "replicas" if world > 1 else "single"},
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
@@ -573,6 +623,8 @@ def main():
     ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
                     help="batch workload: start from the isotropic multiplier or a learned prediction")
     ap.add_argument("--nn-steps", type=int, default=4000)
+    ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1],
+                    help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="grid workloads: Hessian-only tiles in split TF32 (MOMOPT_GPU_PRECISION mixed)")
     args = ap.parse_args()

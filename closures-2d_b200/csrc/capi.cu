@@ -387,9 +387,12 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     ctx->C = (long long)ctx->NX * ctx->NY;
     const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
     CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    // the change-of-basis solve forms its Hessians from the basis products
-    // (optcb.cpp calls fobj without the Gaunt table)
-    const int gauntNewton = (opts->opt_type == 1) ? 0 : ang->use_gaunt;
+    // Both optimisation types sum the moment-basis Hessian the way the deck
+    // asks (Gaunt table or basis products).  The change-of-basis solve then
+    // transforms it to its working basis; optcb.cpp instead transforms the
+    // degree-N basis rows and sums products, which is the same Hessian in
+    // exact arithmetic.
+    const int gauntNewton = ang->use_gaunt;
     cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi,
                                         ang->eta, ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
                                         ang->gaunt_nnz);

@@ -466,21 +466,15 @@ __device__ void converge(const NewtonArgs &a, const NewtonProblem &pb, Layout &L
     finish_slot(a, pb, L, s, uo, ao, 0, lane);
 }
 
-// Newton logic for one slot after its evaluation (warp-wide).
-__device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
-                           int warp)
+// The slot's symmetric H (row stride ldh) from its contraction results Gs:
+// the Gaunt sums H_ij = sum_k c_ijk G_k from the ELL table in shared memory
+// (fobj.cpp:129-155), or the packed products p_i p_j (fobj.cpp:37-129).
+__device__ __forceinline__ void hessian_from_contractions(const NewtonArgs &a, const NewtonProblem &pb,
+                                                         const Layout &L, const double *Gs, double *Hs,
+                                                         int lane)
 {
-    const int n = pb.n;
-    const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
-    const bool act = lane < n;
-    int *si = L.ints + s * SI_N;
-    double *sc = L.scal + s * SC_N;
-    double *Hs = L.H + warp * (kMaxN * ldh);
-    double *vec = L.vec + warp * 64;
-    const double *Gs = L.G + s * ldG;
+    const int n = pb.n, ldh = a.ldh;
     const int npairs = n * (n + 1) / 2;
-
-    // H from the contraction results (fobj.cpp:129-155)
     if (a.useGaunt) {
         for (int c = 0; c < pb.ellChunks; c++) {
             const unsigned short pr = L.ellPair[c * 32 + lane];
@@ -516,6 +510,23 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
             Hs[j * ldh + i] = v;
         }
     }
+}
+
+// Newton logic for one slot after its evaluation (warp-wide).
+__device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
+                           int warp)
+{
+    const int n = pb.n;
+    const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
+    const bool act = lane < n;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    double *Hs = L.H + warp * (kMaxN * ldh);
+    double *vec = L.vec + warp * 64;
+    const double *Gs = L.G + s * ldG;
+
+    // H from the contraction results
+    hessian_from_contractions(a, pb, L, Gs, Hs, lane);
     __syncwarp();
 
     const double ui = act ? L.u[s * ldv + lane] : 0.0;
@@ -969,16 +980,9 @@ __device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layo
     double *APs = cb_ap(a, s), *AMs = cb_am(a, s), *DMs = cb_dm(a, s);
     double *vec = L.vec + warp * 64;
     const double *Gs = L.G + s * ldG;
-    const int npairs = n * (n + 1) / 2;
 
-    // H_M from the product columns (fobj.cpp:37-129)
-    for (int pi = lane; pi < npairs; pi += 32) {
-        const unsigned short pr = pb.pairs[pi];
-        const int i = pr >> 8, j = pr & 255;
-        const double v = Gs[pi];
-        Hs[i * ldh + j] = v;
-        Hs[j * ldh + i] = v;
-    }
+    // H_M in the moment basis (Gaunt sums or products)
+    hessian_from_contractions(a, pb, L, Gs, Hs, lane);
     __syncwarp();
     const double ui = act ? L.u[s * ldv + lane] : 0.0;
     const double am = act ? L.alpha[s * ldv + lane] : 0.0;

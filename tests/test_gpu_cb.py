@@ -11,7 +11,10 @@ import pyoracle as oracle_lib
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(2, 20, cb.CL_MN), (3, 30, cb.CL_MN), (4, 30, cb.CL_MN), (6, 40, cb.CL_MN), (3, 20, cb.CL_PPN)]
+# (order, Q, moment type, Gaunt): with the Gaunt table the GPU sums the
+# moment-basis Hessian through it; the oracle always sums basis products
+CASES = [(2, 20, cb.CL_MN, 0), (3, 30, cb.CL_MN, 0), (4, 30, cb.CL_MN, 0), (6, 40, cb.CL_MN, 0),
+         (3, 20, cb.CL_PPN, 0), (4, 30, cb.CL_MN, 1), (6, 40, cb.CL_MN, 1), (3, 20, cb.CL_PPN, 1)]
 
 
 def _gpu_call(a, u, P2M, aP, moment_type):
@@ -41,9 +44,9 @@ def _oracle_call(order, Q, u, P2M, aP, moment_type, fma=False):
     return (uu, al, it, rg, st, P, A)
 
 
-@pytest.mark.parametrize("order,Q,mt", CASES)
-def test_change_of_basis_matches_oracle(order, Q, mt):
-    a = cb.Angular(order, Q, 0)
+@pytest.mark.parametrize("order,Q,mt,gaunt", CASES)
+def test_change_of_basis_matches_oracle(order, Q, mt, gaunt):
+    a = cb.Angular(order, Q, gaunt)
     u, _ = cb.sample_moment_vectors(a, 400, seed=13, s_range=(0.1, 3.0))
     P2M, aP = oracle_lib.cb_init(a.n, u.shape[0], mt, 1e-10)
     # two calls in a row; each call starts all three solvers from the same
@@ -86,6 +89,8 @@ GRID = [
     # summation order decides, for plain Newton as well
     ("m4_pulse", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.25, floor=1e-8, moment_order=4,
                       quad_order=30, tol=1e-8, use_gaunt=0, opt_type=1)),
+    ("m4_pulse_gaunt", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.25, floor=1e-8,
+                            moment_order=4, quad_order=30, tol=1e-8, use_gaunt=1, opt_type=1)),
 ]
 
 
