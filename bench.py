@@ -176,8 +176,9 @@ def run_oracle_steps(deck, max_steps, budget_s):
     return done, t_total, 2 * C * done, threads
 
 
-def run_oracle_cb_sample(deck, w, budget_s):
-    """The reference's change-of-basis solve on the host cores (oracle
+def run_oracle_cb_sample(deck, w, opt_type, budget_s):
+    """The reference's change-of-basis solve (opt_type 1: optcb, 2: optbfgs)
+    on the host cores (oracle
     restatement, OpenMP over the cells): the first stage's cell-solves of the
     deck from t = 0 (every cell from the reference's initial basis), on a
     random sample of cells grown until it takes about budget_s.
@@ -202,7 +203,7 @@ def run_oracle_cb_sample(deck, w, budget_s):
         al = np.zeros_like(u)
         t0 = time.perf_counter()
         pyoracle.optcb_batch(order, Q, u, P2M, aP, al, moment_type=moment_type,
-                             tol=w["tol"])
+                             tol=w["tol"], opt_type=opt_type)
         secs = time.perf_counter() - t0
         if secs >= 0.3 * budget_s or len(idx) == u_all.shape[0]:
             return len(idx), secs, threads
@@ -355,7 +356,7 @@ def native_arm(args, world, rank, local):
     newton_ms = float(kernel_ms[0] + kernel_ms[2])
     flux_ms = float(kernel_ms[1] + kernel_ms[3])
     per_iter = flops_per_iteration(n, ang.n2, ang.nq, w["use_gaunt"], nnz)
-    if args.opt_type == 1:
+    if args.opt_type != 0:
         # the change of basis adds the two triangular solves of
         # H_P = T^-1 H_M T^-T and the basis update T <- T L (n^3 each)
         per_iter += 3.0 * n ** 3
@@ -404,12 +405,12 @@ def native_arm(args, world, rank, local):
         # the oracle's change-of-basis solve transforms the basis rows at
         # every iteration, so a full step takes minutes on the host: a
         # sample of the first stage's cells instead
-        cells, secs, threads = run_oracle_cb_sample(deck, w, budget_s=20.0)
+        cells, secs, threads = run_oracle_cb_sample(deck, w, args.opt_type, budget_s=20.0)
         cpu = {"value": cells / secs, "unit": "cell-solves/s", "cores": threads,
                "kind": "port",
                "sample": "%d random cells of the deck's first stage from t=0 (reference initial "
-                         "basis), change-of-basis solve on all %d host threads (oracle "
-                         "restatement, -O3 -fopenmp)" % (cells, threads)}
+                         "basis), %s on all %d host threads (oracle restatement, -O3 -fopenmp)"
+                         % (cells, "optcb" if args.opt_type == 1 else "optbfgs", threads)}
 
     if rank == 0:
         line = {
@@ -623,8 +624,9 @@ def main():
     ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
                     help="batch workload: start from the isotropic multiplier or a learned prediction")
     ap.add_argument("--nn-steps", type=int, default=4000)
-    ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1],
-                    help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton)")
+    ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1, 2],
+                    help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton, "
+                         "2: BFGS sub-iterations in the change of basis)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="grid workloads: Hessian-only tiles in split TF32 (MOMOPT_GPU_PRECISION mixed)")
     args = ap.parse_args()

@@ -45,7 +45,8 @@ class cl_angular(C.Structure):
 class cl_options(C.Structure):
     _fields_ = [("moment_type", C.c_int), ("opt_type", C.c_int), ("max_iter", C.c_int),
                 ("tol", C.c_double), ("cond_h_max", C.c_double), ("delta_ppn", C.c_double),
-                ("tol_gamma", C.c_double), ("precision", C.c_int)]
+                ("tol_gamma", C.c_double), ("precision", C.c_int), ("max_bfgs_iter", C.c_int),
+                ("cond_h_max_bfgs", C.c_double)]
 
 
 class cl_grid(C.Structure):
@@ -211,9 +212,9 @@ class Angular:
 
 
 def make_options(moment_type=CL_MN, max_iter=100, tol=1e-8, cond_h_max=1e10, delta_ppn=1e-10,
-                 tol_gamma=0.0, precision=CL_FP64, opt_type=0):
+                 tol_gamma=0.0, precision=CL_FP64, opt_type=0, max_bfgs_iter=5, cond_h_max_bfgs=20.0):
     return cl_options(moment_type, opt_type, max_iter, tol, cond_h_max, delta_ppn, tol_gamma,
-                      precision)
+                      precision, max_bfgs_iter, cond_h_max_bfgs)
 
 
 class Context:
@@ -317,7 +318,7 @@ class Context:
 
     def solve_batch_cb_device(self, d_u, d_P2M, d_alphaP, d_alpha, d_iters=None, d_reg=None,
                               d_status=None, count=None):
-        """Change-of-basis solve (opt_type 1 contexts): per-vector basis and
+        """Change-of-basis solve (opt_type 1 or 2 contexts): per-vector basis and
         alphaP state in/out, alpha out (moment basis)."""
         ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
         _check(lib().cl_solve_batch_cb_device(self._ctx, count, ptr(d_u), ptr(d_P2M), ptr(d_alphaP),

@@ -194,9 +194,14 @@ int check_options(const cl_options *o, std::string &err)
         err = "null options";
         return CL_ERR_ARG;
     }
-    if (o->opt_type != 0 && o->opt_type != 1) {
-        err = "MOMOPT_OPTIMIZATION_TYPE " + std::to_string(o->opt_type) +
-              " (BFGS) is not provided by the B200 path";
+    if (o->opt_type < 0 || o->opt_type > 2) {
+        err = "MOMOPT_OPTIMIZATION_TYPE " + std::to_string(o->opt_type) + " out of range";
+        return CL_ERR_ARG;
+    }
+    if (o->opt_type == 2 && o->max_bfgs_iter < 1) {
+        // optbfgs.cpp would never take a step and end in "Max regularization
+        // achieved."
+        err = "MOMOPT_MAX_BFGS_ITER must be >= 1";
         return CL_ERR_ARG;
     }
     if (o->moment_type != CL_MN && o->moment_type != CL_PPN) {
@@ -225,6 +230,9 @@ void fill_newton_options(NewtonArgs &a, const cl_options &o, int useGaunt)
     a.mixed = o.precision == CL_MIXED;
     a.optType = o.opt_type;
     a.tolGamma = o.tol_gamma;
+    a.maxBfgsIter = o.max_bfgs_iter;
+    a.condHMaxBfgs = o.cond_h_max_bfgs;
+    a.cbStride = (o.opt_type == 2) ? kBfgsSlotDoubles : kCbSlotDoubles;
 }
 
 int sm_count()
@@ -427,7 +435,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     a.err = ctx->dErr;
     a.NX = ctx->NX;
     a.NY = ctx->NY;
-    if (opts->opt_type == 1) {
+    if (opts->opt_type != 0) {
         // momopt_init.cpp:146-157: alphaP isotropic, and the first n entries
         // of each P2M block (its first column, as the reference stores it
         // column-major) set to one -- singular, so each cell's first solve
@@ -458,8 +466,8 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
     ctx->nCtas = sm_count() * newton_ctas_per_sm(a);
-    if (opts->opt_type == 1) {
-        if (cudaMalloc(&ctx->dCbScratch, (size_t)ctx->nCtas * a.T * kCbSlotDoubles * sizeof(double)) != cudaSuccess) {
+    if (opts->opt_type != 0) {
+        if (cudaMalloc(&ctx->dCbScratch, (size_t)ctx->nCtas * a.T * a.cbStride * sizeof(double)) != cudaSuccess) {
             ctx->err = "device allocation failed";
             return ctx_fail(ctx, CL_ERR_CUDA);
         }
@@ -820,7 +828,7 @@ int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_a
 {
     if (!ctx || count < 0 || (count > 0 && (!d_u || !d_alpha)))
         return CL_ERR_ARG;
-    if (ctx->nargs.optType == 1) {
+    if (ctx->nargs.optType != 0) {
         ctx->err = "change-of-basis contexts solve batches with cl_solve_batch_cb_device";
         return CL_ERR_STATE;
     }
@@ -847,8 +855,8 @@ int cl_solve_batch_cb_device(cl_ctx *ctx, int count, double *d_u, double *d_P2M,
 {
     if (!ctx || count < 0 || (count > 0 && (!d_u || !d_P2M || !d_alphaP || !d_alpha)))
         return CL_ERR_ARG;
-    if (ctx->nargs.optType != 1) {
-        ctx->err = "the context was not created for MOMOPT_OPTIMIZATION_TYPE 1";
+    if (ctx->nargs.optType == 0) {
+        ctx->err = "the context was not created for MOMOPT_OPTIMIZATION_TYPE 1 or 2";
         return CL_ERR_STATE;
     }
     if (count == 0)

@@ -14,6 +14,10 @@ constexpr int kNumReg = 5;
 // basis T and the rows of L^-1 ([kMaxN][kMaxN] each), then alphaP, the
 // line-search alphaM and step, and 1/T_ii ([kMaxN] each)
 constexpr int kCbSlotDoubles = 2 * kMaxN * kMaxN + 4 * kMaxN;
+// BFGS sub-iterations add the approximations of H and H^-1 in the working
+// basis ([kMaxN][kMaxN] each, column j at j * kMaxN, lane i holding row i),
+// the previous gradient and the current gradient in that basis
+constexpr int kBfgsSlotDoubles = kCbSlotDoubles + 2 * kMaxN * kMaxN + 2 * kMaxN;
 
 // opt/opt.h:39-40
 __device__ __constant__ const double kRegularizations[kNumReg] = {0.0, 1e-3, 1e-2, 1e-1, 5e-1};

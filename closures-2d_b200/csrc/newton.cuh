@@ -55,7 +55,7 @@ struct NewtonProblem {
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
 enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
 enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_R, SC_N };
-enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_CB, SI_N };
+enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_CB, SI_BFGS, SI_N };
 
 struct NewtonArgs {
     NewtonProblem prob[kMaxProblems];
@@ -80,8 +80,12 @@ struct NewtonArgs {
     int ntExact, nbk;           // single problem on the fused path: its column tiles and
                                 // GEMM1 k-steps (selects a specialised instance), else 0
     int mixed;                  // Hessian-only tiles by split TF32 (CL_MIXED); needs ntExact
-    int optType;                // 0 Newton (opt.cpp), 1 change of basis (optcb.cpp)
-    double *cbScratch;          // optType 1: per-slot working state, [grid][T][kCbSlotDoubles]
+    int optType;                // 0 Newton (opt.cpp), 1 change of basis (optcb.cpp),
+                                // 2 BFGS sub-iterations in the change of basis (optbfgs.cpp)
+    int maxBfgsIter;            // optType 2: MOMOPT_MAX_BFGS_ITER
+    double condHMaxBfgs;        // optType 2: MOMOPT_COND_H_MAX_BFGS
+    int cbStride;               // doubles per slot of cbScratch (kCbSlotDoubles or kBfgsSlotDoubles)
+    double *cbScratch;          // optType 1, 2: per-slot working state, [grid][T][cbStride]
 };
 
 // Fills the layout fields from the problems' sizes; returns 0, -1 when the

@@ -727,7 +727,7 @@ enum { CB_START_STD = 1, CB_HIT_MAX = 2 };
 
 __device__ __forceinline__ double *cb_slot(const NewtonArgs &a, int s)
 {
-    return a.cbScratch + ((size_t)blockIdx.x * a.T + s) * kCbSlotDoubles;
+    return a.cbScratch + ((size_t)blockIdx.x * a.T + s) * a.cbStride;
 }
 __device__ __forceinline__ double *cb_basis(const NewtonArgs &a, int s) { return cb_slot(a, s); }
 __device__ __forceinline__ double *cb_linv(const NewtonArgs &a, int s) { return cb_slot(a, s) + kMaxN * kMaxN; }
@@ -866,6 +866,7 @@ __device__ void init_slot_cb(const NewtonArgs &a, const NewtonProblem &pb, Layou
         si[SI_MAXITER] = a.maxIter;
         si[SI_PRED] = 0;
         si[SI_CB] = 0;
+        si[SI_BFGS] = 0;
         si[SI_STATE] = S_NEWTON;
     }
     __syncwarp();
@@ -967,6 +968,195 @@ __device__ void cb_converge(const NewtonArgs &a, const NewtonProblem &pb, Layout
     finish_slot(a, pb, L, s, uo, ao, 0, lane);
 }
 
+// ---------------------------------------------------------------------------
+// BFGS sub-iterations (MOMOPT_OPTIMIZATION_TYPE 2, opt/optbfgs.cpp:163-512).
+// The outer iteration is the change-of-basis Newton iteration above; after
+// each basis change H and H^-1 in the new basis start at the identity and up
+// to MOMOPT_MAX_BFGS_ITER quasi-Newton steps d_P = -H^-1 g_P follow, each
+// with the Armijo line search, while cond(H) cond(H^-1) (the reference's
+// cond(): largest absolute column sums of the matrices) stays below
+// MOMOPT_COND_H_MAX_BFGS.  Only the outer iterations count as iterations.
+// Every line-search evaluation carries f, g and H_M, so when the BFGS loop
+// ends at an accepted point the outer iteration runs on that evaluation (the
+// reference re-evaluates at the same point).  H and H^-1 live in the slot's
+// scratch, column j at j * kMaxN, lane i updating row i.
+__device__ __forceinline__ double *bfgs_h(const NewtonArgs &a, int s) { return cb_slot(a, s) + kCbSlotDoubles; }
+__device__ __forceinline__ double *bfgs_hinv(const NewtonArgs &a, int s) { return bfgs_h(a, s) + kMaxN * kMaxN; }
+__device__ __forceinline__ double *bfgs_gold(const NewtonArgs &a, int s) { return bfgs_h(a, s) + 2 * kMaxN * kMaxN; }
+
+// x = T^-1 y (lane i holds y_i, returns x_i): forward substitution with the
+// reciprocal diagonal rd.
+__device__ double cb_solve_l(const double *Tg, const double *rd, double y, int n, int lane)
+{
+    const double rl = (lane < n) ? rd[lane] : 0.0;
+    double acc = 0.0, x = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double xi = __shfl_sync(0xffffffffu, (y - acc) * rl, i);
+        if (lane == i)
+            x = xi;
+        if (lane > i && lane < n)
+            acc = fma(Tg[lane * kMaxN + i], xi, acc);
+    }
+    return (lane < n) ? x : 0.0;
+}
+
+// H = H^-1 = I after a change of basis (optbfgs.cpp:363-364).
+__device__ void bfgs_reset(const NewtonArgs &a, int s, int n, int lane)
+{
+    double *Hp = bfgs_h(a, s), *Hi = bfgs_hinv(a, s);
+    if (lane < n)
+        for (int j = 0; j < n; j++) {
+            Hp[j * kMaxN + lane] = (j == lane) ? 1.0 : 0.0;
+            Hi[j * kMaxN + lane] = (j == lane) ? 1.0 : 0.0;
+        }
+    __syncwarp();
+}
+
+// cond(H) cond(H^-1) as optbfgs.cpp:515-545 computes it; NaN when an update
+// divided by zero (a step that did not move alpha), which ends the loop as
+// the reference's comparison with NaN does.
+__device__ double bfgs_cond(const NewtonArgs &a, int s, int n, int lane)
+{
+    __syncwarp();
+    const double *Hp = bfgs_h(a, s), *Hi = bfgs_hinv(a, s);
+    double s1 = 0.0, s2 = 0.0;
+    if (lane < n)
+        for (int j = 0; j < n; j++) {
+            s1 += fabs(Hp[lane * kMaxN + j]);
+            s2 += fabs(Hi[lane * kMaxN + j]);
+        }
+    const bool nan = __any_sync(0xffffffffu, isnan(s1) || isnan(s2));
+    const double c = warp_max(s1) * warp_max(s2);
+    return nan ? __longlong_as_double(0x7ff8000000000000ll) : c;
+}
+
+// The BFGS updates of H and H^-1 with the step ad = alphaDiff and the
+// gradient change gd = gDiff (optbfgs.cpp:455-485, the dger/dgemv sequence
+// element by element in the same order).
+__device__ void bfgs_update(const NewtonArgs &a, int s, int n, int lane, double ad, double gd)
+{
+    const bool act = lane < n;
+    double *Hp = bfgs_h(a, s), *Hi = bfgs_hinv(a, s);
+    const double ag = warp_sum(ad * gd);
+    const double c1 = 1.0 / ag;
+    for (int j = 0; j < n; j++) {
+        const double gj = __shfl_sync(0xffffffffu, gd, j);
+        if (act)
+            Hp[j * kMaxN + lane] += gd * (c1 * gj);
+    }
+    double t1 = 0.0;
+    for (int j = 0; j < n; j++) {
+        const double aj = __shfl_sync(0xffffffffu, ad, j);
+        if (act)
+            t1 = fma(aj, Hp[j * kMaxN + lane], t1);
+    }
+    const double c2 = -1.0 / warp_sum(ad * t1);
+    double t2 = 0.0;
+    for (int j = 0; j < n; j++) {
+        const double tj = __shfl_sync(0xffffffffu, t1, j);
+        const double gj = __shfl_sync(0xffffffffu, gd, j);
+        if (act) {
+            Hp[j * kMaxN + lane] += t1 * (c2 * tj);
+            t2 = fma(gj, Hi[j * kMaxN + lane], t2);
+        }
+    }
+    const double gHg = warp_sum(gd * t2);
+    const double c3 = (gHg + ag) / (ag * ag), c4 = -1.0 / ag;
+    for (int j = 0; j < n; j++) {
+        const double aj = __shfl_sync(0xffffffffu, ad, j);
+        const double tj = __shfl_sync(0xffffffffu, t2, j);
+        if (act) {
+            double h = Hi[j * kMaxN + lane];
+            h += ad * (c3 * aj);
+            h += t2 * (c4 * aj);
+            h += ad * (c4 * tj);
+            Hi[j * kMaxN + lane] = h;
+        }
+    }
+}
+
+// One pass of the BFGS loop body at alphaP with gradient gp (working basis),
+// f and the moment-basis gradient norm err (optbfgs.cpp:371-445): the
+// direction, the stopping test, and the line search set-up.
+__device__ void bfgs_step(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane, double gp,
+                          double f, double err)
+{
+    const int n = pb.n, ldv = a.ldv;
+    const bool act = lane < n;
+    int *si = L.ints + s * SI_N;
+    double *sc = L.scal + s * SC_N;
+    double *APs = cb_ap(a, s), *AMs = cb_am(a, s), *DMs = cb_dm(a, s);
+    const double *Hi = bfgs_hinv(a, s);
+    __syncwarp();
+    if (lane == 0)
+        si[SI_BFGS] += 1;
+    double dp = 0.0;
+    for (int j = 0; j < n; j++) {
+        const double gj = __shfl_sync(0xffffffffu, gp, j);
+        if (act)
+            dp = fma(-gj, Hi[j * kMaxN + lane], dp);
+    }
+    if (err <= sc[SC_RTOL]) {
+        cb_converge(a, pb, L, s, lane);
+        return;
+    }
+    const double ap = act ? APs[lane] : 0.0;
+    const double am = act ? L.alpha[s * ldv + lane] : 0.0;
+    const double gd = warp_sum(gp * dp);
+    const double maxf = warp_max(act ? fabs(dp) / (fabs(ap) + 1e-100) : 0.0);
+    if (1.0 * maxf > DBL_EPSILON / 2) {
+        const double dmv = cb_solve_t(cb_basis(a, s), dp, n, lane);   // moment-basis step T^-T d_P
+        if (act) {
+            L.aold[s * ldv + lane] = ap;
+            L.d[s * ldv + lane] = dp;
+            bfgs_gold(a, s)[lane] = gp;
+            AMs[lane] = am;
+            DMs[lane] = dmv;
+            L.alpha[s * ldv + lane] = am + dmv;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            sc[SC_T] = 1.0;
+            sc[SC_FREF] = f;
+            sc[SC_GD] = gd;
+            sc[SC_MAXF] = maxf;
+            si[SI_STATE] = S_TRIAL;
+        }
+        return;
+    }
+    // no step possible: the line search returns 0 and the next outer
+    // iteration regularises
+    __syncwarp();
+    if (lane == 0) {
+        sc[SC_T] = 0.0;
+        si[SI_ITER] += 1;
+        si[SI_TOTAL] += 1;
+    }
+    __syncwarp();
+    cb_regularize(a, pb, L, s, lane);
+}
+
+// After an accepted line search: the gradient at the new point in the
+// working basis, the BFGS updates, and the loop test.  Returns false when the
+// loop ends (the outer iteration then runs on this evaluation).
+__device__ bool bfgs_after_step(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
+                                double gm, double f)
+{
+    const int n = pb.n, ldv = a.ldv;
+    const bool act = lane < n;
+    const int *si = L.ints + s * SI_N;
+    const double gp = cb_solve_l(cb_basis(a, s), cb_rdiag(a, s), gm, n, lane);
+    const double ad = act ? cb_ap(a, s)[lane] - L.aold[s * ldv + lane] : 0.0;
+    const double gdf = act ? gp - bfgs_gold(a, s)[lane] : 0.0;
+    bfgs_update(a, s, n, lane, ad, gdf);
+    const double c = bfgs_cond(a, s, n, lane);
+    if (c < a.condHMaxBfgs && si[SI_BFGS] < a.maxBfgsIter) {
+        bfgs_step(a, pb, L, s, lane, gp, f, sqrt(warp_sum(gm * gm)));
+        return true;
+    }
+    return false;
+}
+
 // Newton logic of one change-of-basis slot after its evaluation.
 __device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane, int warp)
 {
@@ -1027,11 +1217,13 @@ __device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layo
             cb_regularize(a, pb, L, s, lane);
             return;
         }
-        // accepted: alphaP <- alphaP + t d_P, and this evaluation is the next
-        // iteration's
+        // accepted: alphaP <- alphaP + t d_P; this evaluation is the next
+        // outer iteration's, or (BFGS) the next quasi-Newton step's
         if (act)
             APs[lane] = L.aold[s * ldv + lane] + t * L.d[s * ldv + lane];
         __syncwarp();
+        if (a.optType == 2 && bfgs_after_step(a, pb, L, s, lane, gi, fsum))
+            return;
     }
 
     const int iter = si[SI_ITER] + 1;
@@ -1166,6 +1358,20 @@ __device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layo
     if (act)
         APs[lane] = apn;
     __syncwarp();
+    if (a.optType == 2) {
+        // BFGS loop from H = H^-1 = I, where cond = 1 (optbfgs.cpp:363-371)
+        bfgs_reset(a, s, n, lane);
+        if (lane == 0)
+            si[SI_BFGS] = 0;
+        if (1.0 < a.condHMaxBfgs && 0 < a.maxBfgsIter) {
+            bfgs_step(a, pb, L, s, lane, gpn, fH, err);
+        } else {
+            __syncwarp();
+            if (lane == 0)
+                si[SI_STATE] = S_NEWTON;   // no step: evaluate again
+        }
+        return;
+    }
     if (err <= sc[SC_RTOL]) {
         cb_converge(a, pb, L, s, lane);
         return;
@@ -1533,7 +1739,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         }
         for (int s = warp; s < T; s += kWarps)
             if (L.ints[s * SI_N + SI_STATE] == S_NEW)
-                (a.optType == 1) ? init_slot_cb(a, pb, L, s, lane, ldv) : init_slot(a, pb, L, s, lane, ldv);
+                (a.optType != 0) ? init_slot_cb(a, pb, L, s, lane, ldv) : init_slot(a, pb, L, s, lane, ldv);
         __syncthreads();
 
         // ---- phase A: evaluation contractions over the quadrature
@@ -1675,7 +1881,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         for (int s = warp; s < T; s += kWarps) {
             int st = L.ints[s * SI_N + SI_STATE];
             if (st == S_NEWTON || st == S_TRIAL) {
-                if (a.optType == 1)
+                if (a.optType != 0)
                     slot_logic_cb(a, pb, L, s, lane, warp);
                 else
                     slot_logic(a, pb, L, s, lane, warp);

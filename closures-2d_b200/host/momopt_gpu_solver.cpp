@@ -133,6 +133,8 @@ int MomOptGpuSolver::tryInit(double dx, double dy, double *maxDtOut)
             lastError = std::string("momopt input error: missing ") + k.k;
             return CL_ERR_ARG;
         }
+    m_opt.max_bfgs_iter = maxIterBfgs;
+    m_opt.cond_h_max_bfgs = condHMaxBfgs;
     // optional extensions (unknown to the reference, ignored by its reader)
     if (!d.get("MOMOPT_TOL_GAMMA", &m_opt.tol_gamma))
         m_opt.tol_gamma = 0.0;

@@ -73,14 +73,20 @@ void cl_angular_free(cl_angular *a);
 /* Solver options: the MOMOPT_* deck keys read at momopt_init.cpp:56-68. */
 typedef struct {
     int moment_type;        /* CL_MN or CL_PPN */
-    int opt_type;           /* 0 Newton (opt.cpp), 1 change of basis (optcb.cpp);
-                               2 (BFGS, optbfgs.cpp) is rejected */
+    int opt_type;           /* MOMOPT_OPTIMIZATION_TYPE: 0 Newton (opt.cpp),
+                               1 change of basis (optcb.cpp), 2 BFGS
+                               sub-iterations in the change of basis
+                               (optbfgs.cpp) */
     int max_iter;           /* MOMOPT_MAX_ITER */
     double tol;             /* MOMOPT_TOL (relative gradient tolerance) */
     double cond_h_max;      /* MOMOPT_COND_H_MAX */
     double delta_ppn;       /* MOMOPT_DELTA_PPN */
-    double tol_gamma;       /* optional supplementary test, 0 = off (see DESIGN) */
+    double tol_gamma;       /* optional supplementary stopping test
+                               modcfl(d) <= tol_gamma, commented out in
+                               opt.cpp:99-126; 0 = off */
     int precision;          /* CL_FP64 or CL_MIXED */
+    int max_bfgs_iter;      /* MOMOPT_MAX_BFGS_ITER (opt_type 2, >= 1) */
+    double cond_h_max_bfgs; /* MOMOPT_COND_H_MAX_BFGS (opt_type 2) */
 } cl_options;
 
 /* Grid description: Solver fields of solver.h:15-61 for one node. */
@@ -157,10 +163,11 @@ int cl_solve_batch_device(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
 int cl_solve_batch_device_start(cl_ctx *ctx, int count, double *d_u, double *d_alpha,
                                 const double *d_alpha_start, int *d_iters, double *d_reg,
                                 int *d_status);
-/* Change-of-basis solve (optcb(), optcb.cpp:87-415; replaces the
- * OPT_TYPE_CHANGE_BASIS branch of momopt_update.cpp:240-244) on device
- * pointers, for a context created with opt_type 1: each vector carries its
- * basis d_P2M [count][n][n] (row-major, lower triangular) and multipliers
+/* Change-of-basis solves on device pointers: optcb() (optcb.cpp:87-415,
+ * the OPT_TYPE_CHANGE_BASIS branch of momopt_update.cpp:240-244) for a
+ * context created with opt_type 1, optbfgs() (optbfgs.cpp:90-512, the
+ * OPT_TYPE_BFGS branch of momopt_update.cpp:245-248) with opt_type 2.  Each
+ * vector carries its basis d_P2M [count][n][n] (row-major, lower triangular) and multipliers
  * d_alphaP [count][n] in that basis, read at the start and written back on
  * convergence; d_alpha receives the multipliers in the moment basis and d_u
  * the regularised input moments, as the reference returns them.  A grid

@@ -125,7 +125,8 @@ static double inv_norm1_estimate(int n, const double *l, double *x, double *v, i
             x[i] = 0.0;
         x[j] = 1.0;
         orc_chol_solve(n, l, x);
-        memcpy(v, x, sizeof(double) * n);
+        for (int i = 0; i < n; i++)
+            v[i] = x[i];
         double estold = est;
         est = asum(n, v);
         int same = 1;

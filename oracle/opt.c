@@ -580,6 +580,255 @@ static int optcb_scaled(int nm, int nq, double *u, double *P2M, double *alphaP, 
     return status;
 }
 
+/* The reference's cond(): the product of the largest absolute row sums of
+ * the two arrays as it stores them (column-major, so of the columns of the
+ * matrices here) (optbfgs.cpp:515-545). */
+static double bfgs_cond(int n, const double *h, const double *hInv)
+{
+    double n1 = 0.0, n2 = 0.0;
+    for (int j = 0; j < n; j++) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = 0; i < n; i++) {
+            s1 += fabs(h[i * n + j]);
+            s2 += fabs(hInv[i * n + j]);
+        }
+        if (s1 > n1)
+            n1 = s1;
+        if (s2 > n2)
+            n2 = s2;
+    }
+    return n1 * n2;
+}
+
+/* y <- c A x (dgemv N with beta 0: columns of A scaled by c x_j, in order) */
+static void gemv_n(int n, double c, const double *a, const double *x, double *y)
+{
+    for (int i = 0; i < n; i++)
+        y[i] = 0.0;
+    for (int j = 0; j < n; j++) {
+        const double s = c * x[j];
+        for (int i = 0; i < n; i++)
+            y[i] += s * a[i * n + j];
+    }
+}
+
+/* A <- A + c x y^T (dger) */
+static void ger(int n, double c, const double *x, const double *y, double *a)
+{
+    for (int j = 0; j < n; j++) {
+        const double s = c * y[j];
+        for (int i = 0; i < n; i++)
+            a[i * n + j] += x[i] * s;
+    }
+}
+
+static double dot(int n, const double *x, const double *y)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++)
+        s += x[i] * y[i];
+    return s;
+}
+
+/* optbfgs.cpp:163-512.  The outer loop is optcb's Newton iteration in the
+ * change of basis; after each basis change up to maxBfgsIter quasi-Newton
+ * steps run on BFGS approximations of H and H^-1 in the new basis (both
+ * start at the identity), while cond(H) cond(H^-1) < condHMaxBfgs.  Only
+ * the outer iterations are counted. */
+static int optbfgs_scaled(int nm, int nq, double *u, double *P2M, const double *alphaPin,
+                          double *alphaP, double *alphaM, const double *w, const double *p, int np,
+                          orc_options *o, orc_outs *outs)
+{
+    double f = 0.0;
+    double alphaP0[ORC_NMAX], dP[ORC_NMAX], gP[ORC_NMAX], uP[ORC_NMAX], gM[ORC_NMAX];
+    double gOldP[ORC_NMAX], alphaOldP[ORC_NMAX], gDiff[ORC_NMAX], alphaDiff[ORC_NMAX];
+    double tmp[ORC_NMAX];
+    double chol[ORC_NMAX * ORC_NMAX], hP[ORC_NMAX * ORC_NMAX], hInvP[ORC_NMAX * ORC_NMAX];
+    double P2Min[ORC_NMAX * ORC_NMAX];
+    double work[3 * ORC_NMAX];
+    double gExt[ORC_N2MAX];
+    int iwork[ORC_NMAX];
+    double *pP = (double *)malloc(sizeof(double) * (size_t)nq * nm);
+    if (!pP)
+        return ORC_ERR_INPUT;
+    int status = ORC_OK;
+    memcpy(alphaP0, alphaPin, sizeof(double) * nm);
+    memcpy(P2Min, P2M, sizeof(double) * (size_t)nm * (size_t)nm);
+    basis_to_p(nm, nq, P2Min, p, np, pP);
+    int maxIter = o->maxIter;
+    const double tolRel = o->tolRel;
+    double r = 0.0;
+    const double condHMax = o->condHMax;
+    int regIndex = 0;
+    memcpy(uP, u, sizeof(double) * nm);
+    trsv_l(nm, P2M, uP);
+    double rtol = orc_nrm2(nm, u) * tolRel;
+    int iter = 0, totalIter = 0;
+    double t = 1.0, err = 0.0;
+    int hitMaxRegularization = 0;
+    memcpy(alphaP, alphaP0, sizeof(double) * nm);
+
+    while (1) {
+        iter = iter + 1;
+        totalIter = totalIter + 1;
+        f = orc_fobj(o->momentType, nm, nm, nq, alphaP, uP, w, pP, o->deltaPPn, gP, hP, 0, NULL,
+                     gExt);
+        memcpy(chol, hP, sizeof(double) * (size_t)nm * (size_t)nm);
+        int error = orc_cholesky(nm, chol);
+        double norm = orc_norm1(nm, hP);
+        double condest = 1.0 / orc_rcond(nm, chol, norm, work, iwork);
+
+        /* optbfgs.cpp:280-300: first evaluation with a bad Hessian */
+        if (totalIter == 1 && (error != 0 || condest > condHMax)) {
+            isotropic_alpha(nm, alphaP0, o->momentType, o->deltaPPn);
+            set_identity(nm, P2M);
+            set_identity(nm, P2Min);
+            memcpy(alphaP, alphaP0, sizeof(double) * nm);
+            memcpy(uP, u, sizeof(double) * nm);
+            for (int q = 0; q < nq; q++)
+                for (int k = 0; k < nm; k++)
+                    pP[(size_t)q * nm + k] = p[(size_t)q * np + k];
+            rtol = orc_nrm2(nm, u) * tolRel;
+            iter = 0;
+            t = 1.0;
+            continue;
+        }
+
+        /* optbfgs.cpp:303-348 */
+        if (iter >= maxIter || error != 0 || t == 0 || condest > condHMax) {
+            if (regIndex < ORC_NUM_REG - 1) {
+                regIndex++;
+                r = ORC_REGULARIZATIONS[regIndex];
+                uP[0] = 1.0;
+                for (int i = 1; i < nm; i++)
+                    uP[i] = u[i] * (1.0 - r);
+            } else {
+                if (hitMaxRegularization) {
+                    status = ORC_ERR_MAXREG;
+                    break;
+                }
+                isotropic_alpha(nm, alphaP0, o->momentType, o->deltaPPn);
+                set_identity(nm, P2Min);
+                memcpy(uP, u, sizeof(double) * nm);
+                regIndex = 0;
+                hitMaxRegularization = 1;
+                maxIter = o->maxIter;
+            }
+            rtol = orc_nrm2(nm, uP) * tolRel;
+            memcpy(alphaP, alphaP0, sizeof(double) * nm);
+            memcpy(P2M, P2Min, sizeof(double) * (size_t)nm * (size_t)nm);
+            trsv_l(nm, P2M, uP);
+            basis_to_p(nm, nq, P2M, p, np, pP);
+            iter = 0;
+            t = 1.0;
+            if (regIndex == ORC_NUM_REG - 1)
+                maxIter = 10 * maxIter;
+            continue;
+        }
+
+        /* optbfgs.cpp:351-364: change of basis by L, H and H^-1 become I */
+        trsv_l(nm, chol, gP);
+        for (int q = 0; q < nq; q++)
+            trsv_l(nm, chol, pP + (size_t)q * nm);
+        trmm_rl(nm, P2M, chol);
+        trmv_lt(nm, chol, alphaP);
+        trsv_l(nm, chol, uP);
+        set_identity(nm, hP);
+        set_identity(nm, hInvP);
+
+        int solved = 0, iterTempBfgs = 0;
+        while (bfgs_cond(nm, hP, hInvP) < o->condHMaxBfgs && iterTempBfgs < o->maxBfgsIter) {
+            iterTempBfgs++;
+            gemv_n(nm, -1.0, hInvP, gP, dP);
+            memcpy(gM, gP, sizeof(double) * nm);
+            trmv_l(nm, P2M, gM);
+            err = orc_nrm2(nm, gM);
+            if (err <= rtol) {
+                memcpy(alphaM, alphaP, sizeof(double) * nm);
+                trsv_lt(nm, P2M, alphaM);
+                u[0] = 1.0;
+                for (int i = 1; i < nm; i++)
+                    u[i] = u[i] * (1.0 - r);
+                solved = 1;
+                break;
+            }
+            memcpy(alphaOldP, alphaP, sizeof(double) * nm);
+            memcpy(gOldP, gP, sizeof(double) * nm);
+            t = linesearch(nm, nm, nq, alphaP, dP, f, gP, uP, w, pP, o->deltaPPn, o->momentType, gExt);
+            f = orc_fobj(o->momentType, nm, nm, nq, alphaP, uP, w, pP, o->deltaPPn, gP, NULL, 0, NULL,
+                         gExt);
+            for (int i = 0; i < nm; i++) {
+                gDiff[i] = gP[i] - gOldP[i];
+                alphaDiff[i] = alphaP[i] - alphaOldP[i];
+            }
+            /* H += g g^T / (a.g) - (H a)(H a)^T / (a.H a)   (optbfgs.cpp:455-466);
+             * a failed line search (a = 0) divides by zero, and the NaN in
+             * cond() ends the loop, as in the reference */
+            double coef = 1.0 / dot(nm, alphaDiff, gDiff);
+            ger(nm, coef, gDiff, gDiff, hP);
+            gemv_n(nm, 1.0, hP, alphaDiff, tmp);
+            coef = -1.0 / dot(nm, alphaDiff, tmp);
+            ger(nm, coef, tmp, tmp, hP);
+            /* H^-1 update (optbfgs.cpp:469-485) */
+            gemv_n(nm, 1.0, hInvP, gDiff, tmp);
+            const double gHg = dot(nm, gDiff, tmp);
+            const double ag = dot(nm, alphaDiff, gDiff);
+            coef = (gHg + ag) / (ag * ag);
+            ger(nm, coef, alphaDiff, alphaDiff, hInvP);
+            coef = -1.0 / ag;
+            ger(nm, coef, tmp, alphaDiff, hInvP);
+            ger(nm, coef, alphaDiff, tmp, hInvP);
+        }
+        if (solved)
+            break;
+    }
+    if (outs != NULL) {
+        outs->iter = totalIter;
+        outs->normG = err;
+        outs->r = r;
+    }
+    free(pP);
+    return status;
+}
+
+/* optbfgs.cpp:90-154: scaling wrapper (optScaled iterates on alphaP from a
+ * copy of the input) */
+int orc_optbfgs(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
+                orc_options options, const double *w, const double *p, int np, orc_outs *outs)
+{
+    if (nm > ORC_NMAX)
+        return ORC_ERR_INPUT;
+    const double u0 = u[0];
+    if (u0 <= 0)
+        return ORC_ERR_U0;
+    if (options.maxBfgsIter < 1)
+        return ORC_ERR_INPUT;   /* no step would ever be taken */
+    double alphaPin[ORC_NMAX];
+    memcpy(alphaPin, alphaP, sizeof(double) * nm);
+    int status;
+    if (options.momentType == ORC_MN) {
+        const double alphaScale = log(u0) * 2.0 * sqrt(M_PI);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] / u0;
+        status = optbfgs_scaled(nm, nq, u, P2M, alphaPin, alphaP, alphaM, w, p, np, &options, outs);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] * u0;
+        alphaM[0] = alphaM[0] + alphaScale;
+    } else if (options.momentType == ORC_PPN) {
+        options.deltaPPn = options.deltaPPn / (u0 * u0);
+        for (int i = 0; i < nm; i++)
+            u[i] = u[i] / u0;
+        status = optbfgs_scaled(nm, nq, u, P2M, alphaPin, alphaP, alphaM, w, p, np, &options, outs);
+        for (int i = 0; i < nm; i++) {
+            alphaM[i] = alphaM[i] * u0;
+            u[i] = u[i] * u0;
+        }
+    } else {
+        return ORC_ERR_INPUT;
+    }
+    return status;
+}
+
 /* optcb.cpp:87-153: scaling wrapper */
 int orc_optcb(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
               orc_options options, const double *w, const double *p, int np, orc_outs *outs)
@@ -624,16 +873,17 @@ void orc_optcb_init(int nm, int momentType, double delta, double *P2M, double *a
     isotropic_alpha(nm, alphaP, momentType, delta);
 }
 
-int orc_optcb_batch(const orc_setup *s, orc_options opts, int count, double *u, double *P2M,
-                    double *alphaP, double *alpha, int *iters, double *regs, int *status)
+int orc_optcb_batch(const orc_setup *s, orc_options opts, int optType, int count, double *u,
+                    double *P2M, double *alphaP, double *alpha, int *iters, double *regs, int *status)
 {
     const int n = s->n;
     int worst = ORC_OK;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int c = 0; c < count; c++) {
         orc_outs outs = {0.0, 0, 0.0};
-        int st = orc_optcb(n, s->nq, u + (size_t)c * n, P2M + (size_t)c * n * n, alphaP + (size_t)c * n,
-                           alpha + (size_t)c * n, opts, s->w, s->p, s->n2, &outs);
+        int st = (optType == 2 ? orc_optbfgs : orc_optcb)(n, s->nq, u + (size_t)c * n, P2M + (size_t)c * n * n,
+                                                          alphaP + (size_t)c * n, alpha + (size_t)c * n, opts,
+                                                          s->w, s->p, s->n2, &outs);
         if (iters)
             iters[c] = outs.iter;
         if (regs)

@@ -38,7 +38,7 @@ extern const double ORC_REGULARIZATIONS[ORC_NUM_REG];
  * the oracle returns them so tests can observe the failure. */
 enum { ORC_OK = 0, ORC_ERR_U0 = -1, ORC_ERR_MAXREG = -2, ORC_ERR_INPUT = -3 };
 
-/* opt/opt.h:11-23 (BFGS-only fields dropped; tolAbs is unused by opt.cpp). */
+/* opt/opt.h:11-23 (tolAbs is unused by the optimisers). */
 typedef struct {
     int momentType;
     int maxIter;
@@ -52,6 +52,10 @@ typedef struct {
      * reference's current behaviour; 1.1 reproduces the revision that wrote
      * the delta and lattice regression goldens. */
     double tolGamma;
+    /* BFGS only (optbfgs.cpp): quasi-Newton steps per Hessian evaluation and
+     * the bound on cond(H) * cond(H^-1) of the BFGS approximations */
+    int maxBfgsIter;
+    double condHMaxBfgs;
 } orc_options;
 
 /* opt/opt.h:25-32 */
@@ -105,8 +109,13 @@ int orc_optcb(int nm, int nq, double *u, double *P2M, double *alphaP, double *al
               orc_options opts, const double *w, const double *p, int np, orc_outs *outs);
 /* momopt_init.cpp:146-157 initial state of a cell (see opt.c). */
 void orc_optcb_init(int nm, int momentType, double delta, double *P2M, double *alphaP);
-int orc_optcb_batch(const orc_setup *s, orc_options opts, int count, double *u, double *P2M,
-                    double *alphaP, double *alpha, int *iters, double *regs, int *status);
+/* BFGS sub-iterations in the change of basis: opt/optbfgs.cpp (type 2); same
+ * per-cell state and initialisation as orc_optcb. */
+int orc_optbfgs(int nm, int nq, double *u, double *P2M, double *alphaP, double *alphaM,
+                orc_options options, const double *w, const double *p, int np, orc_outs *outs);
+/* optType 1: orc_optcb, 2: orc_optbfgs on every vector */
+int orc_optcb_batch(const orc_setup *s, orc_options opts, int optType, int count, double *u,
+                    double *P2M, double *alphaP, double *alpha, int *iters, double *regs, int *status);
 
 /* f,g,H evaluation (fobj.cpp); g and h may be NULL as in the reference. */
 double orc_fobj(int momentType, int n, int n2, int nq, const double *alpha,
@@ -122,8 +131,8 @@ typedef struct {
     double ax, ay, bx, by, tFinal, outDeltaT, gaussianSigma, floor_, sigma;
     int initCond;
     /* momopt deck (momopt_init.cpp:56-68) */
-    int momentOrder, quadOrder, useGaunt, momentType, optType, maxIter;
-    double cflFactor, tol, condHMax, theta, deltaPPn;
+    int momentOrder, quadOrder, useGaunt, momentType, optType, maxIter, maxBfgsIter;
+    double cflFactor, tol, condHMax, condHMaxBfgs, theta, deltaPPn;
     double tolGamma;        /* optional key MOMOPT_TOL_GAMMA, default 0 (off) */
 } orc_deck;
 
@@ -142,7 +151,7 @@ typedef struct {
     double dx, dy, maxDt;
     double *initialGrid, *sigmaT, *sigmaS;   /* [NX*NY] */
     double *moments, *alpha, *flux, *momentsOld, *ansatzGrid;
-    double *alphaP, *P2M;   /* change-of-basis state per cell (optType 1) */
+    double *alphaP, *P2M;   /* change-of-basis state per cell (optType 1, 2) */
     orc_stats stats;
     int *lastIters;         /* per-cell iterations of the last stage */
     int status;             /* first error code seen */

@@ -28,11 +28,12 @@ int orc_batch(int order, int Q, int useGaunt, int momentType, int maxIter, doubl
     return st;
 }
 
-/* Batched change-of-basis opt (optcb.cpp) with per-vector P2M and alphaP
- * state, in place. */
-int orc_batch_cb(int order, int Q, int momentType, int maxIter, double tol, double condHMax,
-                 double deltaPPn, int count, double *u, double *P2M, double *alphaP, double *alpha,
-                 int *iters, double *regs, int *status)
+/* Batched change-of-basis opt (optType 1: optcb.cpp, 2: optbfgs.cpp) with
+ * per-vector P2M and alphaP state, in place. */
+int orc_batch_cb(int order, int Q, int momentType, int optType, int maxIter, double tol,
+                 double condHMax, double deltaPPn, int maxBfgsIter, double condHMaxBfgs, int count,
+                 double *u, double *P2M, double *alphaP, double *alpha, int *iters, double *regs,
+                 int *status)
 {
     orc_setup s;
     int st = orc_setup_create(order, Q, 0, &s);
@@ -45,7 +46,9 @@ int orc_batch_cb(int order, int Q, int momentType, int maxIter, double tol, doub
     o.tolRel = tol;
     o.condHMax = condHMax;
     o.deltaPPn = deltaPPn;
-    st = orc_optcb_batch(&s, o, count, u, P2M, alphaP, alpha, iters, regs, status);
+    o.maxBfgsIter = maxBfgsIter;
+    o.condHMaxBfgs = condHMaxBfgs;
+    st = orc_optcb_batch(&s, o, optType, count, u, P2M, alphaP, alpha, iters, regs, status);
     orc_setup_free(&s);
     return st;
 }

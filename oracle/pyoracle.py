@@ -61,8 +61,9 @@ def _bind(L):
         L.orc_solver_stats.argtypes = [vp, ip, dp, C.POINTER(C.c_longlong), ip]
         L.orc_solver_close.argtypes = [vp]
         L.orc_solver_last_iters.argtypes = [vp, ip]
-        L.orc_batch_cb.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                   C.c_double, C.c_int, dp, dp, dp, dp, ip, dp, ip]
+        L.orc_batch_cb.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, dp, dp, dp,
+                                   dp, ip, dp, ip]
         L.orc_cb_init.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, dp, dp]
         L.orc_cb_init.restype = None
     return L
@@ -115,15 +116,18 @@ def cb_init(n, count, moment_type=0, delta_ppn=1e-10):
 
 
 def optcb_batch(order, Q, u, P2M, alphaP, alpha, moment_type=0, max_iter=100, tol=1e-8,
-                cond_h_max=1e10, delta_ppn=1e-10, fma=False):
-    """Change-of-basis opt (optcb.cpp) on each row in place: u, P2M, alphaP
-    updated, alpha receives the multipliers.  Returns iters, regs, status."""
+                cond_h_max=1e10, delta_ppn=1e-10, fma=False, opt_type=1, max_bfgs_iter=5,
+                cond_h_max_bfgs=20.0):
+    """Change-of-basis opt (opt_type 1: optcb.cpp, 2: optbfgs.cpp) on each
+    row in place: u, P2M, alphaP updated, alpha receives the multipliers.
+    Returns iters, regs, status."""
     count = u.shape[0]
     iters = np.zeros(count, np.int32)
     regs = np.zeros(count)
     status = np.zeros(count, np.int32)
-    lib(fma).orc_batch_cb(order, Q, moment_type, max_iter, tol, cond_h_max, delta_ppn, count, _dp(u),
-                          _dp(P2M), _dp(alphaP), _dp(alpha), _ip(iters), _dp(regs), _ip(status))
+    lib(fma).orc_batch_cb(order, Q, moment_type, opt_type, max_iter, tol, cond_h_max, delta_ppn,
+                          max_bfgs_iter, cond_h_max_bfgs, count, _dp(u), _dp(P2M), _dp(alphaP),
+                          _dp(alpha), _ip(iters), _dp(regs), _ip(status))
     return iters, regs, status
 
 

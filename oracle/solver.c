@@ -134,16 +134,14 @@ int orc_deck_read(const char *path, orc_deck *d)
     ok &= kv_dbl(&l, "FLOOR", &d->floor_);
     ok &= kv_int(&l, "INIT_COND", &d->initCond);
     ok &= kv_dbl(&l, "SIGMA", &d->sigma);
-    double dummy;
-    int idummy;
     ok &= kv_int(&l, "MOMOPT_MOMENT_ORDER", &d->momentOrder);
     ok &= kv_int(&l, "MOMOPT_QUAD_ORDER", &d->quadOrder);
     ok &= kv_dbl(&l, "MOMOPT_CFL_FACTOR", &d->cflFactor);
     ok &= kv_dbl(&l, "MOMOPT_TOL", &d->tol);
     ok &= kv_dbl(&l, "MOMOPT_COND_H_MAX", &d->condHMax);
-    ok &= kv_dbl(&l, "MOMOPT_COND_H_MAX_BFGS", &dummy);
+    ok &= kv_dbl(&l, "MOMOPT_COND_H_MAX_BFGS", &d->condHMaxBfgs);
     ok &= kv_int(&l, "MOMOPT_MAX_ITER", &d->maxIter);
-    ok &= kv_int(&l, "MOMOPT_MAX_BFGS_ITER", &idummy);
+    ok &= kv_int(&l, "MOMOPT_MAX_BFGS_ITER", &d->maxBfgsIter);
     ok &= kv_int(&l, "MOMOPT_USE_GAUNT", &d->useGaunt);
     ok &= kv_dbl(&l, "MOMOPT_THETA", &d->theta);
     ok &= kv_dbl(&l, "MOMOPT_DELTA_PPN", &d->deltaPPn);
@@ -165,7 +163,7 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
 {
     memset(s, 0, sizeof(*s));
     s->deck = *d;
-    if ((d->optType != 0 && d->optType != 1) || (d->momentType != ORC_MN && d->momentType != ORC_PPN))
+    if (d->optType < 0 || d->optType > 2 || (d->momentType != ORC_MN && d->momentType != ORC_PPN))
         return ORC_ERR_INPUT;
     const int ng = 2;
     int sizeX = d->numCellsX, sizeY = d->numCellsY;
@@ -247,7 +245,7 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
     s->momentsOld = (double *)calloc(C * n, sizeof(double));
     s->ansatzGrid = (double *)malloc(sizeof(double) * C);
     s->lastIters = (int *)calloc(C, sizeof(int));
-    if (d->optType == 1) {
+    if (d->optType == 1 || d->optType == 2) {
         /* momopt_init.cpp:114-157 */
         s->alphaP = (double *)malloc(sizeof(double) * C * n);
         s->P2M = (double *)malloc(sizeof(double) * C * n * n);
@@ -326,11 +324,17 @@ static void solve_optimization(orc_solver *s)
     o.deltaPPn = d->deltaPPn;
     o.useGaunt = (d->useGaunt == 1);
     o.tolGamma = d->tolGamma;
+    o.maxBfgsIter = d->maxBfgsIter;
+    o.condHMaxBfgs = d->condHMaxBfgs;
 #pragma omp parallel for schedule(dynamic, 1)
     for (long index = 0; index < (long)C; index++) {
         orc_outs outs = {0.0, 0, 0.0};
         int st;
-        if (d->optType == 1)
+        if (d->optType == 2)
+            st = orc_optbfgs(n, s->set.nq, &s->moments[(size_t)index * n], &s->P2M[(size_t)index * n * n],
+                             &s->alphaP[(size_t)index * n], &s->alpha[(size_t)index * n], o, s->set.w,
+                             s->set.p, s->set.n2, &outs);
+        else if (d->optType == 1)
             st = orc_optcb(n, s->set.nq, &s->moments[(size_t)index * n], &s->P2M[(size_t)index * n * n],
                            &s->alphaP[(size_t)index * n], &s->alpha[(size_t)index * n], o, s->set.w,
                            s->set.p, s->set.n2, &outs);

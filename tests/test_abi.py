@@ -74,22 +74,23 @@ def test_no_cpu_fallback():
     assert e.value.code == cb.CL_ERR_CUDA
 
 
-def test_rejects_bfgs_accepts_change_of_basis(tmp_path):
-    """MOMOPT_OPTIMIZATION_TYPE 2 (BFGS) is an input error; type 1 (change of
-    basis) passes validation and, without a GPU, stops at the device."""
-    d = tmp_path / "deck2"
-    decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=2,
-                                              moment_order=1, quad_order=4))
-    with pytest.raises(cb.ClosuresError) as e:
-        cb.Solver(str(d), str(tmp_path))
-    assert e.value.code == cb.CL_ERR_ARG
-    assert "OPTIMIZATION_TYPE" in str(e.value)
-    d = tmp_path / "deck1"
-    decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, opt_type=1,
-                                              moment_order=1, quad_order=4))
-    with pytest.raises(cb.ClosuresError) as e:
-        cb.Solver(str(d), str(tmp_path))
-    assert e.value.code == cb.CL_ERR_CUDA
+def test_optimization_types_are_validated(tmp_path):
+    """MOMOPT_OPTIMIZATION_TYPE 0-2 pass validation and, without a GPU, stop
+    at the device; type 3 and BFGS without sub-iterations
+    (MOMOPT_MAX_BFGS_ITER 0, where optbfgs.cpp never steps) are input errors."""
+    def solver_error(name, **kw):
+        d = tmp_path / name
+        decks.write_deck(str(d), decks.deck_text(num_cells_x=4, num_cells_y=4, moment_order=1,
+                                                  quad_order=4, **kw))
+        with pytest.raises(cb.ClosuresError) as e:
+            cb.Solver(str(d), str(tmp_path))
+        return e.value
+    for t in (1, 2):
+        assert solver_error("deck%d" % t, opt_type=t).code == cb.CL_ERR_CUDA
+    e = solver_error("deck3", opt_type=3)
+    assert e.code == cb.CL_ERR_ARG and "OPTIMIZATION_TYPE" in str(e)
+    e = solver_error("deck_bfgs0", opt_type=2, max_bfgs_iter=0)
+    assert e.code == cb.CL_ERR_ARG and "MAX_BFGS_ITER" in str(e)
 
 
 def test_missing_deck_key_is_an_input_error(tmp_path):

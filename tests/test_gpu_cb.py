@@ -1,7 +1,8 @@
-"""Change-of-basis Newton (MOMOPT_OPTIMIZATION_TYPE 1, optcb.cpp) on the GPU
-against the oracle's restatement: two calls in a row on the same vectors,
-the second starting from the basis and alphaP the first one stored, and
-grid steps of a deck with optimisation type 1."""
+"""Change-of-basis solves on the GPU against the oracle's restatements:
+Newton (MOMOPT_OPTIMIZATION_TYPE 1, optcb.cpp) and BFGS sub-iterations
+(type 2, optbfgs.cpp).  Two calls in a row on the same vectors, the second
+starting from the bases and alphaP the first one stored, and grid steps of
+decks with those optimisation types."""
 import numpy as np
 import pytest
 
@@ -17,10 +18,10 @@ CASES = [(2, 20, cb.CL_MN, 0), (3, 30, cb.CL_MN, 0), (4, 30, cb.CL_MN, 0), (6, 4
          (3, 20, cb.CL_PPN, 0), (4, 30, cb.CL_MN, 1), (6, 40, cb.CL_MN, 1), (3, 20, cb.CL_PPN, 1)]
 
 
-def _gpu_call(a, u, P2M, aP, moment_type):
+def _gpu_call(a, u, P2M, aP, moment_type, opt_type):
     import torch
     dev = torch.device("cuda", 0)
-    ctx = cb.Context.for_batches(a, cb.make_options(moment_type=moment_type, tol=1e-8, opt_type=1))
+    ctx = cb.Context.for_batches(a, cb.make_options(moment_type=moment_type, tol=1e-8, opt_type=opt_type))
     cnt = u.shape[0]
     dP = torch.from_numpy(P2M.copy()).to(dev)
     dA = torch.from_numpy(aP.copy()).to(dev)
@@ -36,16 +37,18 @@ def _gpu_call(a, u, P2M, aP, moment_type):
             st.cpu().numpy(), dP.cpu().numpy(), dA.cpu().numpy())
 
 
-def _oracle_call(order, Q, u, P2M, aP, moment_type, fma=False):
+def _oracle_call(order, Q, u, P2M, aP, moment_type, opt_type, fma=False):
     P, A = P2M.copy(), aP.copy()
     uu = u.copy()
     al = np.zeros_like(u)
-    it, rg, st = oracle_lib.optcb_batch(order, Q, uu, P, A, al, moment_type=moment_type, fma=fma)
+    it, rg, st = oracle_lib.optcb_batch(order, Q, uu, P, A, al, moment_type=moment_type, fma=fma,
+                                        opt_type=opt_type)
     return (uu, al, it, rg, st, P, A)
 
 
+@pytest.mark.parametrize("opt_type", [1, 2])
 @pytest.mark.parametrize("order,Q,mt,gaunt", CASES)
-def test_change_of_basis_matches_oracle(order, Q, mt, gaunt):
+def test_change_of_basis_matches_oracle(order, Q, mt, gaunt, opt_type):
     a = cb.Angular(order, Q, gaunt)
     u, _ = cb.sample_moment_vectors(a, 400, seed=13, s_range=(0.1, 3.0))
     P2M, aP = oracle_lib.cb_init(a.n, u.shape[0], mt, 1e-10)
@@ -54,9 +57,9 @@ def test_change_of_basis_matches_oracle(order, Q, mt, gaunt):
     # the first call), the second from bases adapted to these vectors
     second = []
     for call in range(2):
-        g = _gpu_call(a, u, P2M, aP, mt)
-        o = _oracle_call(order, Q, u, P2M, aP, mt)
-        f = _oracle_call(order, Q, u, P2M, aP, mt, fma=True)
+        g = _gpu_call(a, u, P2M, aP, mt, opt_type)
+        o = _oracle_call(order, Q, u, P2M, aP, mt, opt_type)
+        f = _oracle_call(order, Q, u, P2M, aP, mt, opt_type, fma=True)
         ug, ag, itg, rgg, stg, Pg, Ag = g
         uo, ao, ito, rgo, sto, Po, Ao = o
         uf, af, itf, rgf, stf, _, _ = f
@@ -83,21 +86,22 @@ def test_change_of_basis_matches_oracle(order, Q, mt, gaunt):
 
 GRID = [
     ("m3_gaussian", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.4, moment_order=3,
-                         quad_order=20, tol=1e-8, use_gaunt=0, opt_type=1)),
+                         quad_order=20, tol=1e-8, use_gaunt=0)),
     # a pulse resolved by the grid: a sharper one (sigma 0.1 on dx 0.15) has
     # near-boundary cells whose regularisation steps the quadrature's
     # summation order decides, for plain Newton as well
     ("m4_pulse", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.25, floor=1e-8, moment_order=4,
-                      quad_order=30, tol=1e-8, use_gaunt=0, opt_type=1)),
+                      quad_order=30, tol=1e-8, use_gaunt=0)),
     ("m4_pulse_gaunt", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.25, floor=1e-8,
-                            moment_order=4, quad_order=30, tol=1e-8, use_gaunt=1, opt_type=1)),
+                            moment_order=4, quad_order=30, tol=1e-8, use_gaunt=1)),
 ]
 
 
+@pytest.mark.parametrize("opt_type", [1, 2])
 @pytest.mark.parametrize("name,kw", GRID, ids=[g[0] for g in GRID])
-def test_change_of_basis_grid_steps_match_oracle(tmp_path, name, kw):
+def test_change_of_basis_grid_steps_match_oracle(tmp_path, name, kw, opt_type):
     deck = str(tmp_path / "input.deck")
-    decks.write_deck(deck, decks.deck_text(**kw))
+    decks.write_deck(deck, decks.deck_text(opt_type=opt_type, **kw))
     orc = oracle_lib.GridSolver(deck)
     fma = oracle_lib.GridSolver(deck, fma=True)
     s = cb.Solver(deck, str(tmp_path))
@@ -114,8 +118,8 @@ def test_change_of_basis_grid_steps_match_oracle(tmp_path, name, kw):
     err = float(np.max(np.abs(m_g - m_o) / scale))
     env = float(np.max(np.abs(m_f - m_o) / scale))
     so, sg = orc.stats(), s.stats()
-    print("grid change of basis %s: moments %.3e (oracle builds %.3e), iterations gpu %.3f oracle %.3f"
-          % (name, err, env, sg["iter_mean"], so["iter_mean"]))
+    print("grid change of basis (type %d) %s: moments %.3e (oracle builds %.3e), iterations gpu %.3f oracle %.3f"
+          % (opt_type, name, err, env, sg["iter_mean"], so["iter_mean"]))
     assert sg["num_solves"] == so["num_solves"]
     if env < 1e-10:
         # rounding does not move the reference here: same decisions up to
