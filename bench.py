@@ -17,8 +17,12 @@ so no explicit L2 flush is needed between steps.
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle restatement, OpenMP over all host threads) on the same deck.
-Under torchrun each rank runs an independent replica (weak scaling); the
-timed region is bracketed by barriers and the max over ranks is reported.
+Under torchrun (N ranks, one GPU each) grid workloads run partitioned as the
+reference's MPI build runs them: the deck's grid is widened N times in x and
+split into N x 1 nodes (NUM_MPI_PARTITIONS_X = N), each rank stepping one
+node of the workload's size and exchanging its halo with its neighbours over
+NCCL before every RK stage (weak scaling).  The timed region is bracketed by
+barriers and the max over ranks is reported.
 """
 import argparse
 import json
@@ -137,10 +141,17 @@ def dist_setup():
     return world, rank, local
 
 
-def write_deck(tmpdir, workload, precision="fp64", opt_type=0):
+def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1):
+    """The workload's deck; with nodes > 1 the grid and domain are widened
+    nodes times in x and split into nodes x 1 partitions, so every node holds
+    the workload's grid."""
     path = os.path.join(tmpdir, "input.deck")
     kw = dict(WORKLOADS[workload])
     kw["opt_type"] = opt_type
+    if nodes > 1:
+        kw["num_cells_x"] = kw["num_cells_x"] * nodes
+        kw["b_x"] = kw.get("a_x", -1.5) + (kw.get("b_x", 1.5) - kw.get("a_x", -1.5)) * nodes
+        kw["partitions"] = (nodes, 1)
     if precision == "mixed":
         kw["extra"] = {"MOMOPT_GPU_PRECISION": "mixed"}
     decks.write_deck(path, decks.deck_text(**kw))
@@ -292,8 +303,11 @@ def native_arm(args, world, rank, local):
                                 device_id=torch.device("cuda", local))
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
-    deck = write_deck(tmp, args.workload, args.precision, args.opt_type)
-    solver = cb.Solver(deck, tmp)
+    deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world)
+    if world > 1:
+        solver = cb.NodeSolver(deck, tmp, node=rank, num_nodes=world)
+    else:
+        solver = cb.Solver(deck, tmp)
     ctx = solver.context()
     dt, dx, dy = solver.max_dt, solver.dx, solver.dy
     C = solver.NX * solver.NY
@@ -335,14 +349,27 @@ def native_arm(args, world, rank, local):
     sampler.start()
     t0 = time.perf_counter()
     kernel_ms = np.zeros(4)
+    exchange_ms = 0.0
     for _ in range(args.steps):
-        kernel_ms += np.array(ctx.step_timed(dt, dx, dy))
+        if world > 1:
+            for stage in (1, 2):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(solver.stream)
+                solver.exchange()
+                e1.record(solver.stream)
+                k1, fl = solver.stage_timed(stage, dt)
+                kernel_ms[2 * (stage - 1)] += k1
+                kernel_ms[2 * (stage - 1) + 1] += fl
+                exchange_ms += e0.elapsed_time(e1)
+        else:
+            kernel_ms += np.array(ctx.step_timed(dt, dx, dy))
     barrier()
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     launches = cb.launch_count() - launches0
     st1 = solver.stats()
-    device_ms = float(kernel_ms.sum())
+    device_ms = float(kernel_ms.sum()) + exchange_ms
     if world > 1:
         import torch.distributed as dist
         tt = torch.tensor([device_ms], device="cuda")
@@ -379,7 +406,7 @@ def native_arm(args, world, rank, local):
     t1 = time.perf_counter()
     for _ in range(e2e_steps):
         ctx.set_state(hm, ha)
-        ctx.step(dt, dx, dy)
+        solver.update(dt)
         lib = cb.lib()
         rc = lib.cl_get_state(ctx._ctx, cb._dp(hm), cb._dp(ha))
         if rc:
@@ -420,18 +447,20 @@ def native_arm(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f64, Hessian-only tiles split tf32",
             "data": "synthetic",
-            "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+            "config": {"workload": args.workload, "grid": [w["num_cells_x"] * world, w["num_cells_y"]],
+                       "grid_per_gpu": [w["num_cells_x"], w["num_cells_y"]],
                        "moment_order": w["moment_order"], "n": n, "quad_order": w["quad_order"],
                        "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
                        "moment_type": w["moment_type"] if "moment_type" in w else "mn",
                        "newton": args.newton, "precision": args.precision, "opt_type": args.opt_type,
                        "t_start": args.warmup * dt,
                        "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
-                       "parallelism": "replicas" if world > 1 else "single"},
+                       "parallelism": ("halo %dx1 (NCCL point-to-point before each RK stage)" % world)
+                       if world > 1 else "single"},
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
             "fallback_restarts": st1["fallbacks"] - st0["fallbacks"],
             "nn": nn_info,
-            "kernel_ms": {"newton": newton_ms, "flux": flux_ms},
+            "kernel_ms": {"newton": newton_ms, "flux": flux_ms, "halo_exchange": exchange_ms},
             "roofline": {
                 "bound": "fp64", "kernel": dominant,
                 "achieved": ach_newton if dominant == "newton" else ach_flux,

@@ -54,6 +54,12 @@ class cl_grid(C.Structure):
                 ("init_x", C.c_double), ("init_y", C.c_double), ("theta", C.c_double)]
 
 
+class cl_node(C.Structure):
+    _fields_ = [("node", C.c_int), ("nodes_x", C.c_int), ("nodes_y", C.c_int), ("node_x", C.c_int),
+                ("node_y", C.c_int), ("size_x", C.c_int), ("size_y", C.c_int),
+                ("init_x", C.c_double), ("init_y", C.c_double)]
+
+
 class cl_stats(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
                 ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64),
@@ -134,6 +140,20 @@ def lib():
             "cl_solve_batch_noalloc": (C.c_int, [C.POINTER(cl_angular), C.POINTER(cl_options),
                                                  C.c_int, vp, vp, vp, vp, vp, vp]),
             "cl_noalloc_last_error": (C.c_char_p, []),
+            "cl_stage": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double]),
+            "cl_stage_timed": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.POINTER(C.c_float)]),
+            "cl_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_halo_counts": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+            "cl_halo_pack": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_halo_unpack": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_partition": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.POINTER(cl_node)]),
+            "cl_solver_create_node": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int,
+                                                C.POINTER(vp), dp]),
+            "cl_solver_node": (C.c_int, [vp, C.POINTER(cl_node)]),
+            "cl_solver_stage": (C.c_int, [vp, C.c_int, C.c_double]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -377,7 +397,10 @@ class Solver:
         md = C.c_double()
         _check(lib().cl_solver_create(deck_path.encode(), out_dir.encode(), C.byref(self._s),
                                       C.byref(md)), lib().cl_global_error)
-        self.max_dt = md.value
+        self._geometry(md.value)
+
+    def _geometry(self, max_dt):
+        self.max_dt = max_dt
         nx, ny, n = C.c_int(), C.c_int(), C.c_int()
         dx, dy, tf, odt = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         lib().cl_solver_geometry(self._s, C.byref(nx), C.byref(ny), C.byref(n), C.byref(dx),
@@ -437,6 +460,221 @@ class Solver:
     def __del__(self):
         if _lib is not None and getattr(self, "_s", None):
             self.close()
+
+
+# ---------------------------------------------------------------------------
+# Partitioned grids: one node per process (GPU) as the reference's MPI build
+# runs them (main.cpp:157-193, comm.cpp:31-147, momopt_boundaries.cpp).
+
+NORTH, SOUTH, EAST, WEST = 0, 1, 2, 3
+SIDES = (NORTH, SOUTH, EAST, WEST)
+OPPOSITE = {NORTH: SOUTH, SOUTH: NORTH, EAST: WEST, WEST: EAST}
+
+
+def partition(num_cells_x, num_cells_y, nodes_x, nodes_y, num_nodes, node, ax, ay, bx, by):
+    """The block of `node` (main.cpp:157-193) as a dict of cl_node's fields."""
+    out = cl_node()
+    _check(lib().cl_partition(num_cells_x, num_cells_y, nodes_x, nodes_y, num_nodes, node, ax, ay,
+                              bx, by, C.byref(out)), lib().cl_global_error)
+    return {f: getattr(out, f) for f, _ in cl_node._fields_}
+
+
+class HaloPlan:
+    """comm.cpp:31-147 for one node: peer[side] is the node that side
+    exchanges with -- the neighbour in the partition, across the domain edge
+    for the periodic initial condition (INIT_COND 2), itself when the
+    partition has one node in that direction -- or None at a domain edge.
+    The data a node sends towards `side` fills its peer's ghost strip on the
+    opposite side."""
+
+    def __init__(self, node, nodes_x, nodes_y, periodic):
+        self.node = node
+        nx_, ny_ = node // nodes_y, node % nodes_y
+        idx = lambda x, y: (y + nodes_y) % nodes_y + nodes_y * ((x + nodes_x) % nodes_x)
+        self.peer = {
+            NORTH: idx(nx_, ny_ + 1) if (periodic or ny_ < nodes_y - 1) else None,
+            SOUTH: idx(nx_, ny_ - 1) if (periodic or ny_ > 0) else None,
+            EAST: idx(nx_ + 1, ny_) if (periodic or nx_ < nodes_x - 1) else None,
+            WEST: idx(nx_ - 1, ny_) if (periodic or nx_ > 0) else None,
+        }
+
+
+def exchange_local(plans, sends, recvs):
+    """All nodes of a partition in one process: recvs[b][opposite side] <-
+    sends[a][side] for every side of every node a with peer b (numpy arrays
+    or tensors on one device, in launch order)."""
+    for a, plan in enumerate(plans):
+        for side in SIDES:
+            b = plan.peer[side]
+            if b is not None:
+                recvs[b][OPPOSITE[side]][...] = sends[a][side]
+
+
+def exchange_distributed(plan, send, recv, group=None):
+    """This process's node of a partition with one process per node
+    (torch.distributed ranks = nodes; NCCL on GPUs, gloo on CPUs): the
+    point-to-point messages of comm.cpp:99-137 in one batch.  Sends go out in
+    side order and each receive is posted in the order of the sender's side,
+    so backends that match messages by order (NCCL) and by tag agree; a node
+    that is its own peer copies locally, as MPI delivers a message to self."""
+    import torch.distributed as dist
+    ops = []
+    for side in SIDES:
+        p = plan.peer[side]
+        if p is not None and p != plan.node:
+            ops.append(dist.P2POp(dist.isend, send[side], p, group, side))
+    for side in SIDES:
+        p = plan.peer[OPPOSITE[side]]
+        if p is not None and p != plan.node:
+            ops.append(dist.P2POp(dist.irecv, recv[OPPOSITE[side]], p, group, side))
+    for side in SIDES:
+        if plan.peer[side] == plan.node:
+            recv[OPPOSITE[side]].copy_(send[side])
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+
+
+def deck_value(deck_path, key):
+    """A deck entry as the reference's reader sees it (key case-insensitive,
+    first whitespace-separated token after it), or None."""
+    with open(deck_path) as f:
+        for line in f:
+            tok = line.split()
+            if len(tok) >= 2 and tok[0].upper() == key.upper():
+                return tok[1]
+    return None
+
+
+class NodeSolver(Solver):
+    """The solver of one node of the deck's NUM_MPI_PARTITIONS_X x _Y
+    partition (num_nodes nodes, this one `node`), stepped as the reference's
+    MPI build steps it: before each RK stage the halo strips go to the
+    neighbour nodes (comm.cpp:31-147), then the stage runs on the device.
+    The halo buffers are device tensors; pack, exchange and unpack are
+    ordered with the library's stream, so no host synchronisation is needed
+    inside a step.  Output files are out_<t>_<node>.{pn,opt}."""
+
+    def __init__(self, deck_path, out_dir=".", node=0, num_nodes=1, device=None):
+        import torch
+        self._s = C.c_void_p()
+        md = C.c_double()
+        _check(lib().cl_solver_create_node(deck_path.encode(), out_dir.encode(), node, num_nodes,
+                                           C.byref(self._s), C.byref(md)), lib().cl_global_error)
+        self._geometry(md.value)
+        info = cl_node()
+        lib().cl_solver_node(self._s, C.byref(info))
+        self.node_info = {f: getattr(info, f) for f, _ in cl_node._fields_}
+        periodic = int(deck_value(deck_path, "INIT_COND") or 0) == 2
+        self.plan = HaloPlan(node, info.nodes_x, info.nodes_y, periodic)
+        self._ctxp = lib().cl_solver_context(self._s)
+        counts = (C.c_longlong * 4)()
+        lib().cl_halo_counts(self._ctxp, counts)
+        self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.send = [torch.empty(int(c), dtype=torch.float64, device=self.device) for c in counts]
+        self.recv = [torch.empty(int(c), dtype=torch.float64, device=self.device) for c in counts]
+        st = C.c_void_p()
+        lib().cl_stream(self._ctxp, C.byref(st))
+        self.stream = torch.cuda.ExternalStream(st.value, device=self.device)
+
+    def _ptrs(self, bufs, sides):
+        return (C.c_void_p * 4)(*[bufs[k].data_ptr() if k in sides else None for k in SIDES])
+
+    def pack(self):
+        """getInnerBoundaries for the sides that have a peer."""
+        sides = [k for k in SIDES if self.plan.peer[k] is not None]
+        _check(lib().cl_halo_pack(self._ctxp, self._ptrs(self.send, sides)),
+               lambda: lib().cl_last_error(self._ctxp))
+
+    def unpack(self):
+        """setOuterBoundaries for the sides that have a peer (the peer of a
+        side sends the strip for it)."""
+        sides = [k for k in SIDES if self.plan.peer[k] is not None]
+        _check(lib().cl_halo_unpack(self._ctxp, self._ptrs(self.recv, sides)),
+               lambda: lib().cl_last_error(self._ctxp))
+
+    def stage(self, stage, dt):
+        _check(lib().cl_solver_stage(self._s, stage, dt), self._err)
+
+    def stage_timed(self, stage, dt):
+        """The stage, waited for: (optimisation ms, flux/update ms)."""
+        ms = (C.c_float * 2)()
+        _check(lib().cl_stage_timed(self._ctxp, stage, dt, self.dx, self.dy, ms),
+               lambda: lib().cl_last_error(self._ctxp))
+        return ms[0], ms[1]
+
+    def exchange(self, group=None):
+        """The halo exchange before a stage: pack on the library's stream,
+        the point-to-point messages on the current stream, unpack on the
+        library's stream, each waiting for the previous one on the device."""
+        import torch
+        cur = torch.cuda.current_stream(self.device)
+        self.pack()
+        cur.wait_stream(self.stream)
+        exchange_distributed(self.plan, self.send, self.recv, group)
+        self.stream.wait_stream(cur)
+        self.unpack()
+
+    def sync(self):
+        _check(lib().cl_sync(self._ctxp), lambda: lib().cl_last_error(self._ctxp))
+
+    def update(self, dt, group=None):
+        """One RK2 step with the halo exchanged over torch.distributed before
+        each stage (momopt_update.cpp:311, :339)."""
+        for stage in (1, 2):
+            self.exchange(group)
+            self.stage(stage, dt)
+        self.sync()
+
+
+def update_nodes_local(nodes, dt):
+    """One RK2 step of all nodes of a partition held by this process (one
+    GPU), the halo exchanged by device copies: the partitioned run of the
+    reference on one device, for tests and for comparing partitions."""
+    import torch
+    cur = torch.cuda.current_stream()
+    plans = [s.plan for s in nodes]
+    for stage in (1, 2):
+        for s in nodes:
+            s.pack()
+            cur.wait_stream(s.stream)
+        exchange_local(plans, [s.send for s in nodes], [s.recv for s in nodes])
+        for s in nodes:
+            s.stream.wait_stream(cur)
+            s.unpack()
+            s.stage(stage, dt)
+    for s in nodes:
+        s.sync()
+
+
+def run_deck_distributed(deck_path, out_dir=".", max_steps=-1, group=None):
+    """main.cpp:45-251 on one node per torch.distributed rank (the deck's
+    NUM_MPI_PARTITIONS_X x _Y must equal the world size): outputs
+    out_<t>_<rank>.{pn,opt} at t = 0 and every OUT_DELTA_T up to T_FINAL."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    s = NodeSolver(deck_path, out_dir, node=rank, num_nodes=world)
+    t_final = s.t_final
+    t, steps = 0.0, 0
+    s.output_data(t)
+    t_out = min(t + s.out_delta_t, t_final)
+    while t_out <= t_final:
+        dt = s.max_dt
+        while t < t_out:
+            t += dt
+            if t > t_out:
+                dt = t_out - (t - dt)
+                t = t_out
+            s.update(dt, group)
+            steps += 1
+            if 0 <= max_steps <= steps:
+                s.close()
+                return
+        s.output_data(t)
+        if t_out > t_final - 1e-12 * t_final:
+            break
+        t_out = min(t_out + s.out_delta_t, t_final)
+    s.close()
 
 
 def solve_batch_noalloc(angular, options, d_u, d_alpha, count, d_iters=None, d_reg=None,

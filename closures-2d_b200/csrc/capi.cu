@@ -548,6 +548,49 @@ void cl_destroy(cl_ctx *ctx)
     delete ctx;
 }
 
+// Enqueues RK stage `stage` (0 or 1) on the context's stream: [periodic
+// ghost copy], [warm-start prediction], K1, K2+K3 (stage 1 also the Heun
+// average).  The stage's work counter must be zero when K1 starts.
+static cudaError_t enqueue_stage(cl_ctx *ctx, int stage, double dt, double dx, double dy, bool ghostCopy,
+                                 int *nk, cudaEvent_t beforeK1 = nullptr, cudaEvent_t afterK1 = nullptr)
+{
+    cudaError_t e;
+    if (ghostCopy) {
+        if ((e = launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, ctx->stream)) != cudaSuccess)
+            return e;
+        *nk += 2;
+    }
+    if (ctx->warm) {
+        if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
+            return cudaErrorLaunchFailure;
+        *nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+    }
+    NewtonArgs a = ctx->nargs;
+    a.prob[0].count = (int)ctx->C;
+    a.prob[0].u = ctx->dMom;
+    a.prob[0].alpha = ctx->dAlpha;
+    a.prob[0].queue = ctx->dQueue + stage;
+    a.prob[0].iters = ctx->dIters;
+    a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
+    a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
+    if (beforeK1 && (e = cudaEventRecord(beforeK1, ctx->stream)) != cudaSuccess)
+        return e;
+    if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
+        return e;
+    *nk += 1;
+    if (afterK1 && (e = cudaEventRecord(afterK1, ctx->stream)) != cudaSuccess)
+        return e;
+    FluxArgs f = ctx->fargs;
+    f.dt = dt;
+    f.dx = dx;
+    f.dy = dy;
+    f.momentsOld = (stage == 1) ? ctx->dOld : nullptr;
+    if ((e = launch_flux(f, ctx->stream)) != cudaSuccess)
+        return e;
+    *nk += 1;
+    return cudaSuccess;
+}
+
 // Enqueues one RK2 step on the context's stream (uncaptured form).
 static cudaError_t enqueue_step(cl_ctx *ctx, double dt, double dx, double dy, int *kernels)
 {
@@ -556,37 +599,9 @@ static cudaError_t enqueue_step(cl_ctx *ctx, double dt, double dx, double dy, in
     const bool periodic = ctx->grid.init_cond == 2;
     if ((e = cudaMemsetAsync(ctx->dQueue, 0, 2 * sizeof(unsigned), ctx->stream)) != cudaSuccess)
         return e;
-    for (int stage = 0; stage < 2; stage++) {
-        if (periodic) {
-            if ((e = launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, ctx->stream)) != cudaSuccess)
-                return e;
-            nk += 2;
-        }
-        if (ctx->warm) {
-            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
-                return cudaErrorLaunchFailure;
-            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
-        }
-        NewtonArgs a = ctx->nargs;
-        a.prob[0].count = (int)ctx->C;
-        a.prob[0].u = ctx->dMom;
-        a.prob[0].alpha = ctx->dAlpha;
-        a.prob[0].queue = ctx->dQueue + stage;
-        a.prob[0].iters = ctx->dIters;
-        a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
-        a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
-        if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
+    for (int stage = 0; stage < 2; stage++)
+        if ((e = enqueue_stage(ctx, stage, dt, dx, dy, periodic, &nk)) != cudaSuccess)
             return e;
-        nk++;
-        FluxArgs f = ctx->fargs;
-        f.dt = dt;
-        f.dx = dx;
-        f.dy = dy;
-        f.momentsOld = (stage == 1) ? ctx->dOld : nullptr;
-        if ((e = launch_flux(f, ctx->stream)) != cudaSuccess)
-            return e;
-        nk++;
-    }
     if (kernels)
         *kernels = nk;
     return cudaSuccess;
@@ -715,6 +730,84 @@ int cl_sync(cl_ctx *ctx)
         return CL_ERR_ARG;
     return read_device_error(ctx);
 }
+
+int cl_stage(cl_ctx *ctx, int stage, double dt, double dx, double dy)
+{
+    if (!ctx || (stage != 1 && stage != 2))
+        return CL_ERR_ARG;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dQueue + (stage - 1), 0, sizeof(unsigned), ctx->stream));
+    int nk = 0;
+    cudaError_t e = enqueue_stage(ctx, stage - 1, dt, dx, dy, false, &nk);
+    g_launches += nk;
+    if (e != cudaSuccess) {
+        ctx->err = std::string("stage: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return CL_OK;
+}
+
+int cl_stage_timed(cl_ctx *ctx, int stage, double dt, double dx, double dy, float *ms)
+{
+    if (!ctx || !ms || (stage != 1 && stage != 2))
+        return CL_ERR_ARG;
+    cudaEvent_t ev[3];
+    for (int i = 0; i < 3; i++)
+        CUDA_TRY(ctx, cudaEventCreate(&ev[i]));
+    cudaError_t e = cudaMemsetAsync(ctx->dQueue + (stage - 1), 0, sizeof(unsigned), ctx->stream);
+    int nk = 0;
+    if (e == cudaSuccess)
+        e = enqueue_stage(ctx, stage - 1, dt, dx, dy, false, &nk, ev[0], ev[1]);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(ev[2], ctx->stream);
+    g_launches += nk;
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) {
+        cudaEventElapsedTime(&ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[1], ev[1], ev[2]);
+    }
+    for (int i = 0; i < 3; i++)
+        cudaEventDestroy(ev[i]);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("timed stage: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return read_device_error(ctx);
+}
+
+int cl_stream(cl_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream)
+        return CL_ERR_ARG;
+    *stream = (void *)ctx->stream;
+    return CL_OK;
+}
+
+int cl_halo_counts(const cl_ctx *ctx, long long counts[4])
+{
+    if (!ctx || !counts)
+        return CL_ERR_ARG;
+    const long long nx = ctx->NX - 4, ny = ctx->NY - 4, n = ctx->n;
+    counts[CL_NORTH] = counts[CL_SOUTH] = 2 * nx * n;
+    counts[CL_EAST] = counts[CL_WEST] = 2 * ny * n;
+    return CL_OK;
+}
+
+static int halo(cl_ctx *ctx, double *const bufs[4], int pack)
+{
+    if (!ctx || !bufs)
+        return CL_ERR_ARG;
+    HaloBuffers b;
+    for (int s = 0; s < 4; s++)
+        b.p[s] = bufs[s];
+    CUDA_TRY(ctx, launch_halo(ctx->dMom, ctx->n, ctx->NX, ctx->NY, b, pack, ctx->stream));
+    g_launches += 1;
+    return CL_OK;
+}
+
+int cl_halo_pack(cl_ctx *ctx, double *const bufs[4]) { return halo(ctx, bufs, 1); }
+
+int cl_halo_unpack(cl_ctx *ctx, double *const bufs[4]) { return halo(ctx, bufs, 0); }
 
 int cl_step(cl_ctx *ctx, double dt, double dx, double dy)
 {

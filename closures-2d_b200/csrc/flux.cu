@@ -16,6 +16,8 @@
 // coordinate, and (stage 2) the average with the saved moments.
 #include "flux.cuh"
 
+#include "closures_gpu.h"
+
 namespace clb {
 
 namespace {
@@ -295,7 +297,67 @@ __global__ void ghost_periodic_y_kernel(double *m, int n, int NX, int NY)
     }
 }
 
+// Node halo (momopt_boundaries.cpp:30-188) for all four sides in one launch:
+// pack copies the inner strips of the block into bufs[side], unpack the
+// buffers into the ghost strips.  North/south: the two columns next to
+// y = max / y = min over the interior i, element (j, i - 2, k) at
+// (j * nx + i - 2) * n + k; east/west: the two rows next to x = max / x = min
+// over the interior j likewise.  Corners are not exchanged.
+__global__ void halo_kernel(double *m, int n, int NX, int NY, HaloBuffers b, int pack)
+{
+    const int nx = NX - 4, ny = NY - 4;
+    const long long cntNS = 2LL * nx * n, cntEW = 2LL * ny * n;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int side;
+    if (idx < 2 * cntNS) {
+        side = idx < cntNS ? CL_NORTH : CL_SOUTH;
+        idx -= (side == CL_SOUTH) ? cntNS : 0;
+    } else {
+        idx -= 2 * cntNS;
+        if (idx >= 2 * cntEW)
+            return;
+        side = idx < cntEW ? CL_EAST : CL_WEST;
+        idx -= (side == CL_WEST) ? cntEW : 0;
+    }
+    double *buf = b.p[side];
+    if (buf == nullptr)
+        return;
+    const int k = (int)(idx % n);
+    const long long r = idx / n;
+    int i, j;
+    if (side == CL_NORTH || side == CL_SOUTH) {
+        const int s = (int)(r / nx);
+        i = 2 + (int)(r % nx);
+        if (pack)
+            j = (side == CL_NORTH) ? NY - 4 + s : 2 + s;
+        else
+            j = (side == CL_NORTH) ? NY - 2 + s : s;
+    } else {
+        const int s = (int)(r / ny);
+        j = 2 + (int)(r % ny);
+        if (pack)
+            i = (side == CL_EAST) ? NX - 4 + s : 2 + s;
+        else
+            i = (side == CL_EAST) ? NX - 2 + s : s;
+    }
+    double *cell = m + ((size_t)i * NY + j) * n + k;
+    if (pack)
+        buf[idx] = *cell;
+    else
+        *cell = buf[idx];
+}
+
 }  // namespace
+
+cudaError_t launch_halo(double *moments, int n, int NX, int NY, const HaloBuffers &b, int pack,
+                        cudaStream_t stream)
+{
+    const long long total = 4LL * (NX - 4) * n + 4LL * (NY - 4) * n;
+    if (total <= 0)
+        return cudaSuccess;
+    halo_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(moments, n, NX, NY, b, pack);
+    return cudaGetLastError();
+}
 
 int plan_flux(FluxArgs &f)
 {

@@ -33,5 +33,12 @@ cudaError_t prepare_flux(const FluxArgs &f);
 cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream);
 // duplicateBoundaries (momopt_boundaries.cpp:190-223) on device moments.
 cudaError_t launch_ghost_periodic(double *moments, int n, int NX, int NY, cudaStream_t stream);
+// Halo strips of a node's block: pack (1) the inner strips into p[side] or
+// unpack (0) p[side] into the ghost strips; null sides are skipped.
+struct HaloBuffers {
+    double *p[4];
+};
+cudaError_t launch_halo(double *moments, int n, int NX, int NY, const HaloBuffers &b, int pack,
+                        cudaStream_t stream);
 
 }  // namespace clb

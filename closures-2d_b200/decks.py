@@ -17,15 +17,15 @@ def deck_text(solver="momopt", num_cells_x=50, num_cells_y=50, a_x=-1.5, b_x=1.5
               floor=1e-4, init_cond="gaussian", sigma=1.0, moment_order=3, quad_order=30,
               cfl_factor=0.9, tol=1e-4, cond_h_max=1e10, cond_h_max_bfgs=20, max_iter=100,
               max_bfgs_iter=5, use_gaunt=1, theta=2.0, delta_ppn=1e-10, moment_type="mn",
-              opt_type=0, extra=None):
+              opt_type=0, partitions=(1, 1), extra=None):
     ic = INIT_CONDS[init_cond] if isinstance(init_cond, str) else int(init_cond)
     mt = MOMENT_TYPES[moment_type] if isinstance(moment_type, str) else int(moment_type)
     lines = [
         "SOLVER %s" % solver,
         "NUM_CELLS_X %d" % num_cells_x,
         "NUM_CELLS_Y %d" % num_cells_y,
-        "NUM_MPI_PARTITIONS_X 1",
-        "NUM_MPI_PARTITIONS_Y 1",
+        "NUM_MPI_PARTITIONS_X %d" % partitions[0],
+        "NUM_MPI_PARTITIONS_Y %d" % partitions[1],
         "A_X %.17f" % a_x,
         "B_X %.17f" % b_x,
         "A_Y %.17f" % a_y,

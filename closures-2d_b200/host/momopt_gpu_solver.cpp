@@ -352,9 +352,50 @@ void MomOptGpuSolver::duplicateBoundaries()
         fail(cl_last_error(m_ctx));
 }
 
-// Deck keys of main.cpp:69-83 into a solver (one node).
+// main.cpp:157-193: the block of `node` in the nodesX x nodesY partition.
+static int partition(int numCellsX, int numCellsY, int nodesX, int nodesY, int numNodes, int node, double ax,
+              double ay, double bx, double by, cl_node &out, std::string &err)
+{
+    if (nodesX < 1 || nodesY < 1 || numCellsX < nodesX || numCellsY < nodesY) {
+        err = "Init: Number of partitions larger than number of cells.";
+        return CL_ERR_ARG;
+    }
+    if (nodesX * nodesY != numNodes) {
+        err = "Init: Number of Nodes != numPartitionsX * numPartitionsY.";
+        return CL_ERR_ARG;
+    }
+    if (node < 0 || node >= numNodes) {
+        err = "Init: node index out of range.";
+        return CL_ERR_ARG;
+    }
+    const double dx = (bx - ax) / numCellsX, dy = (by - ay) / numCellsY;
+    out.node = node;
+    out.nodes_x = nodesX;
+    out.nodes_y = nodesY;
+    out.node_x = node / nodesY;
+    out.node_y = node % nodesY;
+    out.size_x = numCellsX / nodesX;
+    if (out.node_x < numCellsX % nodesX) {
+        out.size_x++;
+        out.init_x = ax + dx * out.size_x * out.node_x;
+    } else {
+        out.init_x = bx - dx * out.size_x * (nodesX - out.node_x);
+    }
+    out.size_y = numCellsY / nodesY;
+    if (out.node_y < numCellsY % nodesY) {
+        out.size_y++;
+        out.init_y = ay + dy * out.size_y * out.node_y;
+    } else {
+        out.init_y = by - dy * out.size_y * (nodesY - out.node_y);
+    }
+    return CL_OK;
+}
+
+// Deck keys of main.cpp:69-83 into a solver: one node (numNodes 1, the
+// partition keys are read but unused, as in the build without MPI) or node
+// `node` of the deck's NUM_MPI_PARTITIONS_X x _Y partition.
 static int setup_from_deck(MomOptGpuSolver &s, const char *deckPath, double &dx, double &dy, double &tFinal,
-                           double &outDeltaT, std::string &err)
+                           double &outDeltaT, std::string &err, int node = 0, int numNodes = 1)
 {
     InputDeck deck;
     if (!deck.read(deckPath)) {
@@ -392,6 +433,22 @@ static int setup_from_deck(MomOptGpuSolver &s, const char *deckPath, double &dx,
     s.c_by = by;
     s.c_initX = ax;
     s.c_initY = ay;
+    if (numNodes > 1 || node != 0) {
+        cl_node part;
+        int rc = partition(numCellsX, numCellsY, nodesX, nodesY, numNodes, node, ax, ay, bx, by, part, err);
+        if (rc)
+            return rc;
+        s.c_node = node;
+        s.c_numNodes = numNodes;
+        s.c_nodeX = part.node_x;
+        s.c_nodeY = part.node_y;
+        s.c_numNodesX = nodesX;
+        s.c_numNodesY = nodesY;
+        s.c_sizeX = part.size_x;
+        s.c_sizeY = part.size_y;
+        s.c_initX = part.init_x;
+        s.c_initY = part.init_y;
+    }
     s.initializeGrid(s.getNumGhostCells(), dx, dy, sigma);
     return CL_OK;
 }
@@ -475,6 +532,69 @@ int cl_solver_create(const char *deck_path, const char *out_dir, cl_solver **out
         *max_dt = h->maxDt;
     *out = h;
     return CL_OK;
+}
+
+int cl_partition(int num_cells_x, int num_cells_y, int nodes_x, int nodes_y, int num_nodes, int node, double ax,
+                 double ay, double bx, double by, cl_node *out)
+{
+    if (!out)
+        return CL_ERR_ARG;
+    std::string err;
+    int rc = clb::partition(num_cells_x, num_cells_y, nodes_x, nodes_y, num_nodes, node, ax, ay, bx, by, *out, err);
+    if (rc)
+        clb_set_global_error(err.c_str());
+    return rc;
+}
+
+int cl_solver_create_node(const char *deck_path, const char *out_dir, int node, int num_nodes, cl_solver **out,
+                          double *max_dt)
+{
+    if (!deck_path || !out || num_nodes < 1)
+        return CL_ERR_ARG;
+    *out = nullptr;
+    cl_solver *h = new cl_solver();
+    h->s.outDir = out_dir ? out_dir : ".";
+    std::string err;
+    int rc = clb::setup_from_deck(h->s, deck_path, h->dx, h->dy, h->tFinal, h->outDeltaT, err, node, num_nodes);
+    if (rc == CL_OK) {
+        rc = h->s.tryInit(h->dx, h->dy, &h->maxDt);
+        err = h->s.lastError;
+    }
+    if (rc != CL_OK) {
+        clb_set_global_error(err.c_str());
+        delete h;
+        return rc;
+    }
+    if (max_dt)
+        *max_dt = h->maxDt;
+    *out = h;
+    return CL_OK;
+}
+
+int cl_solver_node(const cl_solver *h, cl_node *out)
+{
+    if (!h || !out)
+        return CL_ERR_ARG;
+    out->node = h->s.c_node;
+    out->nodes_x = h->s.c_numNodesX;
+    out->nodes_y = h->s.c_numNodesY;
+    out->node_x = h->s.c_nodeX;
+    out->node_y = h->s.c_nodeY;
+    out->size_x = h->s.c_sizeX;
+    out->size_y = h->s.c_sizeY;
+    out->init_x = h->s.c_initX;
+    out->init_y = h->s.c_initY;
+    return CL_OK;
+}
+
+int cl_solver_stage(cl_solver *h, int stage, double dt)
+{
+    if (!h)
+        return CL_ERR_ARG;
+    int rc = cl_stage(h->s.context(), stage, dt, h->dx, h->dy);
+    if (rc)
+        h->err = cl_last_error(h->s.context());
+    return rc;
 }
 
 int cl_solver_geometry(cl_solver *h, int *nx, int *ny, int *n, double *dx, double *dy, double *t_final,

@@ -137,6 +137,36 @@ int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms);
 int cl_step_async(cl_ctx *ctx, double dt, double dx, double dy);
 int cl_sync(cl_ctx *ctx);
 
+/* One RK stage of the step (stage 1 or 2, in that order; momopt_update.cpp
+ * :311-336 and :339-377): optimisation of every cell, flux and the Euler,
+ * collision and source update of the interior, stage 2 also the Heun
+ * average.  No ghost copy: a node of a partitioned grid fills its ghost
+ * strips from its neighbours (cl_halo_*) before each stage, as
+ * communicateBoundaries does (comm.cpp:31-147).  Asynchronous on the
+ * context's stream; errors surface at the next cl_sync(). */
+int cl_stage(cl_ctx *ctx, int stage, double dt, double dx, double dy);
+/* Same stage, waited for, with the durations of its optimisation kernel
+ * (ms[0]) and flux/update kernel (ms[1]) from CUDA events on the context's
+ * stream; reports a device-side error like cl_step. */
+int cl_stage_timed(cl_ctx *ctx, int stage, double dt, double dx, double dy, float *ms);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work (the halo exchange) with the library's. */
+int cl_stream(cl_ctx *ctx, void **stream);
+
+/* Halo of a node's block (momopt_boundaries.cpp:17-188).  Sides: */
+enum { CL_NORTH = 0, CL_SOUTH = 1, CL_EAST = 2, CL_WEST = 3 };
+/* Doubles per side: north/south 2 * nx * n (the two columns next to the
+ * largest / least y over the interior x), east/west 2 * ny * n (the two rows
+ * next to the largest / least x over the interior y); corners are not
+ * exchanged.  Buffer order [strip][cell][k] as getInnerBoundaries packs. */
+int cl_halo_counts(const cl_ctx *ctx, long long counts[4]);
+/* getInnerBoundaries: the inner strips into the device buffers bufs[side]
+ * (null entries skipped), on the context's stream. */
+int cl_halo_pack(cl_ctx *ctx, double *const bufs[4]);
+/* setOuterBoundaries: the device buffers into the ghost strips (null
+ * entries skipped), on the context's stream. */
+int cl_halo_unpack(cl_ctx *ctx, double *const bufs[4]);
+
 /* Copies the full state (all cells, ghosts included) to / from the host. */
 int cl_get_state(cl_ctx *ctx, double *moments, double *alpha);
 int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha);
@@ -209,6 +239,28 @@ int cl_solver_output(cl_solver *s, double time);        /* Solver::outputData */
 cl_ctx *cl_solver_context(cl_solver *s);
 const char *cl_solver_last_error(const cl_solver *s);
 void cl_solver_destroy(cl_solver *s);
+/* A node of the block partition of main.cpp:157-193 (the MPI build): the
+ * grid of num_cells_x x num_cells_y cells on [ax,bx] x [ay,by] split into
+ * nodes_x x nodes_y blocks, node = node_x * nodes_y + node_y. */
+typedef struct {
+    int node, nodes_x, nodes_y, node_x, node_y;
+    int size_x, size_y;     /* interior cells of the node (c_sizeX, c_sizeY) */
+    double init_x, init_y;  /* c_initX, c_initY: least x, y of its interior */
+} cl_node;
+/* Fails with CL_ERR_ARG as main.cpp:160-169 aborts: more partitions than
+ * cells, or num_nodes != nodes_x * nodes_y. */
+int cl_partition(int num_cells_x, int num_cells_y, int nodes_x, int nodes_y, int num_nodes, int node,
+                 double ax, double ay, double bx, double by, cl_node *out);
+/* The solver of one node of the deck's NUM_MPI_PARTITIONS_X x _Y partition
+ * (num_nodes processes, this one `node`): its block, initial condition and
+ * output files out_<t>_<node>.{pn,opt} as the reference's MPI build writes
+ * them.  A node steps with cl_solver_stage after filling its halo. */
+int cl_solver_create_node(const char *deck_path, const char *out_dir, int node, int num_nodes,
+                          cl_solver **out, double *max_dt);
+int cl_solver_node(const cl_solver *s, cl_node *out);
+/* cl_stage on the solver's context with its dx, dy (stage 1 or 2). */
+int cl_solver_stage(cl_solver *s, int stage, double dt);
+
 /* main.cpp:204-230: outputs at t = 0 and every OUT_DELTA_T up to T_FINAL;
  * max_steps >= 0 stops after that many RK2 steps. */
 int cl_run_deck(const char *deck_path, const char *out_dir, int max_steps);

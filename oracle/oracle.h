@@ -131,6 +131,7 @@ typedef struct {
     double ax, ay, bx, by, tFinal, outDeltaT, gaussianSigma, floor_, sigma;
     int initCond;
     /* momopt deck (momopt_init.cpp:56-68) */
+    int nodesX, nodesY;     /* NUM_MPI_PARTITIONS_X, _Y */
     int momentOrder, quadOrder, useGaunt, momentType, optType, maxIter, maxBfgsIter;
     double cflFactor, tol, condHMax, condHMaxBfgs, theta, deltaPPn;
     double tolGamma;        /* optional key MOMOPT_TOL_GAMMA, default 0 (off) */
@@ -146,6 +147,10 @@ typedef struct {
 typedef struct {
     orc_deck deck;
     orc_setup set;
+    /* this process's block of the partition (main.cpp:157-193; node 0 of
+     * 1 x 1 without MPI) */
+    int node, numNodes, nodeX, nodeY, numNodesX, numNodesY;
+    double initX, initY;
     int gX[4], gY[4];
     int NX, NY;             /* with ghosts */
     double dx, dy, maxDt;
@@ -161,6 +166,19 @@ typedef struct {
 /* Deck parsing with the reference's semantics (input_deck_reader.cpp). */
 int orc_deck_read(const char *path, orc_deck *d);
 int orc_solver_create(const orc_deck *d, orc_solver *s);
+/* node of the deck's NUM_MPI_PARTITIONS_X x _Y partition on numNodes nodes */
+int orc_solver_create_node(const orc_deck *d, int node, int numNodes, orc_solver *s);
+/* The stages of update() for a node whose ghosts a halo exchange fills
+ * (comm.cpp:31-147 in place of the periodic copy): save the interior,
+ * one stage without the ghost copy, the Heun average. */
+void orc_solver_save_old(orc_solver *s);
+int orc_solver_stage_exchanged(orc_solver *s, double dt);
+void orc_solver_average(orc_solver *s);
+/* momopt_boundaries.cpp:17-188: doubles per side (north, south, east,
+ * west), and the inner strips packed into / the ghost strips unpacked from
+ * buf. */
+long long orc_solver_halo_count(const orc_solver *s, int side);
+void orc_solver_halo(orc_solver *s, int side, int pack, double *buf);
 void orc_solver_free(orc_solver *s);
 /* One RK2 step, momopt_update.cpp:283-382.  Returns the status. */
 int orc_solver_update(orc_solver *s, double dt);

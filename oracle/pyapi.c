@@ -96,19 +96,42 @@ int orc_setup_copy(int order, int Q, int useGaunt, double *w, double *xi, double
     return 0;
 }
 
-/* Whole-grid solver handle. */
-void *orc_solver_open(const char *deckPath)
+/* Whole-grid solver handle (one node), or node `node` of numNodes. */
+void *orc_solver_open_node(const char *deckPath, int node, int numNodes)
 {
     orc_deck d;
     if (orc_deck_read(deckPath, &d))
         return NULL;
     orc_solver *s = (orc_solver *)malloc(sizeof(orc_solver));
-    if (orc_solver_create(&d, s)) {
+    if (orc_solver_create_node(&d, node, numNodes, s)) {
         free(s);
         return NULL;
     }
     return s;
 }
+
+void *orc_solver_open(const char *deckPath) { return orc_solver_open_node(deckPath, 0, 1); }
+
+void orc_solver_node_info(void *h, int *info, double *origin)
+{
+    orc_solver *s = (orc_solver *)h;
+    info[0] = s->node;
+    info[1] = s->numNodesX;
+    info[2] = s->numNodesY;
+    info[3] = s->nodeX;
+    info[4] = s->nodeY;
+    info[5] = s->gX[2] - s->gX[1] + 1;
+    info[6] = s->gY[2] - s->gY[1] + 1;
+    origin[0] = s->initX;
+    origin[1] = s->initY;
+}
+
+void orc_solver_save_old_h(void *h) { orc_solver_save_old((orc_solver *)h); }
+int orc_solver_stage_exchanged_h(void *h, double dt) { return orc_solver_stage_exchanged((orc_solver *)h, dt); }
+void orc_solver_average_h(void *h) { orc_solver_average((orc_solver *)h); }
+long long orc_solver_halo_count_h(void *h, int side) { return orc_solver_halo_count((orc_solver *)h, side); }
+void orc_solver_halo_h(void *h, int side, int pack, double *buf) { orc_solver_halo((orc_solver *)h, side, pack, buf); }
+int orc_solver_output_h(void *h, double time, const char *dir) { return orc_solver_output((orc_solver *)h, time, dir); }
 
 void orc_solver_dims(void *h, int *NX, int *NY, int *n, double *maxDt, double *dx, double *dy)
 {

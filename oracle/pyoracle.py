@@ -53,6 +53,16 @@ def _bind(L):
         L.orc_setup_copy.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, ip, ip, dp]
         L.orc_solver_open.restype = vp
         L.orc_solver_open.argtypes = [C.c_char_p]
+        L.orc_solver_open_node.restype = vp
+        L.orc_solver_open_node.argtypes = [C.c_char_p, C.c_int, C.c_int]
+        L.orc_solver_node_info.argtypes = [vp, ip, dp]
+        L.orc_solver_save_old_h.argtypes = [vp]
+        L.orc_solver_stage_exchanged_h.argtypes = [vp, C.c_double]
+        L.orc_solver_average_h.argtypes = [vp]
+        L.orc_solver_halo_count_h.argtypes = [vp, C.c_int]
+        L.orc_solver_halo_count_h.restype = C.c_longlong
+        L.orc_solver_halo_h.argtypes = [vp, C.c_int, C.c_int, dp]
+        L.orc_solver_output_h.argtypes = [vp, C.c_double, C.c_char_p]
         L.orc_solver_dims.argtypes = [vp, ip, ip, ip, dp, dp, dp]
         L.orc_solver_steps.argtypes = [vp, C.c_int]
         L.orc_solver_step_dt.argtypes = [vp, C.c_double]
@@ -132,9 +142,12 @@ def optcb_batch(order, Q, u, P2M, alphaP, alpha, moment_type=0, max_iter=100, to
 
 
 class GridSolver:
-    def __init__(self, deck_path, fma=False):
+    """The oracle's solver of a deck: the whole grid (one node), or node
+    `node` of the deck's NUM_MPI_PARTITIONS_X x _Y partition on num_nodes."""
+
+    def __init__(self, deck_path, fma=False, node=0, num_nodes=1):
         self.L = lib(fma)
-        self.h = self.L.orc_solver_open(deck_path.encode())
+        self.h = self.L.orc_solver_open_node(deck_path.encode(), node, num_nodes)
         assert self.h, "oracle rejected the deck"
         NX, NY, n = C.c_int(), C.c_int(), C.c_int()
         md, dx, dy = C.c_double(), C.c_double(), C.c_double()
@@ -157,6 +170,42 @@ class GridSolver:
         m = np.ascontiguousarray(m, dtype=np.float64)
         a = np.ascontiguousarray(a, dtype=np.float64)
         self.L.orc_solver_set_state(self.h, _dp(m), _dp(a))
+
+    def node_info(self):
+        info = np.zeros(7, np.int32)
+        origin = np.zeros(2)
+        self.L.orc_solver_node_info(self.h, _ip(info), _dp(origin))
+        keys = ("node", "nodes_x", "nodes_y", "node_x", "node_y", "size_x", "size_y")
+        d = dict(zip(keys, info.tolist()))
+        d["init_x"], d["init_y"] = origin.tolist()
+        return d
+
+    # a node's RK2 step with the halo exchanged between the stages
+    def save_old(self):
+        self.L.orc_solver_save_old_h(self.h)
+
+    def stage_exchanged(self, dt):
+        st = self.L.orc_solver_stage_exchanged_h(self.h, dt)
+        assert st == 0, "oracle error %d" % st
+
+    def average(self):
+        self.L.orc_solver_average_h(self.h)
+
+    def halo_counts(self):
+        return [self.L.orc_solver_halo_count_h(self.h, side) for side in range(4)]
+
+    def halo_pack(self, side):
+        buf = np.empty(self.L.orc_solver_halo_count_h(self.h, side))
+        self.L.orc_solver_halo_h(self.h, side, 1, _dp(buf))
+        return buf
+
+    def halo_unpack(self, side, buf):
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        self.L.orc_solver_halo_h(self.h, side, 0, _dp(buf))
+
+    def output(self, time, out_dir):
+        st = self.L.orc_solver_output_h(self.h, time, out_dir.encode())
+        assert st == 0, "oracle output error %d" % st
 
     def last_iterations(self):
         it = np.empty(self.NX * self.NY, np.int32)

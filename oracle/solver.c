@@ -134,6 +134,8 @@ int orc_deck_read(const char *path, orc_deck *d)
     ok &= kv_dbl(&l, "FLOOR", &d->floor_);
     ok &= kv_int(&l, "INIT_COND", &d->initCond);
     ok &= kv_dbl(&l, "SIGMA", &d->sigma);
+    ok &= kv_int(&l, "NUM_MPI_PARTITIONS_X", &d->nodesX);
+    ok &= kv_int(&l, "NUM_MPI_PARTITIONS_Y", &d->nodesY);
     ok &= kv_int(&l, "MOMOPT_MOMENT_ORDER", &d->momentOrder);
     ok &= kv_int(&l, "MOMOPT_QUAD_ORDER", &d->quadOrder);
     ok &= kv_dbl(&l, "MOMOPT_CFL_FACTOR", &d->cflFactor);
@@ -159,7 +161,9 @@ int orc_deck_read(const char *path, orc_deck *d)
 #define I2D(i, j) ((i) * s->NY + (j))
 #define I3D(i, j, k) (((size_t)(i) * s->NY + (j)) * n + (k))
 
-int orc_solver_create(const orc_deck *d, orc_solver *s)
+int orc_solver_create(const orc_deck *d, orc_solver *s) { return orc_solver_create_node(d, 0, 1, s); }
+
+int orc_solver_create_node(const orc_deck *d, int node, int numNodes, orc_solver *s)
 {
     memset(s, 0, sizeof(*s));
     s->deck = *d;
@@ -171,6 +175,38 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
     s->dy = (d->by - d->ay) / sizeY;
     double dx = s->dx, dy = s->dy;
     double initX = d->ax, initY = d->ay;
+    s->node = 0;
+    s->numNodes = 1;
+    s->numNodesX = s->numNodesY = 1;
+    if (numNodes > 1) {
+        /* main.cpp:157-193 */
+        const int nX = d->nodesX, nY = d->nodesY;
+        if (nX < 1 || nY < 1 || d->numCellsX < nX || d->numCellsY < nY || nX * nY != numNodes || node < 0 ||
+            node >= numNodes)
+            return ORC_ERR_INPUT;
+        s->node = node;
+        s->numNodes = numNodes;
+        s->numNodesX = nX;
+        s->numNodesY = nY;
+        s->nodeX = node / nY;
+        s->nodeY = node % nY;
+        sizeX = d->numCellsX / nX;
+        if (s->nodeX < d->numCellsX % nX) {
+            sizeX++;
+            initX = d->ax + dx * sizeX * s->nodeX;
+        } else {
+            initX = d->bx - dx * sizeX * (nX - s->nodeX);
+        }
+        sizeY = d->numCellsY / nY;
+        if (s->nodeY < d->numCellsY % nY) {
+            sizeY++;
+            initY = d->ay + dy * sizeY * s->nodeY;
+        } else {
+            initY = d->by - dy * sizeY * (nY - s->nodeY);
+        }
+    }
+    s->initX = initX;
+    s->initY = initY;
     /* main.cpp:261-269 */
     s->gX[0] = 0;
     s->gX[1] = ng;
@@ -197,9 +233,15 @@ int orc_solver_create(const orc_deck *d, orc_solver *s)
                 s->sigmaS[I2D(i, j)] = d->sigma;
             } else if (d->initCond == 0 && d->gaussianSigma == 0.0) {
                 s->initialGrid[I2D(i, j)] = d->floor_;
-                /* single node: nodeX == (1-1)/2 == 0, numNodes odd */
-                if (i == (sizeX + ng) / 2 && j == (sizeY + ng) / 2)
-                    s->initialGrid[I2D(i, j)] = 1.0 / (dx * dy);
+                /* the node at the centre of the partition holds the delta */
+                if (s->nodeX == (s->numNodesX - 1) / 2 && s->nodeY == (s->numNodesY - 1) / 2) {
+                    int hitX = (s->numNodesX % 2 != 0 && i == (sizeX + ng) / 2) ||
+                               (s->numNodesX % 2 == 0 && i == s->gX[2]);
+                    int hitY = (s->numNodesY % 2 != 0 && j == (sizeY + ng) / 2) ||
+                               (s->numNodesY % 2 == 0 && j == s->gY[2]);
+                    if (hitX && hitY)
+                        s->initialGrid[I2D(i, j)] = 1.0 / (dx * dy);
+                }
                 s->sigmaT[I2D(i, j)] = d->sigma;
                 s->sigmaS[I2D(i, j)] = d->sigma;
             } else if (d->initCond == 0) {
@@ -456,8 +498,8 @@ static void euler_collide(orc_solver *s, double dt, double dx, double dy)
                     s->moments[I3D(i, j, k)] * (1.0 - dt * s->sigmaT[I2D(i, j)]) -
                     dt * s->flux[I3D(i, j, k)];
             if (s->deck.initCond == 1) {
-                double x_i = s->deck.ax + (i - s->gX[1]) * dx;
-                double y_j = s->deck.ay + (j - s->gY[1]) * dy;
+                double x_i = s->initX + (i - s->gX[1]) * dx;
+                double y_j = s->initY + (j - s->gY[1]) * dy;
                 if (fabs(x_i) < 0.5 && fabs(y_j) < 0.5)
                     s->moments[I3D(i, j, 0)] = s->moments[I3D(i, j, 0)] + dt * 2.0 * sqrt(M_PI);
             }
@@ -494,7 +536,7 @@ int orc_solver_output(orc_solver *s, double time, const char *dir)
 {
     char fn[1024];
     int n = s->set.n;
-    snprintf(fn, sizeof(fn), "%s/out_%.3f_%d.pn", dir ? dir : ".", time, 0);
+    snprintf(fn, sizeof(fn), "%s/out_%.3f_%d.pn", dir ? dir : ".", time, s->node);
     FILE *f = fopen(fn, "wb");
     if (!f)
         return ORC_ERR_INPUT;
@@ -512,7 +554,7 @@ int orc_solver_output(orc_solver *s, double time, const char *dir)
         for (int j = s->gY[1]; j <= s->gY[2]; j++)
             fwrite(&s->moments[I3D(i, j, 0)], sizeof(double), n, f);
     fclose(f);
-    snprintf(fn, sizeof(fn), "%s/out_%.3f_%d.opt", dir ? dir : ".", time, 0);
+    snprintf(fn, sizeof(fn), "%s/out_%.3f_%d.opt", dir ? dir : ".", time, s->node);
     f = fopen(fn, "w");
     if (!f)
         return ORC_ERR_INPUT;
@@ -572,4 +614,76 @@ int orc_solver_stage(orc_solver *s, double dt)
     solve_flux(s, s->dx, s->dy);
     euler_collide(s, dt, s->dx, s->dy);
     return ORC_OK;
+}
+
+/* ---------------- a node of a partitioned grid ---------------- */
+
+/* momopt_update.cpp:299-308 */
+void orc_solver_save_old(orc_solver *s)
+{
+    int n = s->set.n;
+    for (int i = s->gX[1]; i <= s->gX[2]; i++)
+        for (int j = s->gY[1]; j <= s->gY[2]; j++)
+            for (int k = 0; k < n; k++)
+                s->momentsOld[I3D(i, j, k)] = s->moments[I3D(i, j, k)];
+}
+
+/* momopt_update.cpp:311-336 with the ghosts already exchanged */
+int orc_solver_stage_exchanged(orc_solver *s, double dt)
+{
+    solve_optimization(s);
+    if (s->status != ORC_OK)
+        return s->status;
+    solve_flux(s, s->dx, s->dy);
+    euler_collide(s, dt, s->dx, s->dy);
+    return ORC_OK;
+}
+
+/* momopt_update.cpp:367-377 */
+void orc_solver_average(orc_solver *s)
+{
+    int n = s->set.n;
+    for (int i = s->gX[1]; i <= s->gX[2]; i++)
+        for (int j = s->gY[1]; j <= s->gY[2]; j++)
+            for (int k = 0; k < n; k++)
+                s->moments[I3D(i, j, k)] = 0.5 * (s->moments[I3D(i, j, k)] + s->momentsOld[I3D(i, j, k)]);
+}
+
+/* momopt_boundaries.cpp:17-27 (the used part of the buffers) */
+long long orc_solver_halo_count(const orc_solver *s, int side)
+{
+    long long sx = s->gX[2] - s->gX[1] + 1, sy = s->gY[2] - s->gY[1] + 1;
+    return 2LL * (side < 2 ? sx : sy) * s->set.n;
+}
+
+/* momopt_boundaries.cpp:30-188; side 0 north, 1 south, 2 east, 3 west */
+void orc_solver_halo(orc_solver *s, int side, int pack, double *buf)
+{
+    int n = s->set.n;
+    const int sx = s->gX[2] - s->gX[1] + 1, sy = s->gY[2] - s->gY[1] + 1;
+    for (int g = 0; g < 2; g++) {
+        if (side < 2) {
+            int j = pack ? (side == 0 ? s->gY[2] + 1 - 2 + g : s->gY[1] + g)
+                         : (side == 0 ? s->gY[2] + 1 + g : s->gY[0] + g);
+            for (int i = s->gX[1]; i <= s->gX[2]; i++) {
+                double *b = buf + ((size_t)(i - s->gX[1]) + (size_t)g * sx) * n;
+                double *m = &s->moments[I3D(i, j, 0)];
+                if (pack)
+                    memcpy(b, m, sizeof(double) * n);
+                else
+                    memcpy(m, b, sizeof(double) * n);
+            }
+        } else {
+            int i = pack ? (side == 2 ? s->gX[2] + 1 - 2 + g : s->gX[1] + g)
+                         : (side == 2 ? s->gX[2] + 1 + g : s->gX[0] + g);
+            for (int j = s->gY[1]; j <= s->gY[2]; j++) {
+                double *b = buf + ((size_t)(j - s->gY[1]) + (size_t)g * sy) * n;
+                double *m = &s->moments[I3D(i, j, 0)];
+                if (pack)
+                    memcpy(b, m, sizeof(double) * n);
+                else
+                    memcpy(m, b, sizeof(double) * n);
+            }
+        }
+    }
 }
