@@ -304,7 +304,8 @@ def native_arm(args, world, rank, local):
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
     deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world)
-    if world > 1:
+    partitioned = world > 1 or args.partitioned
+    if partitioned:
         solver = cb.NodeSolver(deck, tmp, node=rank, num_nodes=world)
     else:
         solver = cb.Solver(deck, tmp)
@@ -351,7 +352,7 @@ def native_arm(args, world, rank, local):
     kernel_ms = np.zeros(4)
     exchange_ms = 0.0
     for _ in range(args.steps):
-        if world > 1:
+        if partitioned:
             for stage in (1, 2):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
@@ -456,7 +457,7 @@ def native_arm(args, world, rank, local):
                        "t_start": args.warmup * dt,
                        "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
                        "parallelism": ("halo %dx1 (NCCL point-to-point before each RK stage)" % world)
-                       if world > 1 else "single"},
+                       if partitioned else "single"},
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
             "fallback_restarts": st1["fallbacks"] - st0["fallbacks"],
             "nn": nn_info,
@@ -656,6 +657,9 @@ def main():
     ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1, 2],
                     help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton, "
                          "2: BFGS sub-iterations in the change of basis)")
+    ap.add_argument("--partitioned", action="store_true",
+                    help="grid workloads: step through the partitioned (halo-exchange) path even "
+                         "on one GPU, as a 1 x 1 partition")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="grid workloads: Hessian-only tiles in split TF32 (MOMOPT_GPU_PRECISION mixed)")
     args = ap.parse_args()
