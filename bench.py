@@ -301,6 +301,9 @@ def native_arm(args, world, rank, local):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+        # a collective of all ranks first: the halo's point-to-point batches
+        # then start on an initialised communicator
+        dist.barrier()
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
     deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world)
@@ -403,15 +406,20 @@ def native_arm(args, world, rank, local):
     hm2, ha2 = ctx.get_state()
     hm[:] = hm2.reshape(C, n)
     ha[:] = ha2.reshape(C, n)
+    lib = cb.lib()
+    parts = np.zeros(3)
     barrier()
     t1 = time.perf_counter()
     for _ in range(e2e_steps):
+        ta = time.perf_counter()
         ctx.set_state(hm, ha)
+        tb = time.perf_counter()
         solver.update(dt)
-        lib = cb.lib()
+        tc = time.perf_counter()
         rc = lib.cl_get_state(ctx._ctx, cb._dp(hm), cb._dp(ha))
         if rc:
             raise cb.ClosuresError(rc, lib.cl_last_error(ctx._ctx))
+        parts += (tb - ta, tc - tb, time.perf_counter() - tc)
     barrier()
     e2e_s = time.perf_counter() - t1
     if world > 1:
@@ -474,7 +482,8 @@ def native_arm(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-solves/s",
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
-                    "steps": e2e_steps},
+                    "steps": e2e_steps,
+                    "ms_per_step": dict(zip(("h2d", "step", "d2h"), (1e3 * parts / e2e_steps).tolist()))},
             "gpu_launches": int(launches),
             "clocks": clocks,
             "wall_s": wall,

@@ -654,6 +654,8 @@ def run_deck_distributed(deck_path, out_dir=".", max_steps=-1, group=None):
     import torch.distributed as dist
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     s = NodeSolver(deck_path, out_dir, node=rank, num_nodes=world)
+    if world > 1:
+        dist.barrier(group)   # every rank set up before the first halo batch
     t_final = s.t_final
     t, steps = 0.0, 0
     s.output_data(t)

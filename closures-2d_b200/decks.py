@@ -55,6 +55,37 @@ def deck_text(solver="momopt", num_cells_x=50, num_cells_y=50, a_x=-1.5, b_x=1.5
     return "\n".join(lines) + "\n"
 
 
+FILTER_TYPES = {"none": 0, "hauck": 1, "sspline": 2, "lanczos": 3}
+
+
+def moment_deck_text(moment_order=3, quad_order=30, filter_type="none", filter_tune=100,
+                     cfl_factor=0.9, **grid):
+    """A deck for SOLVER moment (the linear Pn/FPn solver): the grid keys of
+    deck_text and the MOMENT_* keys of moment_init.cpp:57-61 (util/decks.py
+    writes the same five)."""
+    ft = FILTER_TYPES[filter_type] if isinstance(filter_type, str) else int(filter_type)
+    base = deck_text(solver="moment", **grid)
+    lines = [l for l in base.splitlines() if not l.startswith("MOMOPT_")]
+    lines += [
+        "MOMENT_MOMENT_ORDER %d" % moment_order,
+        "MOMENT_QUAD_ORDER %d" % quad_order,
+        "MOMENT_FILTER_TYPE %d" % ft,
+        "MOMENT_FILTER_TUNE %d" % filter_tune,
+        "MOMENT_CFL_FACTOR %.17f" % cfl_factor,
+    ]
+    return "\n".join(lines) + "\n"
+
+
+def regression_moment_deck(init_cond, filter_type, **kw):
+    """The deck the reference's regression harness runs for one moment-solver
+    golden (site_scons/testing.py:109-160, 252-276)."""
+    args = dict(num_cells_x=36, num_cells_y=74, a_x=-1.55, b_x=1.45, a_y=-1.62, b_y=1.38,
+                t_final=1.03, sigma=1.111, init_cond=init_cond,
+                gaussian_sigma=0.0 if init_cond == "delta" else 1.7, filter_type=filter_type)
+    args.update(kw)
+    return moment_deck_text(**args)
+
+
 def regression_deck(init_cond, moment_type, **kw):
     """The deck the reference's regression harness runs for one momopt golden."""
     args = dict(num_cells_x=36, num_cells_y=74, a_x=-1.55, b_x=1.45, a_y=-1.62, b_y=1.38,

@@ -135,6 +135,10 @@ typedef struct {
     int momentOrder, quadOrder, useGaunt, momentType, optType, maxIter, maxBfgsIter;
     double cflFactor, tol, condHMax, condHMaxBfgs, theta, deltaPPn;
     double tolGamma;        /* optional key MOMOPT_TOL_GAMMA, default 0 (off) */
+    /* SOLVER moment (the linear Pn/FPn solver, moment_init.cpp:53-61) */
+    int isMoment;
+    int pnOrder, pnQuadOrder, pnFilterType;
+    double pnFilterTune, pnCflFactor;
 } orc_deck;
 
 typedef struct {
@@ -157,6 +161,8 @@ typedef struct {
     double *initialGrid, *sigmaT, *sigmaS;   /* [NX*NY] */
     double *moments, *alpha, *flux, *momentsOld, *ansatzGrid;
     double *alphaP, *P2M;   /* change-of-basis state per cell (optType 1, 2) */
+    double *pnOps;          /* SOLVER moment: the flux operators xi+, xi-, eta+, eta- [4][n][n] */
+    double *pnFilter;       /* SOLVER moment: filter factor per moment [n] */
     orc_stats stats;
     int *lastIters;         /* per-cell iterations of the last stage */
     int status;             /* first error code seen */
@@ -172,6 +178,9 @@ int orc_solver_create_node(const orc_deck *d, int node, int numNodes, orc_solver
  * (comm.cpp:31-147 in place of the periodic copy): save the interior,
  * one stage without the ghost copy, the Heun average. */
 void orc_solver_save_old(orc_solver *s);
+/* Work of a stage before its exchange: the moment filter of SOLVER moment
+ * (moment_update.cpp:178-179), nothing for momopt. */
+void orc_solver_pre_exchange(orc_solver *s);
 int orc_solver_stage_exchanged(orc_solver *s, double dt);
 void orc_solver_average(orc_solver *s);
 /* momopt_boundaries.cpp:17-188: doubles per side (north, south, east,

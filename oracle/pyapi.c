@@ -127,6 +127,8 @@ void orc_solver_node_info(void *h, int *info, double *origin)
 }
 
 void orc_solver_save_old_h(void *h) { orc_solver_save_old((orc_solver *)h); }
+void orc_solver_pre_exchange_h(void *h) { orc_solver_pre_exchange((orc_solver *)h); }
+int orc_solver_run_h(void *h, const char *dir, int maxSteps) { return orc_solver_run((orc_solver *)h, dir, maxSteps); }
 int orc_solver_stage_exchanged_h(void *h, double dt) { return orc_solver_stage_exchanged((orc_solver *)h, dt); }
 void orc_solver_average_h(void *h) { orc_solver_average((orc_solver *)h); }
 long long orc_solver_halo_count_h(void *h, int side) { return orc_solver_halo_count((orc_solver *)h, side); }
@@ -164,8 +166,12 @@ void orc_solver_state(void *h, double *moments, double *alpha)
     size_t bytes = sizeof(double) * (size_t)s->NX * s->NY * s->set.n;
     if (moments)
         memcpy(moments, s->moments, bytes);
-    if (alpha)
-        memcpy(alpha, s->alpha, bytes);
+    if (alpha) {
+        if (s->alpha)
+            memcpy(alpha, s->alpha, bytes);
+        else
+            memset(alpha, 0, bytes);   /* SOLVER moment has no multipliers */
+    }
 }
 
 void orc_solver_set_state(void *h, const double *moments, const double *alpha)
@@ -174,7 +180,7 @@ void orc_solver_set_state(void *h, const double *moments, const double *alpha)
     size_t bytes = sizeof(double) * (size_t)s->NX * s->NY * s->set.n;
     if (moments)
         memcpy(s->moments, moments, bytes);
-    if (alpha)
+    if (alpha && s->alpha)
         memcpy(s->alpha, alpha, bytes);
 }
 
@@ -203,5 +209,8 @@ long long orc_solver_err_cell(void *h) { return ((orc_solver *)h)->errCell; }
 void orc_solver_last_iters(void *h, int *iters)
 {
     orc_solver *s = (orc_solver *)h;
-    memcpy(iters, s->lastIters, sizeof(int) * (size_t)s->NX * s->NY);
+    if (s->lastIters)
+        memcpy(iters, s->lastIters, sizeof(int) * (size_t)s->NX * s->NY);
+    else
+        memset(iters, 0, sizeof(int) * (size_t)s->NX * s->NY);
 }

@@ -57,6 +57,8 @@ def _bind(L):
         L.orc_solver_open_node.argtypes = [C.c_char_p, C.c_int, C.c_int]
         L.orc_solver_node_info.argtypes = [vp, ip, dp]
         L.orc_solver_save_old_h.argtypes = [vp]
+        L.orc_solver_pre_exchange_h.argtypes = [vp]
+        L.orc_solver_run_h.argtypes = [vp, C.c_char_p, C.c_int]
         L.orc_solver_stage_exchanged_h.argtypes = [vp, C.c_double]
         L.orc_solver_average_h.argtypes = [vp]
         L.orc_solver_halo_count_h.argtypes = [vp, C.c_int]
@@ -183,6 +185,16 @@ class GridSolver:
     # a node's RK2 step with the halo exchanged between the stages
     def save_old(self):
         self.L.orc_solver_save_old_h(self.h)
+
+    def pre_exchange(self):
+        """The stage's work before its halo exchange (the moment filter of
+        SOLVER moment, moment_update.cpp:178-179; nothing for momopt)."""
+        self.L.orc_solver_pre_exchange_h(self.h)
+
+    def run(self, out_dir, max_steps=-1):
+        """main.cpp:204-230 with outputs into out_dir."""
+        st = self.L.orc_solver_run_h(self.h, out_dir.encode(), max_steps)
+        assert st == 0, "oracle error %d" % st
 
     def stage_exchanged(self, dt):
         st = self.L.orc_solver_stage_exchanged_h(self.h, dt)

@@ -12,6 +12,9 @@
  *                                  comm.cpp:149-154)
  *   momopt/momopt_output.cpp:21-77 .pn / .opt writers
  *   main.cpp:204-230               time loop
+ *   moment/moment_init.cpp:53-298, moment_update.cpp:23-247
+ *                                  the linear Pn/FPn solver (SOLVER moment):
+ *                                  flux operators, filters, flux, update
  * Layout is the reference's: I2D(i,j) = i*NY + j, I3D(i,j,k) = (i*NY+j)*n + k.
  */
 #include "oracle.h"
@@ -29,6 +32,7 @@
 #define M_PI 3.14159265358979323846
 #endif
 
+#define ORC_NMAX_PN 512   /* moments per cell of the linear solver (order <= 30) */
 #define MIN(a, b) (((a) < (b)) ? (a) : (b))
 #define MAX(a, b) (((a) > (b)) ? (a) : (b))
 #define SIGN(a, b) ((b) >= 0.0 ? fabs(a) : -fabs(a))
@@ -136,6 +140,18 @@ int orc_deck_read(const char *path, orc_deck *d)
     ok &= kv_dbl(&l, "SIGMA", &d->sigma);
     ok &= kv_int(&l, "NUM_MPI_PARTITIONS_X", &d->nodesX);
     ok &= kv_int(&l, "NUM_MPI_PARTITIONS_Y", &d->nodesY);
+    ok &= kv_get(&l, "SOLVER", solver);
+    if (ok && strcmp(solver, "moment") == 0) {
+        /* moment_init.cpp:57-61 */
+        d->isMoment = 1;
+        ok &= kv_int(&l, "MOMENT_MOMENT_ORDER", &d->pnOrder);
+        ok &= kv_int(&l, "MOMENT_QUAD_ORDER", &d->pnQuadOrder);
+        ok &= kv_int(&l, "MOMENT_FILTER_TYPE", &d->pnFilterType);
+        ok &= kv_dbl(&l, "MOMENT_FILTER_TUNE", &d->pnFilterTune);
+        ok &= kv_dbl(&l, "MOMENT_CFL_FACTOR", &d->pnCflFactor);
+        free(l.items);
+        return ok ? ORC_OK : ORC_ERR_INPUT;
+    }
     ok &= kv_int(&l, "MOMOPT_MOMENT_ORDER", &d->momentOrder);
     ok &= kv_int(&l, "MOMOPT_QUAD_ORDER", &d->quadOrder);
     ok &= kv_dbl(&l, "MOMOPT_CFL_FACTOR", &d->cflFactor);
@@ -161,13 +177,16 @@ int orc_deck_read(const char *path, orc_deck *d)
 #define I2D(i, j) ((i) * s->NY + (j))
 #define I3D(i, j, k) (((size_t)(i) * s->NY + (j)) * n + (k))
 
+static int moment_init(orc_solver *s);
+
 int orc_solver_create(const orc_deck *d, orc_solver *s) { return orc_solver_create_node(d, 0, 1, s); }
 
 int orc_solver_create_node(const orc_deck *d, int node, int numNodes, orc_solver *s)
 {
     memset(s, 0, sizeof(*s));
     s->deck = *d;
-    if (d->optType < 0 || d->optType > 2 || (d->momentType != ORC_MN && d->momentType != ORC_PPN))
+    if (!d->isMoment &&
+        (d->optType < 0 || d->optType > 2 || (d->momentType != ORC_MN && d->momentType != ORC_PPN)))
         return ORC_ERR_INPUT;
     const int ng = 2;
     int sizeX = d->numCellsX, sizeY = d->numCellsY;
@@ -275,6 +294,8 @@ int orc_solver_create_node(const orc_deck *d, int node, int numNodes, orc_solver
             }
         }
     }
+    if (d->isMoment)
+        return moment_init(s);
     /* momopt_init.cpp:72 */
     s->maxDt = d->cflFactor * (2.0 / (2.0 + d->theta)) * (dx * dy) / (dx + dy);
     int st = orc_setup_create(d->momentOrder, d->quadOrder, d->useGaunt, &s->set);
@@ -328,6 +349,8 @@ void orc_solver_free(orc_solver *s)
     free(s->lastIters);
     free(s->alphaP);
     free(s->P2M);
+    free(s->pnOps);
+    free(s->pnFilter);
     orc_setup_free(&s->set);
     memset(s, 0, sizeof(*s));
 }
@@ -506,9 +529,157 @@ static void euler_collide(orc_solver *s, double dt, double dx, double dy)
         }
 }
 
-/* momopt_update.cpp:283-382 */
+/* ---------------- SOLVER moment: the linear Pn / FPn solver ---------------- */
+
+static double filter_sspline(double x) { return 1.0 / (1.0 + x * x * x * x); }
+
+static double filter_lanczos(double x)
+{
+    if (x < .0000001)
+        return 1.0;
+    return sin(x) / x;
+}
+
+/* moment_init.cpp:53-297: maxDt, initial moments, the degree-N basis on the
+ * momopt quadrature, the upwind flux operators and the filter factors */
+static int moment_init(orc_solver *s)
+{
+    const orc_deck *d = &s->deck;
+    const double dx = s->dx, dy = s->dy;
+    s->maxDt = d->pnCflFactor * 0.5 * MIN(dx, dy);
+    if ((d->pnOrder + 1) * (d->pnOrder + 2) / 2 > ORC_NMAX_PN)
+        return ORC_ERR_INPUT;
+    int st = orc_setup_create(d->pnOrder, d->pnQuadOrder, 0, &s->set);
+    if (st)
+        return st;
+    const int n = s->set.n, nq = s->set.nq;
+    const size_t C = (size_t)s->NX * s->NY;
+    s->moments = (double *)malloc(sizeof(double) * C * n);
+    s->flux = (double *)calloc(C * n, sizeof(double));
+    s->momentsOld = (double *)calloc(C * n, sizeof(double));
+    for (int i = s->gX[0]; i <= s->gX[3]; i++)
+        for (int j = s->gY[0]; j <= s->gY[3]; j++) {
+            s->moments[I3D(i, j, 0)] = s->initialGrid[I2D(i, j)] * 2.0 * sqrt(M_PI);
+            for (int k = 1; k < n; k++)
+                s->moments[I3D(i, j, k)] = 0.0;
+        }
+    /* moment_init.cpp:186-222: quadrature sums split by the sign of xi, eta */
+    s->pnOps = (double *)calloc((size_t)4 * n * n, sizeof(double));
+    double *xp = s->pnOps, *xm = xp + n * n, *ep = xm + n * n, *em = ep + n * n;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+            for (int q = 0; q < nq; q++) {
+                const double mi = s->set.p[(size_t)q * s->set.n2 + i];
+                const double mj = s->set.p[(size_t)q * s->set.n2 + j];
+                const double vx = s->set.xi[q] * mi * mj * s->set.w[q];
+                const double ve = s->set.eta[q] * mi * mj * s->set.w[q];
+                if (s->set.xi[q] > 0)
+                    xp[i * n + j] += vx;
+                else
+                    xm[i * n + j] += vx;
+                if (s->set.eta[q] > 0)
+                    ep[i * n + j] += ve;
+                else
+                    em[i * n + j] += ve;
+            }
+    /* moment_init.cpp:225-289 */
+    s->pnFilter = (double *)malloc(sizeof(double) * n);
+    const double N = d->pnOrder;
+    int nm = 0;
+    for (int l = 0; l <= d->pnOrder; l++)
+        for (int m = -l; m <= l; m++) {
+            if ((m + l) % 2 != 0)
+                continue;
+            double f = 1.0;
+            if (d->pnFilterType == 1) {
+                const double omega = d->pnFilterTune, L = 1.0, sigt = 1.0;
+                const double a = omega / (N * N) / (sigt * L + N) / (sigt * L + N);
+                f = 1.0 / (1.0 + a * l * l * (l + 1) * (l + 1));
+            } else if (d->pnFilterType == 2) {
+                const double sp = -d->pnFilterTune * s->maxDt / log(filter_sspline(N / (N + 1)));
+                f = pow(filter_sspline(l / (N + 1)), sp);
+            } else if (d->pnFilterType == 3) {
+                const double sp = -d->pnFilterTune * s->maxDt / log(filter_lanczos(N / (N + 1)));
+                f = pow(filter_lanczos(l / (N + 1)), sp);
+            }
+            s->pnFilter[nm++] = f;
+        }
+    memset(&s->stats, 0, sizeof(s->stats));
+    s->status = ORC_OK;
+    s->errCell = -1;
+    return ORC_OK;
+}
+
+/* moment_update.cpp:23-40 */
+static void moment_scale(orc_solver *s)
+{
+    const int n = s->set.n;
+    for (int i = s->gX[1]; i <= s->gX[2]; i++)
+        for (int j = s->gY[1]; j <= s->gY[2]; j++)
+            for (int k = 0; k < n; k++)
+                s->moments[I3D(i, j, k)] = s->moments[I3D(i, j, k)] * s->pnFilter[k];
+}
+
+/* y = A^T x for the n x n operator a (dgemv T on the array the reference
+ * fills row by row); y += when acc */
+static void op_t(int n, const double *a, const double *x, double *y, int acc)
+{
+    for (int j = 0; j < n; j++) {
+        double t = 0.0;
+        for (int i = 0; i < n; i++)
+            t += a[(size_t)j * n + i] * x[i];
+        y[j] = acc ? y[j] + t : t;
+    }
+}
+
+/* moment_update.cpp:49-162 */
+static void moment_flux(orc_solver *s, double dx, double dy)
+{
+    const int n = s->set.n;
+    const double *xp = s->pnOps, *xm = xp + n * n, *ep = xm + n * n, *em = ep + n * n;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = s->gX[1]; i <= s->gX[2]; i++) {
+        double t[ORC_NMAX_PN], ew[ORC_NMAX_PN], ns[ORC_NMAX_PN];
+        for (int j = s->gY[1]; j <= s->gY[2]; j++) {
+            const double *m = s->moments;
+            for (int k = 0; k < n; k++)
+                t[k] = 0.25 * m[I3D(i + 1, j, k)] + 0.75 * m[I3D(i, j, k)] - 1.25 * m[I3D(i - 1, j, k)] +
+                       0.25 * m[I3D(i - 2, j, k)];
+            op_t(n, xp, t, ew, 0);
+            for (int k = 0; k < n; k++)
+                t[k] = -0.25 * m[I3D(i + 2, j, k)] + 1.25 * m[I3D(i + 1, j, k)] - 0.75 * m[I3D(i, j, k)] -
+                       0.25 * m[I3D(i - 1, j, k)];
+            op_t(n, xm, t, ew, 1);
+            for (int k = 0; k < n; k++)
+                t[k] = 0.25 * m[I3D(i, j + 1, k)] + 0.75 * m[I3D(i, j, k)] - 1.25 * m[I3D(i, j - 1, k)] +
+                       0.25 * m[I3D(i, j - 2, k)];
+            op_t(n, ep, t, ns, 0);
+            for (int k = 0; k < n; k++)
+                t[k] = -0.25 * m[I3D(i, j + 2, k)] + 1.25 * m[I3D(i, j + 1, k)] - 0.75 * m[I3D(i, j, k)] -
+                       0.25 * m[I3D(i, j - 1, k)];
+            op_t(n, em, t, ns, 1);
+            for (int k = 0; k < n; k++)
+                s->flux[I3D(i, j, k)] = 1.0 / dx * ew[k] + 1.0 / dy * ns[k];
+        }
+    }
+}
+
+/* momopt_update.cpp:283-382 (SOLVER momopt), moment_update.cpp:169-247
+ * (SOLVER moment) */
 int orc_solver_update(orc_solver *s, double dt)
 {
+    if (s->deck.isMoment) {
+        orc_solver_save_old(s);
+        for (int stage = 0; stage < 2; stage++) {
+            orc_solver_pre_exchange(s);
+            if (s->deck.initCond == 2)
+                duplicate_boundaries(s);
+            moment_flux(s, s->dx, s->dy);
+            euler_collide(s, dt, s->dx, s->dy);
+        }
+        orc_solver_average(s);
+        return ORC_OK;
+    }
     int n = s->set.n;
     double dx = s->dx, dy = s->dy;
     for (int i = s->gX[1]; i <= s->gX[2]; i++)
@@ -554,6 +725,8 @@ int orc_solver_output(orc_solver *s, double time, const char *dir)
         for (int j = s->gY[1]; j <= s->gY[2]; j++)
             fwrite(&s->moments[I3D(i, j, 0)], sizeof(double), n, f);
     fclose(f);
+    if (s->deck.isMoment)
+        return ORC_OK;   /* moment_output.cpp writes the .pn file only */
     snprintf(fn, sizeof(fn), "%s/out_%.3f_%d.opt", dir ? dir : ".", time, s->node);
     f = fopen(fn, "w");
     if (!f)
@@ -628,9 +801,21 @@ void orc_solver_save_old(orc_solver *s)
                 s->momentsOld[I3D(i, j, k)] = s->moments[I3D(i, j, k)];
 }
 
-/* momopt_update.cpp:311-336 with the ghosts already exchanged */
+void orc_solver_pre_exchange(orc_solver *s)
+{
+    if (s->deck.isMoment && s->deck.pnFilterType != 0)
+        moment_scale(s);
+}
+
+/* momopt_update.cpp:311-336 (moment_update.cpp:180-203) with the ghosts
+ * already exchanged */
 int orc_solver_stage_exchanged(orc_solver *s, double dt)
 {
+    if (s->deck.isMoment) {
+        moment_flux(s, s->dx, s->dy);
+        euler_collide(s, dt, s->dx, s->dy);
+        return ORC_OK;
+    }
     solve_optimization(s);
     if (s->status != ORC_OK)
         return s->status;

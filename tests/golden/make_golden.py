@@ -1,4 +1,5 @@
-"""Copies the reference's eight momopt regression goldens into tests/golden/.
+"""Copies the reference's regression goldens into tests/golden/: the eight
+momopt files and the sixteen of the linear moment solver.
 
 The reference's regression harness (site_scons/testing.py:109-303) compares
 out_1.030_0.pn against tests/regression/momopt/<ic>/<type>.pn.  Those files
@@ -14,6 +15,7 @@ import sys
 
 ICS = ["delta", "gaussian", "lattice", "smooth"]
 TYPES = ["mn", "ppn"]
+FILTERS = ["none", "hauck", "sspline", "lanczos"]   # site_scons/testing.py:19
 
 
 def main(ref_root):
@@ -27,6 +29,19 @@ def main(ref_root):
             dst = os.path.join(here, "%s_%s.pn.xz" % (ic, t))
             with lzma.open(dst, "wb", preset=9 | lzma.PRESET_EXTREME) as f:
                 f.write(data)
+            print(dst, len(data))
+    # the moment solver's goldens: tests/regression/moment/<ic>/<filter>.pn
+    # (site_scons/testing.py:252-276, same grid and time as momopt)
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "moment")
+    os.makedirs(here, exist_ok=True)
+    for ic in ICS:
+        for f in FILTERS:
+            src = os.path.join(ref_root, "tests", "regression", "moment", ic, f + ".pn")
+            with open(src, "rb") as fh:
+                data = fh.read()
+            dst = os.path.join(here, "%s_%s.pn.xz" % (ic, f))
+            with lzma.open(dst, "wb", preset=9 | lzma.PRESET_EXTREME) as fh:
+                fh.write(data)
             print(dst, len(data))
 
 

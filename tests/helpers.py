@@ -40,6 +40,11 @@ def read_golden(ic, mtype):
         return parse_pn(f.read())
 
 
+def read_moment_golden(ic, filt):
+    with lzma.open(os.path.join(GOLDEN_DIR, "moment", "%s_%s.pn.xz" % (ic, filt)), "rb") as f:
+        return parse_pn(f.read())
+
+
 def density(m):
     """util/formats.py:185-189: density grid u0 / (2 sqrt(pi))."""
     return m[:, :, 0] / (2.0 * math.sqrt(math.pi))
