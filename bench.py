@@ -499,6 +499,156 @@ def native_arm(args, world, rank, local):
 BATCH_ORDERS = [5, 4, 3, 2, 1]   # most expensive first (longest-processing-time order)
 
 
+# The linear Pn/FPn solver (SOLVER moment): a P6 Gaussian pulse on 800 x 800
+# with the Hauck filter; the quadrature only builds the flux operators.
+PN_WORKLOADS = {
+    "pn6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
+                    gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian", moment_order=6,
+                    quad_order=40, filter_type="hauck", filter_tune=100, t_final=1.0),
+}
+PN_METRIC = "linear Pn cell-updates/s (interior cells x RK stages), 1 B200"
+
+
+def pn_flops_per_update(n):
+    """FLOPs of one interior cell in one stage (FMA = 2): four n x n operator
+    products, four stencil combinations and the update."""
+    return 8 * n * n + 4 * 7 * n + 10 * n
+
+
+def pn_arm(args, world, rank, local):
+    """The linear moment solver: N x 1 partitions of the workload widened N
+    times in x under torchrun (as the grid workloads), one node per rank."""
+    import torch
+    import closures_b200 as cb
+
+    w = dict(PN_WORKLOADS[args.workload])
+    tmp = tempfile.mkdtemp(prefix="bench_pn_")
+    if world > 1:
+        w["num_cells_x"] *= world
+        w["b_x"] = w["a_x"] + (w["b_x"] - w["a_x"]) * world
+        w["partitions"] = (world, 1)
+    deck = os.path.join(tmp, "input.deck")
+    decks.write_deck(deck, decks.moment_deck_text(**w))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps, secs, _, threads = run_oracle_steps(deck, args.steps, budget_s=150.0)
+        nx, ny = PN_WORKLOADS[args.workload]["num_cells_x"], PN_WORKLOADS[args.workload]["num_cells_y"]
+        value = 2 * nx * ny * steps / secs
+        print(json.dumps({
+            "impl": "reference", "metric": PN_METRIC, "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * secs / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "grid": [nx, ny],
+                                            "moment_order": w["moment_order"]},
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": "first %d RK2 step(s) of the deck from t=0" % steps},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        dist.barrier()
+    solver = cb.NodeSolver(deck, tmp, node=rank, num_nodes=world)
+    dt, n = solver.max_dt, solver.n
+    C_int = solver.nx * solver.ny
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        solver.update(dt)
+    peak = cb.fp64_peak_tflops()
+    launches0 = cb.launch_count()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    stage_ms, exchange_ms = 0.0, 0.0
+    for _ in range(args.steps):
+        for stage in (1, 2):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(solver.stream)
+            solver.exchange()
+            e1.record(solver.stream)
+            stage_ms += solver.stage_timed(stage, dt)[1]
+            exchange_ms += e0.elapsed_time(e1)
+    barrier()
+    clocks = sampler.stop()
+    launches = cb.launch_count() - launches0
+    device_ms = stage_ms + exchange_ms
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([device_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        device_ms = float(tt.item())
+    updates = 2 * C_int * args.steps
+    value = world * updates / (device_ms * 1e-3)
+    achieved = updates * pn_flops_per_update(n) / (stage_ms * 1e-3) / 1e12
+
+    # end to end: the state from pinned host memory, the step, the state back
+    C = solver.NX * solver.NY
+    hm = torch.empty((C, n), dtype=torch.float64).pin_memory().numpy()
+    hm[:] = solver.moments().reshape(C, n)
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.set_moments(hm)
+        solver.update(dt)
+        hm[:] = solver.moments().reshape(C, n)
+    barrier()
+    e2e_s = time.perf_counter() - t1
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        steps, secs, _, threads = run_oracle_steps(deck, 1, budget_s=60.0)
+        cpu = {"value": 2 * C_int * steps / secs, "unit": "cell-updates/s", "cores": threads,
+               "kind": "port", "sample": "first RK2 step of the same deck from t=0 on all %d host "
+                                         "threads (oracle restatement, -O3 -fopenmp)" % threads}
+    if rank == 0:
+        print(json.dumps({
+            "metric": PN_METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": device_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+                       "grid_per_gpu": [PN_WORKLOADS[args.workload]["num_cells_x"], w["num_cells_y"]],
+                       "moment_order": w["moment_order"], "n": n, "filter": w["filter_type"],
+                       "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
+                       "parallelism": ("halo %dx1 (NCCL point-to-point before each RK stage)" % world)
+                       if world > 1 else "single"},
+            "kernel_ms": {"pn_stage": stage_ms, "halo_exchange": exchange_ms},
+            "roofline": {"bound": "fp64", "kernel": "pn_stage", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "FP64 DMMA m16n8k8 throughput measured live (cl_fp64_peak)",
+                         "flops_per_update": pn_flops_per_update(n),
+                         "hbm_gbs_algorithmic": updates * (2.5 * n * 8 + 16) / (stage_ms * 1e-3) / 1e9},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * 2 * C_int * e2e_steps / e2e_s, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": C * n * 8, "d2h_bytes_per_step": C * n * 8, "steps": e2e_steps},
+            "gpu_launches": int(launches), "clocks": clocks}), flush=True)
+    solver.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def sample_batch_torch(angular, count, gen, device):
     """Batched-optimisation workload on the device (FP64): alpha_k ~ N(0, s^2),
     s log-uniform in [0.1, 20], alpha_0 such that u_0 = 1, u = <m e^{alpha.m}>."""
@@ -658,7 +808,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--workload", default="m6_800", choices=sorted(WORKLOADS) + ["batch_2e20"])
+    ap.add_argument("--workload", default="m6_800",
+                    choices=sorted(WORKLOADS) + ["batch_2e20"] + sorted(PN_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
                     help="batch workload: start from the isotropic multiplier or a learned prediction")
@@ -675,6 +826,8 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "batch_2e20":
         return batch_arm(args, world, rank, local)
+    if args.workload in PN_WORKLOADS:
+        return pn_arm(args, world, rank, local)
     if args.impl == "reference":
         return reference_arm(args, world, rank)
     return native_arm(args, world, rank, local)

@@ -24,6 +24,7 @@ CL_OK, CL_ERR_ARG, CL_ERR_CUDA, CL_ERR_U0, CL_ERR_MAXREG, CL_ERR_TIMEOUT, CL_ERR
     0, -1, -2, -3, -4, -5, -6)
 CL_MN, CL_PPN = 0, 1
 CL_FP64, CL_MIXED = 0, 1
+CL_SOLVER_MOMOPT, CL_SOLVER_MOMENT = 0, 1
 REGULARIZATIONS = (0.0, 1e-3, 1e-2, 1e-1, 5e-1)
 
 
@@ -154,6 +155,19 @@ def lib():
                                                 C.POINTER(vp), dp]),
             "cl_solver_node": (C.c_int, [vp, C.POINTER(cl_node)]),
             "cl_solver_stage": (C.c_int, [vp, C.c_int, C.c_double]),
+            "cl_solver_kind": (C.c_int, [vp]),
+            "cl_solver_get_state": (C.c_int, [vp, dp]),
+            "cl_solver_set_state": (C.c_int, [vp, dp]),
+            "cl_solver_pn": (vp, [vp]),
+            "cl_solver_halo_counts": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+            "cl_solver_halo_pack": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_solver_halo_unpack": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_solver_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "cl_solver_sync": (C.c_int, [vp]),
+            "cl_solver_set_exchanged_sides": (C.c_int, [vp, C.c_int]),
+            "cl_pn_stage_timed": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                            C.POINTER(C.c_float)]),
+            "cl_pn_last_error": (C.c_char_p, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -430,8 +444,27 @@ class Solver:
             self._cctx = c
         return c
 
+    @property
+    def kind(self):
+        """CL_SOLVER_MOMOPT or CL_SOLVER_MOMENT (the deck's SOLVER)."""
+        return lib().cl_solver_kind(self._s)
+
+    def moments(self):
+        """The state (ghosts included) as [NX][NY][n]."""
+        m = np.empty((self.NX * self.NY, self.n))
+        _check(lib().cl_solver_get_state(self._s, _dp(m)), self._err)
+        return m.reshape(self.NX, self.NY, self.n)
+
+    def set_moments(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        _check(lib().cl_solver_set_state(self._s, _dp(m)), self._err)
+
     def context_state(self):
+        """Moments and multipliers (momopt; zeros for the multipliers of the
+        linear moment solver, which has none)."""
         ctx = lib().cl_solver_context(self._s)
+        if not ctx:
+            return self.moments(), np.zeros((self.NX, self.NY, self.n))
         m = np.empty((self.NX * self.NY, self.n))
         a = np.empty((self.NX * self.NY, self.n))
         _check(lib().cl_get_state(ctx, _dp(m), _dp(a)), lambda: lib().cl_last_error(ctx))
@@ -567,14 +600,17 @@ class NodeSolver(Solver):
         self.node_info = {f: getattr(info, f) for f, _ in cl_node._fields_}
         periodic = int(deck_value(deck_path, "INIT_COND") or 0) == 2
         self.plan = HaloPlan(node, info.nodes_x, info.nodes_y, periodic)
-        self._ctxp = lib().cl_solver_context(self._s)
         counts = (C.c_longlong * 4)()
-        lib().cl_halo_counts(self._ctxp, counts)
+        _check(lib().cl_solver_halo_counts(self._s, counts), self._err)
+        # the linear solver filters the strips an exchange fills like its
+        # interior (moment_update.cpp:178-182)
+        mask = sum(1 << k for k in SIDES if self.plan.peer[k] is not None)
+        lib().cl_solver_set_exchanged_sides(self._s, mask)
         self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.send = [torch.empty(int(c), dtype=torch.float64, device=self.device) for c in counts]
         self.recv = [torch.empty(int(c), dtype=torch.float64, device=self.device) for c in counts]
         st = C.c_void_p()
-        lib().cl_stream(self._ctxp, C.byref(st))
+        lib().cl_solver_stream(self._s, C.byref(st))
         self.stream = torch.cuda.ExternalStream(st.value, device=self.device)
 
     def _ptrs(self, bufs, sides):
@@ -583,15 +619,13 @@ class NodeSolver(Solver):
     def pack(self):
         """getInnerBoundaries for the sides that have a peer."""
         sides = [k for k in SIDES if self.plan.peer[k] is not None]
-        _check(lib().cl_halo_pack(self._ctxp, self._ptrs(self.send, sides)),
-               lambda: lib().cl_last_error(self._ctxp))
+        _check(lib().cl_solver_halo_pack(self._s, self._ptrs(self.send, sides)), self._err)
 
     def unpack(self):
         """setOuterBoundaries for the sides that have a peer (the peer of a
         side sends the strip for it)."""
         sides = [k for k in SIDES if self.plan.peer[k] is not None]
-        _check(lib().cl_halo_unpack(self._ctxp, self._ptrs(self.recv, sides)),
-               lambda: lib().cl_last_error(self._ctxp))
+        _check(lib().cl_solver_halo_unpack(self._s, self._ptrs(self.recv, sides)), self._err)
 
     def stage(self, stage, dt):
         _check(lib().cl_solver_stage(self._s, stage, dt), self._err)
@@ -599,9 +633,16 @@ class NodeSolver(Solver):
     def stage_timed(self, stage, dt):
         """The stage, waited for: (optimisation ms, flux/update ms)."""
         ms = (C.c_float * 2)()
-        _check(lib().cl_stage_timed(self._ctxp, stage, dt, self.dx, self.dy, ms),
-               lambda: lib().cl_last_error(self._ctxp))
-        return ms[0], ms[1]
+        ctx = lib().cl_solver_context(self._s)
+        if ctx:
+            _check(lib().cl_stage_timed(ctx, stage, dt, self.dx, self.dy, ms),
+                   lambda: lib().cl_last_error(ctx))
+            return ms[0], ms[1]
+        # the linear moment solver has no optimisation: (0, stage ms)
+        pn = lib().cl_solver_pn(self._s)
+        _check(lib().cl_pn_stage_timed(pn, stage, dt, self.dx, self.dy, ms),
+               lambda: lib().cl_pn_last_error(pn))
+        return 0.0, ms[0]
 
     def exchange(self, group=None):
         """The halo exchange before a stage: pack on the library's stream,
@@ -616,7 +657,7 @@ class NodeSolver(Solver):
         self.unpack()
 
     def sync(self):
-        _check(lib().cl_sync(self._ctxp), lambda: lib().cl_last_error(self._ctxp))
+        _check(lib().cl_solver_sync(self._s), self._err)
 
     def update(self, dt, group=None):
         """One RK2 step with the halo exchanged over torch.distributed before

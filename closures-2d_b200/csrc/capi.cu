@@ -304,7 +304,7 @@ int cl_angular_create(int order, int quad_order, int use_gaunt, cl_angular *out)
     memset(out, 0, sizeof(*out));
     Angular A;
     if (build_angular(order, quad_order, use_gaunt, A) != 0) {
-        g_global_err = "unsupported order/quadrature (order 1..6, Q >= 2 even)";
+        g_global_err = "unsupported order/quadrature (order 1..6 with the Gaunt table, 1..9 without; Q >= 2 even)";
         return CL_ERR_ARG;
     }
     out->order = A.order;
@@ -1087,8 +1087,8 @@ int cl_multi_create(int norders, const int *orders, int quad_order, int use_gaun
     a.nprob = norders;
     for (int p = 0; p < norders; p++) {
         Angular A;
-        if (build_angular(orders[p], quad_order, use_gaunt, A) != 0) {
-            g_global_err = "unsupported order";
+        if (orders[p] > 6 || build_angular(orders[p], quad_order, use_gaunt, A) != 0) {
+            g_global_err = "unsupported order (1..6)";
             cl_multi_destroy(m);
             return CL_ERR_ARG;
         }

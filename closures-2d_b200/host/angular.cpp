@@ -159,7 +159,9 @@ struct LeastSquares {
 
 int build_angular(int order, int Q, int useGaunt, Angular &A)
 {
-    if (order < 1 || order > 6 || Q < 2 || Q % 2 != 0)
+    // orders above 6 (more than 32 moments) serve the linear moment solver,
+    // which has no Gaunt table; the entropy-closure kernels take n <= 32
+    if (order < 1 || order > (useGaunt ? 6 : 9) || Q < 2 || Q % 2 != 0)
         return -1;
     A.order = order;
     A.Q = Q;

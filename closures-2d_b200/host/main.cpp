@@ -1,4 +1,4 @@
-// main.cpp -- drop-in driver for SOLVER momopt on one B200.
+// main.cpp -- drop-in driver for SOLVER momopt and SOLVER moment on one B200.
 //
 // Mirrors src/main.cpp:45-251 for one node: reads input.deck from the working
 // directory (or argv[1]), initialises the grid and the solver, runs the
@@ -8,7 +8,7 @@
 #include <cstdlib>
 #include <string>
 
-#include "momopt_gpu_solver.h"
+#include "solver.h"
 
 int main(int argc, char **argv)
 {

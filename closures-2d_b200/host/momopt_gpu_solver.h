@@ -12,35 +12,28 @@ namespace clb {
 class MomOptGpuSolver : public Solver {
 public:
     ~MomOptGpuSolver() override;
-    double init(double dx, double dy) override;
-    int getNumGhostCells() override { return 2; }
-    void update(double dt, double dx, double dy) override;
-    void outputData(double time) override;
-    int getBoundarySizeX() override;
-    int getBoundarySizeY() override;
-    void getInnerBoundaries(char *north, char *south, char *east, char *west) override;
-    void setOuterBoundaries(char *north, char *south, char *east, char *west) override;
-    void duplicateBoundaries() override;
 
-    // Non-aborting forms used by the C ABI wrappers: return CL_OK or an error.
-    int tryInit(double dx, double dy, double *maxDt);
-    int tryUpdate(double dt, double dx, double dy);
-    int tryOutput(double time);
+    int tryInit(double dx, double dy, double *maxDt) override;
+    int tryUpdate(double dt, double dx, double dy) override;
+    int tryOutput(double time) override;
+    int tryStage(int stage, double dt, double dx, double dy) override;
+    int numMoments() const override { return m_n; }
+    int getState(double *moments) override;
+    int setState(const double *moments) override;
+    int haloCounts(long long counts[4]) override;
+    int haloPack(double *const bufs[4]) override;
+    int haloUnpack(double *const bufs[4]) override;
+    void *stream() override;
+    int sync() override;
 
     cl_ctx *context() { return m_ctx; }
-    int numMoments() const { return m_n; }
-    std::string lastError;
-    std::string outDir = ".";
 
 private:
+    int ctxError(int rc);
     int m_n = 0;
     double m_maxDt = 0;
     cl_ctx *m_ctx = nullptr;
     cl_options m_opt{};
 };
-
-// The main.cpp driver for SOLVER momopt: reads the deck, builds the solver,
-// runs the time loop with outputs.  Returns 0 or an error code (message in err).
-int run_deck(const char *deckPath, const char *outDir, int maxSteps, std::string &err);
 
 }  // namespace clb

@@ -66,7 +66,9 @@ typedef struct {
 
 /* Builds the quadrature, the z-even real spherical-harmonic basis (with the
  * Condon-Shortley phase) and, if use_gaunt, the product table, in FP64 on
- * the host.  Replaces MomOptSolver::init's set-up, momopt_init.cpp:88-259. */
+ * the host.  Replaces MomOptSolver::init's set-up, momopt_init.cpp:88-259
+ * (and moment_init.cpp:69-183).  Orders 1..6 with the Gaunt table, 1..9
+ * without (the entropy-closure contexts take orders up to 6). */
 int cl_angular_create(int order, int quad_order, int use_gaunt, cl_angular *out);
 void cl_angular_free(cl_angular *a);
 
@@ -223,22 +225,76 @@ int cl_multi_solve_device_start(cl_multi *m, const int *counts, double *const *d
                                 int *const *d_status);
 /* ------------------------------------------------------------------------
  * Whole solver behind the reference's Solver interface (solver.h:15-61) for
- * SOLVER momopt on one node: deck parsing (input_deck_reader.cpp), grid and
- * initial condition (main.cpp:257-372), MomOptSolver::init
- * (momopt_init.cpp:51-272), update (momopt_update.cpp:283-382) and
- * outputData (momopt_output.cpp:21-77, files out_<t>_0.pn / .opt). */
+ * the deck's SOLVER (main.cpp:93-106): momopt (MomOptSolver,
+ * momopt_init.cpp:51-272, momopt_update.cpp:283-382, momopt_output.cpp:21-77,
+ * files out_<t>_<node>.pn / .opt) or moment (MomentSolver, the linear Pn/FPn
+ * solver, moment_init.cpp:53-297, moment_update.cpp:169-247,
+ * moment_output.cpp:21-56, file out_<t>_<node>.pn); deck parsing
+ * (input_deck_reader.cpp), grid and initial condition (main.cpp:257-372). */
 typedef struct cl_solver cl_solver;
-/* Reads deck_path (input.deck semantics, every MOMOPT_* key required as in
- * momopt_init.cpp:56-68) and creates the solver; *max_dt receives init()'s
- * return value (momopt_init.cpp:72).  Output files go to out_dir. */
+typedef struct cl_pn cl_pn;
+enum { CL_SOLVER_MOMOPT = 0, CL_SOLVER_MOMENT = 1 };
+/* Reads deck_path (input.deck semantics, every key of the solver required as
+ * in momopt_init.cpp:56-68 / moment_init.cpp:57-61) and creates the solver;
+ * *max_dt receives init()'s return value (momopt_init.cpp:72,
+ * moment_init.cpp:65).  Output files go to out_dir. */
 int cl_solver_create(const char *deck_path, const char *out_dir, cl_solver **out, double *max_dt);
+int cl_solver_kind(const cl_solver *s);                 /* CL_SOLVER_MOMOPT or _MOMENT */
 int cl_solver_geometry(cl_solver *s, int *nx, int *ny, int *n, double *dx, double *dy, double *t_final,
                        double *out_delta_t);
 int cl_solver_update(cl_solver *s, double dt);          /* Solver::update */
 int cl_solver_output(cl_solver *s, double time);        /* Solver::outputData */
+/* The state (all cells, ghosts included, [(nx+4)*(ny+4)*n]) to / from the host. */
+int cl_solver_get_state(cl_solver *s, double *moments);
+int cl_solver_set_state(cl_solver *s, const double *moments);
+/* The device context of a momopt solver (null for moment), of a moment
+ * solver (null for momopt). */
 cl_ctx *cl_solver_context(cl_solver *s);
+cl_pn *cl_solver_pn(cl_solver *s);
 const char *cl_solver_last_error(const cl_solver *s);
 void cl_solver_destroy(cl_solver *s);
+
+/* ------------------------------------------------------------------------
+ * The linear Pn / FPn solver (SOLVER moment, src/moment/): moments evolved
+ * by upwind flux operators with an optional filter, no optimisation.  The
+ * host builds the set-up as MomentSolver::init does (moment_init.cpp:53-297);
+ * the context holds the grid state on the device and steps it. */
+typedef struct {
+    int n;                  /* moments per cell, at most 64 (order <= 9) */
+    const double *ops;      /* [4][n][n] c_pnFluxOperatorXiPlus, XiMinus,
+                               EtaPlus, EtaMinus, row i column j as
+                               moment_init.cpp:186-222 fills them */
+    const double *filter;   /* [n] c_momentFilter, or null for
+                               MOMENT_FILTER_TYPE 0 (no filtering) */
+} cl_pn_setup;
+/* Grid as for cl_create; moments [(nx+4)*(ny+4)*n], ghosts included. */
+int cl_pn_create(const cl_grid *grid, const cl_pn_setup *setup, const double *sigma_t,
+                 const double *sigma_s, const double *moments, cl_pn **out);
+void cl_pn_destroy(cl_pn *p);
+const char *cl_pn_last_error(const cl_pn *p);
+/* MomentSolver::update (moment_update.cpp:169-247): one Heun RK2 step, the
+ * periodic ghost copy before each stage for INIT_COND 2; waits. */
+int cl_pn_step(cl_pn *p, double dt, double dx, double dy);
+/* One stage (1 then 2) without the ghost copy, for a node whose halo is
+ * exchanged before each stage (cl_pn_halo_*); asynchronous. */
+int cl_pn_stage(cl_pn *p, int stage, double dt, double dx, double dy);
+/* Same, waited for; *ms receives its duration (CUDA events). */
+int cl_pn_stage_timed(cl_pn *p, int stage, double dt, double dx, double dy, float *ms);
+/* Bit s set: the ghost strip of side s holds a neighbour's interior (the
+ * filter applies to it as to the interior, moment_update.cpp:178-182);
+ * default: all sides for INIT_COND 2, none otherwise. */
+int cl_pn_set_exchanged_sides(cl_pn *p, int mask);
+int cl_pn_sync(cl_pn *p);
+int cl_pn_stream(cl_pn *p, void **stream);
+/* All cells; ghost strips that a periodic copy or a halo exchange fills hold
+ * the values copied before the step's first stage (they are refilled before
+ * every stage, so the interior is the reference's). */
+int cl_pn_get_state(cl_pn *p, double *moments);
+int cl_pn_set_state(cl_pn *p, const double *moments);
+/* As cl_halo_*, on the state the next stage reads (moment_boundaries.cpp). */
+int cl_pn_halo_counts(const cl_pn *p, long long counts[4]);
+int cl_pn_halo_pack(cl_pn *p, double *const bufs[4]);
+int cl_pn_halo_unpack(cl_pn *p, double *const bufs[4]);
 /* A node of the block partition of main.cpp:157-193 (the MPI build): the
  * grid of num_cells_x x num_cells_y cells on [ax,bx] x [ay,by] split into
  * nodes_x x nodes_y blocks, node = node_x * nodes_y + node_y. */
@@ -258,8 +314,18 @@ int cl_partition(int num_cells_x, int num_cells_y, int nodes_x, int nodes_y, int
 int cl_solver_create_node(const char *deck_path, const char *out_dir, int node, int num_nodes,
                           cl_solver **out, double *max_dt);
 int cl_solver_node(const cl_solver *s, cl_node *out);
-/* cl_stage on the solver's context with its dx, dy (stage 1 or 2). */
+/* One RK stage (1 or 2) of the solver with its dx, dy, without the ghost
+ * copy (cl_stage / cl_pn_stage); asynchronous on the solver's stream. */
 int cl_solver_stage(cl_solver *s, int stage, double dt);
+/* The halo of the solver's node (cl_halo_* / cl_pn_halo_*), the stream its
+ * device work runs on, a wait for that work, and the sides whose ghost strips
+ * the exchange fills (the linear solver filters them like the interior). */
+int cl_solver_halo_counts(cl_solver *s, long long counts[4]);
+int cl_solver_halo_pack(cl_solver *s, double *const bufs[4]);
+int cl_solver_halo_unpack(cl_solver *s, double *const bufs[4]);
+int cl_solver_stream(cl_solver *s, void **stream);
+int cl_solver_sync(cl_solver *s);
+int cl_solver_set_exchanged_sides(cl_solver *s, int mask);
 
 /* main.cpp:204-230: outputs at t = 0 and every OUT_DELTA_T up to T_FINAL;
  * max_steps >= 0 stops after that many RK2 steps. */

@@ -93,6 +93,23 @@ def test_optimization_types_are_validated(tmp_path):
     assert e.code == cb.CL_ERR_ARG and "MAX_BFGS_ITER" in str(e)
 
 
+def test_moment_solver_deck_is_validated(tmp_path):
+    """SOLVER moment (the linear Pn/FPn solver) passes the deck checks and,
+    without a GPU, stops at the device; a missing MOMENT_* key is an input
+    error as moment_init.cpp:57-61 makes it."""
+    d = tmp_path / "moment.deck"
+    decks.write_deck(str(d), decks.moment_deck_text(num_cells_x=4, num_cells_y=4, moment_order=2,
+                                                    quad_order=8))
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert e.value.code == cb.CL_ERR_CUDA
+    text = "\n".join(l for l in open(d).read().splitlines() if not l.startswith("MOMENT_FILTER_TUNE"))
+    decks.write_deck(str(d), text + "\n")
+    with pytest.raises(cb.ClosuresError) as e:
+        cb.Solver(str(d), str(tmp_path))
+    assert e.value.code == cb.CL_ERR_ARG and "MOMENT_" in str(e.value)
+
+
 def test_missing_deck_key_is_an_input_error(tmp_path):
     text = decks.deck_text(num_cells_x=4, num_cells_y=4, moment_order=1, quad_order=4)
     text = "\n".join(l for l in text.splitlines() if not l.startswith("MOMOPT_MAX_BFGS_ITER"))
