@@ -1283,6 +1283,9 @@ extern "C" int cl_selftest(void)
 // Lets the host solver layer report through cl_global_error().
 void clb_set_global_error(const char *msg) { g_global_err = msg ? msg : ""; }
 
+// Kernel launches of the other translation units, for cl_launch_count().
+void clb_count_launches(long long k) { g_launches += k; }
+
 // ------------------------------------------------------------- FP64 peak
 namespace {
 // Independent DMMA chains per warp; each m16n8k8 is 1024 FMA = 2048 flops.

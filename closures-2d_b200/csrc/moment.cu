@@ -2,7 +2,8 @@
 // the device: the state of one grid, the RK2 step of MomentSolver::update
 // (moment_update.cpp:169-247) and the halo of a partitioned grid.
 //
-// One kernel per RK stage: for each interior cell it applies the moment
+// One kernel per RK stage (pn_tile_kernel on the FP64 tensor cores up to
+// order 6, pn_stage_kernel above): for each interior cell it applies the moment
 // filter to the stencil values as it loads them (moment_update.cpp:23-40
 // scales the interior in place before the ghost copy, so ghost strips that
 // hold interior copies are filtered too and the physical boundary's are not),
@@ -27,6 +28,7 @@
 using namespace clb;
 
 void clb_set_global_error(const char *msg);
+void clb_count_launches(long long k);
 
 namespace {
 
@@ -161,6 +163,133 @@ __global__ void __launch_bounds__(kPnWarps * 32) pn_stage_kernel(PnArgs a)
     }
 }
 
+// Orders up to 6 (n <= 32): tensor-core form of the same stage.  A CTA owns a
+// tile of kTI x kTJ interior cells; warp w owns row w of it, so the MMA's 16
+// rows are 16 cells along j.  The tile with its 2-cell halo is staged in
+// shared memory (filtered on load by the rule above, moments zero-padded to
+// NP), the four stencil combinations are formed directly as A fragments
+// (16 cells x 8 moments), and the operators, staged once per CTA, are the B
+// fragments: ew = T_xi+ Op_xi+^T + T_xi- Op_xi-^T (likewise ns) accumulate in
+// FP64 tensor-core MMAs.  Cell and operator rows are padded by 4 doubles so
+// the fragment loads spread over the banks.
+constexpr int kTI = 8, kTJ = 16;
+
+template <int NP>
+__global__ void __launch_bounds__(kTI * 32, 2) pn_tile_kernel(PnArgs a)
+{
+    constexpr int CS = NP + 4;   // doubles per cell in the tile
+    constexpr int OS = NP + 4;   // row stride of the staged operators
+    constexpr int RW = kTJ + 4;  // cells per tile row with the halo
+    constexpr int NT = NP / 8;
+    extern __shared__ double sm[];
+    double *ops = sm;                        // [4][NP][OS]: ops[(o*NP + i)*OS + k] = op_o[k][i]
+    double *tile = ops + 4 * NP * OS;        // [kTI+4][RW][CS]
+    const int n = a.n, tid = threadIdx.x;
+    for (int e = tid; e < 4 * NP * NP; e += blockDim.x) {
+        const int o = e / (NP * NP), r = e % (NP * NP), i = r / NP, k = r % NP;
+        ops[(o * NP + i) * OS + k] = (i < n && k < n) ? a.opsT[((size_t)o * n + i) * n + k] : 0.0;
+    }
+    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+    const int nx = a.NX - 4, ny = a.NY - 4;
+    const int tilesJ = (ny + kTJ - 1) / kTJ, tiles = ((nx + kTI - 1) / kTI) * tilesJ;
+    const size_t NY = a.NY;
+    for (int tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
+        const int i0 = 2 + (tl / tilesJ) * kTI, j0 = 2 + (tl % tilesJ) * kTJ;
+        __syncthreads();   // the previous tile's readers are done (and the operators staged)
+        for (int e = tid; e < (kTI + 4) * RW * NP; e += blockDim.x) {
+            const int k = e % NP, cell = e / NP, r = cell / RW, c = cell % RW;
+            const int gi = i0 - 2 + r, gj = j0 - 2 + c;
+            double v = 0.0;
+            if (k < n && gi < a.NX && gj < a.NY) {
+                v = a.in[((size_t)gi * NY + gj) * n + k];
+                if (a.filter && filtered_cell(a, gi, gj))
+                    v = __dmul_rn(v, a.filter[k]);
+            }
+            tile[cell * CS + k] = v;
+        }
+        __syncthreads();
+        const int ii = warp, i = i0 + ii;
+        auto T = [&](int r, int c, int m) { return tile[(r * RW + c) * CS + m]; };
+        double acc[2][NT][4];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int kt = 0; kt < NT; kt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    acc[h][kt][e] = 0.0;
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+#pragma unroll 1
+            for (int ic = 0; ic < NT; ic++) {
+                double av[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    // fragment element q: cell g (+8 for q = 1, 3), moment t (+4 for q >= 2)
+                    const int c = 2 + g + ((q & 1) ? 8 : 0), m = ic * 8 + t + ((q & 2) ? 4 : 0);
+                    const int r = ii + 2;
+                    if (o == 0)
+                        av[q] = stencil4(0.25, T(r + 1, c, m), 0.75, T(r, c, m), -1.25, T(r - 1, c, m), 0.25,
+                                         T(r - 2, c, m));
+                    else if (o == 1)
+                        av[q] = stencil4(-0.25, T(r + 2, c, m), 1.25, T(r + 1, c, m), -0.75, T(r, c, m), -0.25,
+                                         T(r - 1, c, m));
+                    else if (o == 2)
+                        av[q] = stencil4(0.25, T(r, c + 1, m), 0.75, T(r, c, m), -1.25, T(r, c - 1, m), 0.25,
+                                         T(r, c - 2, m));
+                    else
+                        av[q] = stencil4(-0.25, T(r, c + 2, m), 1.25, T(r, c + 1, m), -0.75, T(r, c, m), -0.25,
+                                         T(r, c - 1, m));
+                }
+                const double *ob = ops + (o * NP + ic * 8 + t) * OS + g;
+#pragma unroll
+                for (int kt = 0; kt < NT; kt++)
+                    dmma16x8x8(acc[o >> 1][kt], av[0], av[1], av[2], av[3], ob[kt * 8], ob[4 * OS + kt * 8]);
+            }
+        }
+        if (i >= a.NX - 2)
+            continue;
+        const double dt = a.dt;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int cj = j0 + g + ((e & 2) ? 8 : 0);
+            if (cj >= a.NY - 2)
+                continue;
+            const size_t cell = (size_t)i * NY + cj;
+            const double sT = a.sigT[cell], sS = a.sigS[cell];
+            bool source = false;
+            if (a.initCond == 1) {
+                const double x = __dadd_rn(a.initX, __dmul_rn((double)(i - 2), a.dx));
+                const double y = __dadd_rn(a.initY, __dmul_rn((double)(cj - 2), a.dy));
+                source = fabs(x) < 0.5 && fabs(y) < 0.5;
+            }
+            const double *self = tile + ((ii + 2) * RW + (cj - j0 + 2)) * CS;
+#pragma unroll
+            for (int kt = 0; kt < NT; kt++) {
+                const int k = kt * 8 + 2 * t + (e & 1);
+                if (k >= n)
+                    continue;
+                const double F = __dadd_rn(__dmul_rn(a.rdx, acc[0][kt][e]), __dmul_rn(a.rdy, acc[1][kt][e]));
+                double u;
+                if (k == 0) {
+                    const double gm = __dsub_rn(__dadd_rn(1.0, __dmul_rn(dt, sS)), __dmul_rn(dt, sT));
+                    u = __dsub_rn(__dmul_rn(self[0], gm), __dmul_rn(dt, F));
+                    if (source)
+                        u = __dadd_rn(u, __dmul_rn(__dmul_rn(dt, 2.0), kSqrtPiPn));
+                } else {
+                    u = __dsub_rn(__dmul_rn(self[k], __dsub_rn(1.0, __dmul_rn(dt, sT))), __dmul_rn(dt, F));
+                }
+                if (a.old)
+                    u = __dmul_rn(0.5, __dadd_rn(u, a.old[cell * n + k]));
+                a.out[cell * n + k] = u;
+            }
+        }
+    }
+}
+
+template <int NP>
+size_t pn_tile_smem() { return (size_t)(4 * NP * (NP + 4) + (kTI + 4) * (kTJ + 4) * (NP + 4)) * sizeof(double); }
+
 }  // namespace
 
 struct cl_pn {
@@ -213,11 +342,24 @@ static cudaError_t pn_launch(cl_pn *p, int stage, double dt, double dx, double d
     a.dy = dy;
     a.initX = p->grid.init_x;
     a.initY = p->grid.init_y;
-    const size_t smem = (size_t)4 * p->n * p->n * sizeof(double);
-    if (p->n <= 32)
-        pn_stage_kernel<1><<<p->nCtas, kPnWarps * 32, smem, p->stream>>>(a);
-    else
-        pn_stage_kernel<2><<<p->nCtas, kPnWarps * 32, smem, p->stream>>>(a);
+    const int np = (p->n + 7) / 8 * 8;
+    switch (np) {
+    case 8:
+        pn_tile_kernel<8><<<p->nCtas, kTI * 32, pn_tile_smem<8>(), p->stream>>>(a);
+        break;
+    case 16:
+        pn_tile_kernel<16><<<p->nCtas, kTI * 32, pn_tile_smem<16>(), p->stream>>>(a);
+        break;
+    case 24:
+        pn_tile_kernel<24><<<p->nCtas, kTI * 32, pn_tile_smem<24>(), p->stream>>>(a);
+        break;
+    case 32:
+        pn_tile_kernel<32><<<p->nCtas, kTI * 32, pn_tile_smem<32>(), p->stream>>>(a);
+        break;
+    default:
+        pn_stage_kernel<2><<<p->nCtas, kPnWarps * 32, (size_t)4 * p->n * p->n * sizeof(double), p->stream>>>(a);
+    }
+    clb_count_launches(1);
     return cudaGetLastError();
 }
 
@@ -271,24 +413,34 @@ int cl_pn_create(const cl_grid *grid, const cl_pn_setup *setup, const double *si
     cudaMemcpy(p->U, moments, C * n * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(p->V, moments, C * n * 8, cudaMemcpyHostToDevice);
     p->cur = p->U;
-    const size_t smem = 4 * n * n * 8;
-    cudaError_t e = cudaFuncSetAttribute(pn_stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pn_stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the kernel for this n, its shared memory, and the units it loops over
+    const int np = (int)(n + 7) / 8 * 8;
+    const void *fn = nullptr;
+    size_t smem = 0;
+    long long units = 0;
+    switch (np) {
+    case 8: fn = (const void *)pn_tile_kernel<8>; smem = pn_tile_smem<8>(); break;
+    case 16: fn = (const void *)pn_tile_kernel<16>; smem = pn_tile_smem<16>(); break;
+    case 24: fn = (const void *)pn_tile_kernel<24>; smem = pn_tile_smem<24>(); break;
+    case 32: fn = (const void *)pn_tile_kernel<32>; smem = pn_tile_smem<32>(); break;
+    default: fn = (const void *)pn_stage_kernel<2>; smem = 4 * n * n * 8;
+    }
+    const int threads = (np <= 32) ? kTI * 32 : kPnWarps * 32;
+    if (np <= 32)
+        units = (long long)((grid->nx + kTI - 1) / kTI) * ((grid->ny + kTJ - 1) / kTJ);
+    else
+        units = ((long long)grid->nx * grid->ny + kPnWarps - 1) / kPnWarps;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int occ = 0;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, n <= 32 ? (const void *)pn_stage_kernel<1>
-                                                                         : (const void *)pn_stage_kernel<2>,
-                                                          kPnWarps * 32, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess || occ < 1 || cudaDeviceSynchronize() != cudaSuccess) {
         p->err = std::string("set-up: ") + cudaGetErrorString(e != cudaSuccess ? e : cudaGetLastError());
         return pn_fail(p, CL_ERR_CUDA);
     }
-    const long long cells = (long long)grid->nx * grid->ny;
-    const long long want = (cells + kPnWarps - 1) / kPnWarps;
-    p->nCtas = (int)std::max<long long>(1, std::min<long long>(want, (long long)sms * occ));
+    p->nCtas = (int)std::max<long long>(1, std::min<long long>(units, (long long)sms * occ));
     *out = p;
     return CL_OK;
 }
@@ -338,8 +490,10 @@ int cl_pn_step(cl_pn *p, double dt, double dx, double dy)
     if (!p)
         return CL_ERR_ARG;
     for (int stage = 1; stage <= 2; stage++) {
-        if (p->grid.init_cond == 2)
+        if (p->grid.init_cond == 2) {
             PN_TRY(p, launch_ghost_periodic(p->cur, p->n, p->NX, p->NY, p->stream));
+            clb_count_launches(2);
+        }
         int rc = cl_pn_stage(p, stage, dt, dx, dy);
         if (rc)
             return rc;
@@ -399,7 +553,9 @@ int cl_pn_set_state(cl_pn *p, const double *moments)
         return CL_ERR_ARG;
     PN_TRY(p, cudaStreamSynchronize(p->stream));
     PN_TRY(p, cudaMemcpy(p->U, moments, (size_t)p->C * p->n * 8, cudaMemcpyHostToDevice));
-    PN_TRY(p, cudaMemcpy(p->V, moments, (size_t)p->C * p->n * 8, cudaMemcpyHostToDevice));
+    // the second buffer needs the ghost strips; the device copy is cheaper
+    // than a second upload
+    PN_TRY(p, cudaMemcpyAsync(p->V, p->U, (size_t)p->C * p->n * 8, cudaMemcpyDeviceToDevice, p->stream));
     p->cur = p->U;
     return CL_OK;
 }
@@ -422,6 +578,7 @@ static int pn_halo(cl_pn *p, double *const bufs[4], int pack)
     for (int s = 0; s < 4; s++)
         b.p[s] = bufs[s];
     PN_TRY(p, launch_halo(p->cur, p->n, p->NX, p->NY, b, pack, p->stream));
+    clb_count_launches(1);
     return CL_OK;
 }
 
