@@ -619,13 +619,15 @@ class NodeSolver(Solver):
     def pack(self):
         """getInnerBoundaries for the sides that have a peer."""
         sides = [k for k in SIDES if self.plan.peer[k] is not None]
-        _check(lib().cl_solver_halo_pack(self._s, self._ptrs(self.send, sides)), self._err)
+        if sides:
+            _check(lib().cl_solver_halo_pack(self._s, self._ptrs(self.send, sides)), self._err)
 
     def unpack(self):
         """setOuterBoundaries for the sides that have a peer (the peer of a
         side sends the strip for it)."""
         sides = [k for k in SIDES if self.plan.peer[k] is not None]
-        _check(lib().cl_solver_halo_unpack(self._s, self._ptrs(self.recv, sides)), self._err)
+        if sides:
+            _check(lib().cl_solver_halo_unpack(self._s, self._ptrs(self.recv, sides)), self._err)
 
     def stage(self, stage, dt):
         _check(lib().cl_solver_stage(self._s, stage, dt), self._err)

@@ -196,16 +196,29 @@ __global__ void __launch_bounds__(kTI * 32, 2) pn_tile_kernel(PnArgs a)
     for (int tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
         const int i0 = 2 + (tl / tilesJ) * kTI, j0 = 2 + (tl % tilesJ) * kTJ;
         __syncthreads();   // the previous tile's readers are done (and the operators staged)
-        for (int e = tid; e < (kTI + 4) * RW * NP; e += blockDim.x) {
-            const int k = e % NP, cell = e / NP, r = cell / RW, c = cell % RW;
-            const int gi = i0 - 2 + r, gj = j0 - 2 + c;
-            double v = 0.0;
-            if (k < n && gi < a.NX && gj < a.NY) {
-                v = a.in[((size_t)gi * NY + gj) * n + k];
-                if (a.filter && filtered_cell(a, gi, gj))
-                    v = __dmul_rn(v, a.filter[k]);
+        // staged in batches of 8 loads per thread, all issued before any is used
+        constexpr int kTileElems = (kTI + 4) * RW * NP, kStep = kTI * 32, kBatch = 8;
+        for (int e0 = tid; e0 < kTileElems; e0 += kBatch * kStep) {
+            double v[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                const int e = e0 + b * kStep;
+                const int k = e % NP, cell = e / NP, r = cell / RW, c = cell % RW;
+                const int gi = i0 - 2 + r, gj = j0 - 2 + c;
+                v[b] = (e < kTileElems && k < n && gi < a.NX && gj < a.NY) ? a.in[((size_t)gi * NY + gj) * n + k]
+                                                                          : 0.0;
             }
-            tile[cell * CS + k] = v;
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                const int e = e0 + b * kStep;
+                if (e >= kTileElems)
+                    continue;
+                const int k = e % NP, cell = e / NP, r = cell / RW, c = cell % RW;
+                double x = v[b];
+                if (a.filter && k < n && filtered_cell(a, i0 - 2 + r, j0 - 2 + c))
+                    x = __dmul_rn(x, a.filter[k]);
+                tile[cell * CS + k] = x;
+            }
         }
         __syncthreads();
         const int ii = warp, i = i0 + ii;
