@@ -141,7 +141,7 @@ def dist_setup():
     return world, rank, local
 
 
-def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1):
+def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1, contraction="pairs"):
     """The workload's deck; with nodes > 1 the grid and domain are widened
     nodes times in x and split into nodes x 1 partitions, so every node holds
     the workload's grid."""
@@ -152,8 +152,11 @@ def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1):
         kw["num_cells_x"] = kw["num_cells_x"] * nodes
         kw["b_x"] = kw.get("a_x", -1.5) + (kw.get("b_x", 1.5) - kw.get("a_x", -1.5)) * nodes
         kw["partitions"] = (nodes, 1)
+    kw["extra"] = {}
     if precision == "mixed":
-        kw["extra"] = {"MOMOPT_GPU_PRECISION": "mixed"}
+        kw["extra"]["MOMOPT_GPU_PRECISION"] = "mixed"
+    if contraction == "single":
+        kw["extra"]["MOMOPT_GPU_CONTRACTION"] = "single"
     decks.write_deck(path, decks.deck_text(**kw))
     return path
 
@@ -306,7 +309,8 @@ def native_arm(args, world, rank, local):
         dist.barrier()
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
-    deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world)
+    deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world,
+                      contraction=args.contraction)
     partitioned = world > 1 or args.partitioned
     if partitioned:
         solver = cb.NodeSolver(deck, tmp, node=rank, num_nodes=world)
@@ -462,6 +466,7 @@ def native_arm(args, world, rank, local):
                        "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
                        "moment_type": w["moment_type"] if "moment_type" in w else "mn",
                        "newton": args.newton, "precision": args.precision, "opt_type": args.opt_type,
+                       "contraction": args.contraction,
                        "t_start": args.warmup * dt,
                        "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
                        "parallelism": ("halo %dx1 (NCCL point-to-point before each RK stage)" % world)
@@ -823,6 +828,9 @@ def main():
     ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1, 2],
                     help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton, "
                          "2: BFGS sub-iterations in the change of basis)")
+    ap.add_argument("--contraction", default="pairs", choices=["pairs", "single"],
+                    help="grid workloads: the quadrature directions phi, phi + pi contracted together "
+                         "through the basis parity (default) or one at a time (MOMOPT_GPU_CONTRACTION)")
     ap.add_argument("--partitioned", action="store_true",
                     help="grid workloads: step through the partitioned (halo-exchange) path even "
                          "on one GPU, as a 1 x 1 partition")

@@ -25,6 +25,7 @@ CL_OK, CL_ERR_ARG, CL_ERR_CUDA, CL_ERR_U0, CL_ERR_MAXREG, CL_ERR_TIMEOUT, CL_ERR
 CL_MN, CL_PPN = 0, 1
 CL_FP64, CL_MIXED = 0, 1
 CL_SOLVER_MOMOPT, CL_SOLVER_MOMENT = 0, 1
+CL_CONTRACT_PAIRS, CL_CONTRACT_SINGLE = 0, 1
 REGULARIZATIONS = (0.0, 1e-3, 1e-2, 1e-1, 5e-1)
 
 
@@ -47,7 +48,7 @@ class cl_options(C.Structure):
     _fields_ = [("moment_type", C.c_int), ("opt_type", C.c_int), ("max_iter", C.c_int),
                 ("tol", C.c_double), ("cond_h_max", C.c_double), ("delta_ppn", C.c_double),
                 ("tol_gamma", C.c_double), ("precision", C.c_int), ("max_bfgs_iter", C.c_int),
-                ("cond_h_max_bfgs", C.c_double)]
+                ("cond_h_max_bfgs", C.c_double), ("contraction", C.c_int)]
 
 
 class cl_grid(C.Structure):
@@ -246,9 +247,10 @@ class Angular:
 
 
 def make_options(moment_type=CL_MN, max_iter=100, tol=1e-8, cond_h_max=1e10, delta_ppn=1e-10,
-                 tol_gamma=0.0, precision=CL_FP64, opt_type=0, max_bfgs_iter=5, cond_h_max_bfgs=20.0):
+                 tol_gamma=0.0, precision=CL_FP64, opt_type=0, max_bfgs_iter=5, cond_h_max_bfgs=20.0,
+                 contraction=0):
     return cl_options(moment_type, opt_type, max_iter, tol, cond_h_max, delta_ppn, tol_gamma,
-                      precision, max_bfgs_iter, cond_h_max_bfgs)
+                      precision, max_bfgs_iter, cond_h_max_bfgs, contraction)
 
 
 class Context:

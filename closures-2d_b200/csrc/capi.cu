@@ -39,6 +39,12 @@ int round_up(int x, int m) { return (x + m - 1) / m * m; }
 // Device copy of one moment order's angular data in the kernels' layouts.
 struct DeviceBasis {
     int n = 0, n2 = 0, nq = 0, nb = 0, K2p = 0, nqp = 0, ldP = 0, ldPf = 0, useGaunt = 0;
+    int nqpF = 0;                                  // flux rows (all directions)
+    // direction pairs (Newton layout): basis and Hessian columns grouped by
+    // degree parity, even group first (nbe, K2e columns, multiples of 8)
+    int paired = 0, nbe = 0, K2e = 0;
+    short *binv = nullptr;                         // [nb] moment of each basis column, -1 padding
+    int *pcol = nullptr;                           // [n(n+1)/2] G column of each product (no Gaunt)
     double p0 = 0;
     double *P = nullptr, *w = nullptr;            // Newton layout
     double *Pf = nullptr, *xi = nullptr, *eta = nullptr, *cxw = nullptr, *cyw = nullptr;  // flux
@@ -67,6 +73,8 @@ struct DeviceBasis {
         cudaFree(ellIdx);
         cudaFree(ellVal);
         cudaFree(ellOff);
+        cudaFree(binv);
+        cudaFree(pcol);
         *this = DeviceBasis();
     }
 };
@@ -82,44 +90,105 @@ cudaError_t upload(T **dst, const std::vector<T> &src)
     return e;
 }
 
+// Degree of each z-even harmonic in the basis order (degree l has l + 1).
+static void harmonic_degrees(int count, std::vector<int> &deg)
+{
+    deg.resize(count);
+    int k = 0;
+    for (int l = 0; k < count; l++)
+        for (int m = 0; m <= l && k < count; m++)
+            deg[k++] = l;
+}
+
+// Columns of one group layout: even-parity entries first, then odd, each
+// group padded to a multiple of 8; col[i] = position of entry i.
+static void parity_columns(const std::vector<int> &deg, int paired, std::vector<int> &col, int &evenCols,
+                           int &total)
+{
+    const int cnt = (int)deg.size();
+    col.resize(cnt);
+    if (!paired) {
+        for (int i = 0; i < cnt; i++)
+            col[i] = i;
+        evenCols = 0;
+        total = round_up(cnt, 8);
+        return;
+    }
+    int ne = 0;
+    for (int i = 0; i < cnt; i++)
+        ne += (deg[i] % 2 == 0);
+    evenCols = round_up(ne, 8);
+    int ie = 0, io = 0;
+    for (int i = 0; i < cnt; i++)
+        col[i] = (deg[i] % 2 == 0) ? ie++ : evenCols + io++;
+    total = evenCols + round_up(cnt - ne, 8);
+}
+
 // n, n2, nq, w, xi, eta, p[nq*n2], Gaunt CSR -> device layouts.
+//
+// Newton layout with `paired`: the directions phi and phi + pi of one
+// Gauss-Legendre level (q and q + Q in the reference's order, momopt_init.cpp
+// :181-186) have the same weight and basis values equal up to the degree
+// parity, p_l(q + Q) = (-1)^l p_l(q) (for the Gaunt basis and for products
+// likewise).  Only the first direction of each pair is stored, with the
+// columns grouped by parity, and the kernel evaluates both directions from
+// the two half sums alpha_even . p_even +- alpha_odd . p_odd.
 cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGaunt, const double *w,
                                const double *xi, const double *eta, const double *p, const int *goff,
-                               const int *gidx, const double *gval, int gnnz)
+                               const int *gidx, const double *gval, int gnnz, int paired = 0)
 {
     B.n = n;
     B.n2 = n2;
     B.nq = nq;
     B.useGaunt = useGaunt;
-    B.nb = round_up(n, 8);
+    const int Q = (int)std::lround(std::sqrt((double)nq));
+    if (paired && (Q * Q != nq || Q % 2 != 0))
+        paired = 0;
+    B.paired = paired;
     const int K2 = useGaunt ? n2 : n * (n + 1) / 2;
-    B.K2p = round_up(K2, 8);
-    B.nqp = round_up(nq, 32);
+    std::vector<unsigned short> prod(n * (n + 1) / 2);
+    product_columns(n, prod.data());
+    std::vector<int> degB, degH, colB, colH;
+    harmonic_degrees(n, degB);
+    if (useGaunt) {
+        harmonic_degrees(n2, degH);
+    } else {
+        degH.resize(K2);
+        for (int c = 0; c < K2; c++)
+            degH[c] = degB[prod[c] >> 8] + degB[prod[c] & 255];
+    }
+    parity_columns(degB, paired, colB, B.nbe, B.nb);
+    parity_columns(degH, paired, colH, B.K2e, B.K2p);
+    const int rows = paired ? nq / 2 : nq;
+    B.nqp = round_up(rows, 32);
+    B.nqpF = round_up(nq, 32);
     int ldP = B.nb + B.K2p;
     while (ldP % 16 != 4)
         ldP++;
     B.ldP = ldP;
-    B.ldPf = B.nb + 4;
+    B.ldPf = round_up(n, 8) + 4;
     B.p0 = p[0];
     std::vector<double> P((size_t)B.nqp * ldP + B.nqp, 0.0), W(B.nqp, 0.0);
-    std::vector<unsigned short> prod(n * (n + 1) / 2);
-    product_columns(n, prod.data());
-    std::vector<double> Pf((size_t)B.nqp * B.ldPf, 0.0), XI(B.nqp, 0.0), ET(B.nqp, 0.0), CX(B.nqp, 0.0),
-        CY(B.nqp, 0.0);
-    for (int q = 0; q < nq; q++) {
+    for (int r = 0; r < rows; r++) {
+        const int q = paired ? (r / Q) * 2 * Q + r % Q : r;
         const double *pq = p + (size_t)q * n2;
-        double *row = &P[(size_t)basis_row(q, ldP)];
+        double *row = &P[(size_t)basis_row(r, ldP)];
         for (int k = 0; k < n; k++)
-            row[k] = pq[k];
+            row[colB[k]] = pq[k];
         if (useGaunt) {
             for (int k = 0; k < n2; k++)
-                row[B.nb + k] = pq[k];
+                row[B.nb + colH[k]] = pq[k];
         } else {
-            for (int c = 0; c < n * (n + 1) / 2; c++)
-                row[B.nb + c] = pq[prod[c] >> 8] * pq[prod[c] & 255];
+            for (int c = 0; c < K2; c++)
+                row[B.nb + colH[c]] = pq[prod[c] >> 8] * pq[prod[c] & 255];
         }
-        W[q] = w[q];
-        P[(size_t)basis_wgap(q, ldP)] = w[q];
+        W[r] = w[q];
+        P[(size_t)basis_wgap(r, ldP)] = w[q];
+    }
+    std::vector<double> Pf((size_t)B.nqpF * B.ldPf, 0.0), XI(B.nqpF, 0.0), ET(B.nqpF, 0.0), CX(B.nqpF, 0.0),
+        CY(B.nqpF, 0.0);
+    for (int q = 0; q < nq; q++) {
+        const double *pq = p + (size_t)q * n2;
         for (int k = 0; k < n; k++)
             Pf[(size_t)q * B.ldPf + k] = pq[k];
         XI[q] = xi[q];
@@ -137,6 +206,16 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
     if ((e = upload(&B.cxw, CX)) != cudaSuccess) return e;
     if ((e = upload(&B.cyw, CY)) != cudaSuccess) return e;
     if ((e = upload(&B.pairs, pairs)) != cudaSuccess) return e;
+    if (paired) {
+        std::vector<short> binv(B.nb, (short)-1);
+        for (int k = 0; k < n; k++)
+            binv[colB[k]] = (short)k;
+        if ((e = upload(&B.binv, binv)) != cudaSuccess) return e;
+        if (!useGaunt) {
+            std::vector<int> pcol(colH.begin(), colH.end());
+            if ((e = upload(&B.pcol, pcol)) != cudaSuccess) return e;
+        }
+    }
     if (useGaunt) {
         std::vector<int> off(goff, goff + n * n + 1), idx(gidx, gidx + gnnz);
         std::vector<double> val(gval, gval + gnnz);
@@ -147,20 +226,44 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         std::vector<unsigned short> epair(chunks * 32), eidx((size_t)maxRows * 32);
         std::vector<double> eval((size_t)maxRows * 32);
         std::vector<int> eoff(chunks + 1);
-        int rows = build_gaunt_ell(n, goff, gidx, gval, epair.data(), eidx.data(), eval.data(), eoff.data(),
-                                   maxRows);
-        if (rows < 0)
+        int rows2 = build_gaunt_ell(n, goff, gidx, gval, epair.data(), eidx.data(), eval.data(), eoff.data(),
+                                    maxRows);
+        if (rows2 < 0)
             return cudaErrorInvalidValue;
-        eidx.resize((size_t)rows * 32);
-        eval.resize((size_t)rows * 32);
+        eidx.resize((size_t)rows2 * 32);
+        eval.resize((size_t)rows2 * 32);
+        for (auto &x : eidx)   // G columns in the layout's order
+            x = (unsigned short)colH[x];
         B.ellChunks = chunks;
-        B.ellRows = rows;
+        B.ellRows = rows2;
         if ((e = upload(&B.ellPair, epair)) != cudaSuccess) return e;
         if ((e = upload(&B.ellIdx, eidx)) != cudaSuccess) return e;
         if ((e = upload(&B.ellVal, eval)) != cudaSuccess) return e;
         if ((e = upload(&B.ellOff, eoff)) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// Direction-pair layout counts: column tiles and k-steps of the fused
+// evaluation (the exact-instance key), without building anything.
+static void paired_counts(int n, int n2, int useGaunt, int &nt, int &nbk)
+{
+    std::vector<int> degB, degH, col;
+    std::vector<unsigned short> prod(n * (n + 1) / 2);
+    product_columns(n, prod.data());
+    harmonic_degrees(n, degB);
+    if (useGaunt) {
+        harmonic_degrees(n2, degH);
+    } else {
+        degH.resize(prod.size());
+        for (size_t c = 0; c < prod.size(); c++)
+            degH[c] = degB[prod[c] >> 8] + degB[prod[c] & 255];
+    }
+    int even = 0, nb = 0, k2 = 0;
+    parity_columns(degB, 1, col, even, nb);
+    parity_columns(degH, 1, col, even, k2);
+    nt = k2 / 8;
+    nbk = nb / 8;
 }
 
 NewtonProblem make_problem(const DeviceBasis &B)
@@ -185,6 +288,11 @@ NewtonProblem make_problem(const DeviceBasis &B)
     pb.K2p = B.K2p;
     pb.nqp = B.nqp;
     pb.ldP = B.ldP;
+    pb.paired = B.paired;
+    pb.nbe = B.nbe;
+    pb.K2e = B.K2e;
+    pb.binv = B.binv;
+    pb.pcol = B.pcol;
     return pb;
 }
 
@@ -206,6 +314,10 @@ int check_options(const cl_options *o, std::string &err)
     }
     if (o->moment_type != CL_MN && o->moment_type != CL_PPN) {
         err = "moment type out of range";
+        return CL_ERR_ARG;
+    }
+    if (o->contraction != CL_CONTRACT_PAIRS && o->contraction != CL_CONTRACT_SINGLE) {
+        err = "contraction must be CL_CONTRACT_PAIRS or CL_CONTRACT_SINGLE";
         return CL_ERR_ARG;
     }
     if (o->precision != CL_FP64 && o->precision != CL_MIXED) {
@@ -401,9 +513,17 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     // degree-N basis rows and sums products, which is the same Hessian in
     // exact arithmetic.
     const int gauntNewton = ang->use_gaunt;
+    // direction pairs where a fused instance takes the paired layout (Mn,
+    // FP64, the default contraction)
+    int paired = 0;
+    if (opts->moment_type == CL_MN && opts->precision == CL_FP64 && opts->contraction == CL_CONTRACT_PAIRS) {
+        int pnt = 0, pnbk = 0;
+        paired_counts(ang->n, ang->n2, gauntNewton, pnt, pnbk);
+        paired = newton_pair_supported(pnt, pnbk) ? 1 : 0;
+    }
     cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi,
                                         ang->eta, ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
-                                        ang->gaunt_nnz);
+                                        ang->gaunt_nnz, paired);
     if (ce != cudaSuccess) {
         ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
         return ctx_fail(ctx, CL_ERR_CUDA);
@@ -455,7 +575,22 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         a.prob[0].P2M = ctx->dP2M;
         a.prob[0].alphaP = ctx->dAlphaP;
     }
-    const int pl = plan_newton(a);
+    int pl = plan_newton(a);
+    if (ctx->B.paired && (pl != 0 || a.ntf == 0 || a.ntExact == 0)) {
+        // the paired layout only runs fused: keep one direction at a time
+        ctx->B.release();
+        if ((ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi, ang->eta,
+                                     ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val, ang->gaunt_nnz,
+                                     0)) != cudaSuccess) {
+            ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
+            return ctx_fail(ctx, CL_ERR_CUDA);
+        }
+        NewtonProblem keep = a.prob[0];
+        a.prob[0] = make_problem(ctx->B);
+        a.prob[0].P2M = keep.P2M;
+        a.prob[0].alphaP = keep.alphaP;
+        pl = plan_newton(a);
+    }
     if (pl != 0) {
         ctx->err = pl == -2 ? "mixed precision needs a configuration with at most 16 Hessian column tiles"
                             : "Newton kernel layout does not fit in shared memory";
@@ -486,9 +621,9 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     f.cxw = ctx->B.cxw;
     f.cyw = ctx->B.cyw;
     f.n = ctx->n;
-    f.nb = ctx->B.nb;
+    f.nb = round_up(ctx->n, 8);   // the flux basis keeps the moment order
     f.ldPf = ctx->B.ldPf;
-    f.nqp = ctx->B.nqp;
+    f.nqp = ctx->B.nqpF;
     f.NX = ctx->NX;
     f.NY = ctx->NY;
     f.momentType = opts->moment_type;

@@ -120,6 +120,12 @@ static cudaError_t run(const NewtonArgs &a, int grid, cudaStream_t stream, int m
             return e;
         return cudaErrorInvalidValue;
     }
+    if (a.nprob == 1 && a.prob[0].paired) {
+        // the direction-pair layout runs only its own fused instances
+        if (a.ntf > 0 && a.ntExact > 0 && newton_run_exact_pair(a, grid, stream, mode, occ, &e))
+            return e;
+        return cudaErrorInvalidValue;
+    }
     if (a.ntf > 0 && a.ntExact > 0) {
         if (newton_run_exact_mn_a(a, grid, stream, mode, occ, &e) ||
             newton_run_exact_mn_b(a, grid, stream, mode, occ, &e) ||

@@ -38,6 +38,13 @@ struct NewtonProblem {
     int ellChunks, ellRows;
     double p0;                  // p[0] = Y_00 (fobj.cpp:305 divides by it)
     int n, nb, K2p, nqp, ldP;
+    // direction pairs: the basis stores one direction of each (phi, phi + pi)
+    // pair with its columns grouped by degree parity (nbe even basis columns,
+    // K2e even Hessian columns, each group padded to 8); binv[j] is the moment
+    // of basis column j (-1 padding), pcol[c] the G column of product c
+    int paired, nbe, K2e;
+    const short *binv;
+    const int *pcol;
     int count;                  // vectors to solve
     double *u, *alpha;          // [count][n]; alpha: start (or fallback start) in, solution out
     const double *alphaStart;   // nullable [count][n]: predicted start; alpha is then the
@@ -94,6 +101,8 @@ struct NewtonArgs {
 int plan_newton(NewtonArgs &a);
 // Sets the kernel's shared-memory attribute (call once, outside capture).
 cudaError_t prepare_newton(const NewtonArgs &a);
+// A fused instance exists for the direction-pair layout with these counts.
+bool newton_pair_supported(int nt, int nbk);
 // Launches the persistent kernel on `stream` over `grid` CTAs.
 cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream);
 int newton_ctas_per_sm(const NewtonArgs &a);
@@ -103,6 +112,7 @@ int newton_ctas_per_sm(const NewtonArgs &a);
 // running it (mode 0 launch, 1 shared-memory attribute, 2 occupancy).
 bool newton_run_generic(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_mn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_pair(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_mn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);

@@ -505,7 +505,7 @@ __device__ __forceinline__ void hessian_from_contractions(const NewtonArgs &a, c
         for (int pi = lane; pi < npairs; pi += 32) {
             unsigned short pr = pb.pairs[pi];
             int i = pr >> 8, j = pr & 255;
-            double v = Gs[pi];
+            double v = Gs[pb.pcol ? pb.pcol[pi] : pi];
             Hs[i * ldh + j] = v;
             Hs[j * ldh + i] = v;
         }
@@ -1424,10 +1424,18 @@ __device__ void slot_logic_cb(const NewtonArgs &a, const NewtonProblem &pb, Layo
 // buffers keep one chunk in flight while two are read.
 constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on any wait for a staged chunk
 
-template <int NTF, int PPN, int NT, int NBK, int MIX>
+// PAIR (Mn, FP64): the chunk's rows are one direction q of each (phi,
+// phi + pi) pair and the columns are grouped by degree parity.  GEMM1 forms
+// the even and odd half sums S_e, S_o of alpha . p(q); the pair's exponents
+// are S_e + S_o (direction q) and S_e - S_o (its partner, whose basis values
+// are p(q) with the odd ones negated), and GEMM2 takes their weighted sum as
+// the A operand of the even column tiles and their difference for the odd
+// ones.  Each MMA so serves two directions.
+template <int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0>
 __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int tid,
                                               int lane, int warp, unsigned &mbPhase)
 {
+    static_assert(!PAIR || (PPN == 0 && MIX == 0), "direction pairs: Mn in FP64");
     const int g = lane >> 2, t4 = lane & 3;
     const int kq = a.kq, ldv = a.ldv, ldG = a.ldG;
     const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
@@ -1493,21 +1501,68 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     const int wOff = basis_wgap(qb, ldP);   // weights of rows qb, qb + 1
     const int offB = basis_row(qb, ldP) + g;   // rows qb and qb + 1 share the gap
 
-    // S block of chunk c (the staged copy at Pb)
-    auto gemm1 = [&](const double *Pb, double (&cs)[4]) {
+    // PAIR: the moment of this lane's A columns in each k-step (-1: padding)
+    int kb0[PAIR ? KSL : 1], kb1[PAIR ? KSL : 1];
+    if constexpr (PAIR) {
+#pragma unroll
+        for (int ks = 0; ks < KSL; ks++) {
+            kb0[ks] = pb.binv[ks * 8 + t4];
+            kb1[ks] = pb.binv[ks * 8 + t4 + 4];
+        }
+    }
+    const int nbe = pb.nbe, K2e = pb.K2e;
+    // S block of chunk c (the staged copy at Pb); PAIR: even half sums in
+    // cs, odd ones in co
+    auto gemm1 = [&](const double *Pb, double (&cs)[4], double (&co)[4]) {
         cs[0] = cs[1] = cs[2] = cs[3] = 0.0;
+        co[0] = co[1] = co[2] = co[3] = 0.0;
         const double *B1 = Pb + offA;
 #pragma unroll
-        for (int ks = 0; ks < KSL; ks++)
-            if (NBK > 0 || ks * 8 < nb)
+        for (int ks = 0; ks < KSL; ks++) {
+            if constexpr (PAIR) {
+                const double *Ar0 = L.alpha + r0 * ldv, *Ar1 = L.alpha + r1 * ldv;
+                const int k0 = kb0[ks], k1 = kb1[ks];
+                const double x0 = (k0 >= 0) ? Ar0[k0] : 0.0, x1 = (k0 >= 0) ? Ar1[k0] : 0.0;
+                const double x2 = (k1 >= 0) ? Ar0[k1] : 0.0, x3 = (k1 >= 0) ? Ar1[k1] : 0.0;
+                if (ks * 8 < nbe)
+                    dmma16x8x8(cs, x0, x1, x2, x3, B1[ks * 8 + t4], B1[ks * 8 + t4 + 4]);
+                else
+                    dmma16x8x8(co, x0, x1, x2, x3, B1[ks * 8 + t4], B1[ks * 8 + t4 + 4]);
+            } else if (NBK > 0 || ks * 8 < nb) {
                 dmma16x8x8(cs, A0[ks * 8], A1[ks * 8], A0[ks * 8 + 4], A1[ks * 8 + 4], B1[ks * 8 + t4],
                            B1[ks * 8 + t4 + 4]);
+            }
+        }
     };
     // e[h]: Hessian weights, eg[h]: PPn gradient weights; h = 0..3 is
     // (slot r0, row qb), (r0, qb + 1), (r1, qb), (r1, qb + 1) of chunk c
-    auto weights = [&](const double *Pc, const double (&cs)[4], double (&e)[4], double (&eg)[4]) {
+    // PAIR: e receives the pair sums of the weights (even tiles) and eg the
+    // differences (odd tiles)
+    auto weights = [&](const double *Pc, const double (&cs)[4], const double (&co)[4], double (&e)[4],
+                       double (&eg)[4]) {
         const double w0 = Pc[wOff], w1 = Pc[wOff + 1];   // staged with the chunk
-        if constexpr (PPN == 0) {
+        if constexpr (PAIR) {
+            double sv[8], x[8];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                sv[h] = cs[h] + co[h];
+                sv[4 + h] = cs[h] - co[h];
+            }
+            fast_exp_n<8>(x, sv, L.exptab, invL, L1, L2);
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const double ww = (h & 1) ? w1 : w0;
+                x[h] *= ww;
+                x[4 + h] *= ww;
+            }
+            facc0 += (x[0] + x[1]) + (x[4] + x[5]);
+            facc1 += (x[2] + x[3]) + (x[6] + x[7]);
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                e[h] = x[h] + x[4 + h];
+                eg[h] = x[h] - x[4 + h];
+            }
+        } else if constexpr (PPN == 0) {
             fast_exp_n<4>(e, cs, L.exptab, invL, L1, L2);
             e[0] *= w0;
             e[1] *= w1;
@@ -1548,9 +1603,9 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
         return abandon();
     double e[4], eg[4];
     {
-        double cs[4];
-        gemm1(L.P, cs);
-        weights(L.P, cs, e, eg);
+        double cs[4], co[4];
+        gemm1(L.P, cs, co);
+        weights(L.P, cs, co, e, eg);
     }
     // G += E . Phess for the chunk staged at Pc (E: weights held in e, eg)
     auto gemm2 = [&](const double *Pc) {
@@ -1574,8 +1629,10 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
                     tmma16x8x8(acc32[nt], ah[0], ah[2], ah[1], ah[3], bl0, bl1);
                     tmma16x8x8(acc32[nt], ah[0], ah[2], ah[1], ah[3], bh0, bh1);
                 } else {
-                    const double x0 = hess ? e[0] : eg[0], x1 = hess ? e[1] : eg[1];
-                    const double x2 = hess ? e[2] : eg[2], x3 = hess ? e[3] : eg[3];
+                    // PAIR: even column tiles take the sums, odd ones the differences
+                    const bool useE = PAIR ? (nt * 8 < K2e) : hess;
+                    const double x0 = useE ? e[0] : eg[0], x1 = useE ? e[1] : eg[1];
+                    const double x2 = useE ? e[2] : eg[2], x3 = useE ? e[3] : eg[3];
                     dmma16x8x8(acc[nt], x0, x2, x1, x3, B2[col], B2[col + ldP]);
                 }
             }
@@ -1590,10 +1647,10 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
             return abandon();
         if (c + 2 < nchunks)
             load_chunk(c + 2, bf);
-        double cs[4];
-        gemm1(L.P + bn * chunkDoubles, cs);
+        double cs[4], co[4];
+        gemm1(L.P + bn * chunkDoubles, cs, co);
         gemm2(L.P + bc * chunkDoubles);
-        weights(L.P + bn * chunkDoubles, cs, e, eg);
+        weights(L.P + bn * chunkDoubles, cs, co, e, eg);
         bc = bn;
     }
     gemm2(L.P + bc * chunkDoubles);   // the last chunk (waited for by the last iteration)
@@ -1640,7 +1697,7 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     return true;
 }
 
-template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX>
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0>
 __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
 {
     extern __shared__ __align__(16) double sm[];
@@ -1744,7 +1801,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
         // ---- phase A: evaluation contractions over the quadrature
         if constexpr (NTF > 0) {
-            if (!phase_a_fused<NTF, PPN, NT, NBK, MIX>(a, pb, L, tid, lane, warp, mbPhase))
+            if (!phase_a_fused<NTF, PPN, NT, NBK, MIX, PAIR>(a, pb, L, tid, lane, warp, mbPhase))
                 return;   // a staged chunk never arrived (error recorded)
         } else {
         const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
@@ -1904,10 +1961,10 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
 // One kernel instance: mode 0 launches it, 1 sets its shared-memory limit,
 // 2 writes its resident CTAs per SM to *occ.
-template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX = 0>
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX = 0, int PAIR = 0>
 cudaError_t newton_run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
 {
-    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK, MIX>;
+    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK, MIX, PAIR>;
     if (mode == 1)
         return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smemBytes);
     if (mode == 2) {

@@ -65,6 +65,10 @@ int MomOptGpuSolver::tryInit(double dx, double dy, double *maxDtOut)
     m_opt.precision = CL_FP64;
     if (d.get("MOMOPT_GPU_PRECISION", prec) && prec == "mixed")
         m_opt.precision = CL_MIXED;
+    std::string contraction;
+    m_opt.contraction = CL_CONTRACT_PAIRS;
+    if (d.get("MOMOPT_GPU_CONTRACTION", contraction) && contraction == "single")
+        m_opt.contraction = CL_CONTRACT_SINGLE;
 
     m_maxDt = cfl * (2.0 / (2.0 + theta)) * (dx * dy) / (dx + dy);   // momopt_init.cpp:72
     if (maxDtOut)

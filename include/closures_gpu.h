@@ -89,7 +89,14 @@ typedef struct {
     int precision;          /* CL_FP64 or CL_MIXED */
     int max_bfgs_iter;      /* MOMOPT_MAX_BFGS_ITER (opt_type 2, >= 1) */
     double cond_h_max_bfgs; /* MOMOPT_COND_H_MAX_BFGS (opt_type 2) */
+    int contraction;        /* CL_CONTRACT_PAIRS (default): the quadrature
+                               directions phi and phi + pi share one
+                               contraction through the degree parity of the
+                               basis, where supported (Mn, FP64);
+                               CL_CONTRACT_SINGLE: every direction on its own.
+                               The same sums in another order. */
 } cl_options;
+enum { CL_CONTRACT_PAIRS = 0, CL_CONTRACT_SINGLE = 1 };
 
 /* Grid description: Solver fields of solver.h:15-61 for one node. */
 typedef struct {
@@ -345,7 +352,9 @@ int cl_run_deck(const char *deck_path, const char *out_dir, int max_steps);
  * array's device address; make that first call before any stream capture.
  * All calls share the array, so calls that overlap on the GPU (several
  * streams or threads at once) race; the call waits for its own work on
- * `stream` (a cudaStream_t, null = legacy default stream) before returning. */
+ * `stream` (a cudaStream_t, null = legacy default stream) before returning.
+ * It contracts one quadrature direction at a time (the CL_CONTRACT_SINGLE
+ * sums) whatever opts->contraction holds. */
 int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *opts, int count,
                            double *d_u, double *d_alpha, int *d_iters, double *d_reg,
                            int *d_status, void *stream);

@@ -42,11 +42,11 @@ def _start(a, count, moment_type, u, alpha_exact, warm, seed):
 
 
 def _batch_case(order, Q, gaunt, count, moment_type=cb.CL_MN, tol=1e-8, seed=7, s_range=(0.1, 20.0),
-                warm=False, envelope=False):
+                warm=False, envelope=False, contraction=cb.CL_CONTRACT_PAIRS):
     a = cb.Angular(order, Q, gaunt)
     u, alpha_exact = cb.sample_moment_vectors(a, count, seed=seed, s_range=s_range)
     alpha0 = _start(a, count, moment_type, u, alpha_exact, warm, seed)
-    opts = cb.make_options(moment_type=moment_type, tol=tol)
+    opts = cb.make_options(moment_type=moment_type, tol=tol, contraction=contraction)
     ctx = cb.Context.for_batches(a, opts)
     res = {}
     u_g, a_g = u.copy(), alpha0.copy()
@@ -77,7 +77,20 @@ BATCH_CASES = [(1, 20, 0), (2, 20, 0), (2, 20, 1), (3, 30, 1), (4, 30, 0), (4, 4
 @pytest.mark.parametrize("s_max", [2.0, 20.0])
 @pytest.mark.parametrize("order,Q,gaunt", BATCH_CASES)
 def test_batch_matches_oracle(order, Q, gaunt, s_max):
-    a, r, _ = _batch_case(order, Q, gaunt, 700, s_range=(0.1, s_max), envelope=True)
+    """Default contraction: Mn orders whose fused instance takes the
+    direction-pair layout run it."""
+    _check_batch(*_batch_case(order, Q, gaunt, 700, s_range=(0.1, s_max), envelope=True)[:2])
+
+
+@pytest.mark.parametrize("order,Q,gaunt", [(2, 20, 1), (3, 30, 0), (4, 30, 0), (6, 40, 1)])
+def test_batch_single_contraction_matches_oracle(order, Q, gaunt):
+    """One direction at a time (CL_CONTRACT_SINGLE), the layout the
+    direction pairs replace by default."""
+    _check_batch(*_batch_case(order, Q, gaunt, 700, s_range=(0.1, 20.0), envelope=True,
+                              contraction=cb.CL_CONTRACT_SINGLE)[:2])
+
+
+def _check_batch(a, r):
     g, o, f = r["gpu"], r["oracle"], r["fma"]
     n_go = int((~_agree(g, o)).sum())
     n_fo = int((~_agree(f, o)).sum())

@@ -27,7 +27,8 @@ def _reference_and_noalloc(order, Q, gaunt, count, seed):
     a = cb.Angular(order, Q, gaunt)
     u, _ = cb.sample_moment_vectors(a, count, seed=seed, s_range=(0.1, 2.0))
     alpha0 = cb.isotropic_alpha(a.n, count)
-    opts = cb.make_options(tol=1e-8)
+    # one direction at a time, as the allocation-free entry point contracts
+    opts = cb.make_options(tol=1e-8, contraction=cb.CL_CONTRACT_SINGLE)
     # the existing, allocating entry point
     u_ref, a_ref = u.copy(), alpha0.copy()
     ctx = cb.Context.for_batches(a, opts)
