@@ -251,9 +251,12 @@ def reference_arm(args, world, rank):
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture of this workload (profiles/newton_kernel_m6_800.md); the algorithmic
-# state traffic of that launch is 290 MB read + 433 MB written.
-NCU_TRAFFIC = {("m6_800", "newton"): 672.4e6}
+# capture of the workload: newton on m6_800 (profiles/newton_kernel_m6_800.md;
+# algorithmic state traffic of that launch 290 MB read + 433 MB written) and
+# a stage-1 pn_stage launch on pn6_800 (profiles/pn_tile_kernel_pn6_800.md;
+# algorithmic 2n doubles + 16 bytes per cell = 297 MB, part of the read
+# served by L2 from the stage before).
+NCU_TRAFFIC = {("m6_800", "newton"): 670.6e6, ("pn6_800", "pn_stage"): 255.6e6}
 
 
 def train_grid_mlp(cb, torch, w, n, harvest, args):
@@ -645,7 +648,8 @@ def pn_arm(args, world, rank, local):
                        if world > 1 else "single"},
             "kernel_ms": {"pn_stage": stage_ms, "halo_exchange": exchange_ms},
             "roofline": {"bound": "fp64", "kernel": "pn_stage", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC.get((args.workload, "pn_stage")),
                          "peak_source": "FP64 DMMA m16n8k8 throughput measured live (cl_fp64_peak)",
                          "flops_per_update": pn_flops_per_update(n),
                          "hbm_gbs_algorithmic": updates * (2.5 * n * 8 + 16) / (stage_ms * 1e-3) / 1e9},
