@@ -39,7 +39,11 @@ int round_up(int x, int m) { return (x + m - 1) / m * m; }
 // Device copy of one moment order's angular data in the kernels' layouts.
 struct DeviceBasis {
     int n = 0, n2 = 0, nq = 0, nb = 0, K2p = 0, nqp = 0, ldP = 0, ldPf = 0, useGaunt = 0;
-    int nqpF = 0;                                  // flux rows (all directions)
+    // flux layout: nqpF rows of Pf (directions, or one direction of each
+    // pair with fluxPaired), nbF columns (nbeF even-degree ones first when
+    // paired); xi, eta, cxw, cyw in chunk order, 16 directions per chunk
+    int nqpF = 0, nbF = 0, nbeF = 0, fluxPaired = 0;
+    short *fbinv = nullptr;                        // [nbF] moment of each flux column (paired)
     // direction pairs (Newton layout): basis and Hessian columns grouped by
     // degree parity, even group first (nbe, K2e columns, multiples of 8)
     int paired = 0, nbe = 0, K2e = 0;
@@ -75,6 +79,7 @@ struct DeviceBasis {
         cudaFree(ellOff);
         cudaFree(binv);
         cudaFree(pcol);
+        cudaFree(fbinv);
         *this = DeviceBasis();
     }
 };
@@ -135,15 +140,16 @@ static void parity_columns(const std::vector<int> &deg, int paired, std::vector<
 // the two half sums alpha_even . p_even +- alpha_odd . p_odd.
 cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGaunt, const double *w,
                                const double *xi, const double *eta, const double *p, const int *goff,
-                               const int *gidx, const double *gval, int gnnz, int paired = 0)
+                               const int *gidx, const double *gval, int gnnz, int paired = 0,
+                               int fluxPaired = 0)
 {
     B.n = n;
     B.n2 = n2;
     B.nq = nq;
     B.useGaunt = useGaunt;
     const int Q = (int)std::lround(std::sqrt((double)nq));
-    if (paired && (Q * Q != nq || Q % 2 != 0))
-        paired = 0;
+    if (Q * Q != nq || Q % 2 != 0)
+        paired = fluxPaired = 0;
     B.paired = paired;
     const int K2 = useGaunt ? n2 : n * (n + 1) / 2;
     std::vector<unsigned short> prod(n * (n + 1) / 2);
@@ -161,12 +167,10 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
     parity_columns(degH, paired, colH, B.K2e, B.K2p);
     const int rows = paired ? nq / 2 : nq;
     B.nqp = round_up(rows, 32);
-    B.nqpF = round_up(nq, 32);
     int ldP = B.nb + B.K2p;
     while (ldP % 16 != 4)
         ldP++;
     B.ldP = ldP;
-    B.ldPf = round_up(n, 8) + 4;
     B.p0 = p[0];
     std::vector<double> P((size_t)B.nqp * ldP + B.nqp, 0.0), W(B.nqp, 0.0);
     for (int r = 0; r < rows; r++) {
@@ -185,16 +189,33 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         W[r] = w[q];
         P[(size_t)basis_wgap(r, ldP)] = w[q];
     }
-    std::vector<double> Pf((size_t)B.nqpF * B.ldPf, 0.0), XI(B.nqpF, 0.0), ET(B.nqpF, 0.0), CX(B.nqpF, 0.0),
-        CY(B.nqpF, 0.0);
-    for (int q = 0; q < nq; q++) {
+    // Flux layout.  A chunk holds 16 directions: 16 rows of Pf, or with
+    // fluxPaired 8 rows (pairs r) whose directions are q(r) and q(r) + Q,
+    // the chunk's directions 0..7 and 8..15.  The partner's xi, eta and
+    // weights are its own values (the upwind branch and the flux weight are
+    // per direction); only the basis row is shared.
+    std::vector<int> colF;
+    parity_columns(degB, fluxPaired, colF, B.nbeF, B.nbF);
+    B.fluxPaired = fluxPaired;
+    B.ldPf = B.nbF + 4;
+    const int fchunks = fluxPaired ? (nq / 2 + 7) / 8 : (nq + 15) / 16;
+    const int frows = fluxPaired ? 8 : 16;
+    B.nqpF = fchunks * frows;
+    std::vector<double> Pf((size_t)B.nqpF * B.ldPf, 0.0), XI(fchunks * 16, 0.0), ET(fchunks * 16, 0.0),
+        CX(fchunks * 16, 0.0), CY(fchunks * 16, 0.0);
+    for (int r = 0; r < (fluxPaired ? nq / 2 : nq); r++) {
+        const int q = fluxPaired ? (r / Q) * 2 * Q + r % Q : r;
         const double *pq = p + (size_t)q * n2;
         for (int k = 0; k < n; k++)
-            Pf[(size_t)q * B.ldPf + k] = pq[k];
-        XI[q] = xi[q];
-        ET[q] = eta[q];
-        CX[q] = xi[q] * w[q];
-        CY[q] = eta[q] * w[q];
+            Pf[(size_t)r * B.ldPf + colF[k]] = pq[k];
+        for (int h = 0; h < (fluxPaired ? 2 : 1); h++) {
+            const int qq = q + h * Q;
+            const int d = fluxPaired ? (r / 8) * 16 + h * 8 + r % 8 : r;
+            XI[d] = xi[qq];
+            ET[d] = eta[qq];
+            CX[d] = xi[qq] * w[qq];
+            CY[d] = eta[qq] * w[qq];
+        }
     }
     std::vector<unsigned short> &pairs = prod;
     cudaError_t e;
@@ -215,6 +236,12 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
             std::vector<int> pcol(colH.begin(), colH.end());
             if ((e = upload(&B.pcol, pcol)) != cudaSuccess) return e;
         }
+    }
+    if (fluxPaired) {
+        std::vector<short> fbinv(B.nbF, (short)-1);
+        for (int k = 0; k < n; k++)
+            fbinv[colF[k]] = (short)k;
+        if ((e = upload(&B.fbinv, fbinv)) != cudaSuccess) return e;
     }
     if (useGaunt) {
         std::vector<int> off(goff, goff + n * n + 1), idx(gidx, gidx + gnnz);
@@ -521,9 +548,11 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         paired_counts(ang->n, ang->n2, gauntNewton, pnt, pnbk);
         paired = newton_pair_supported(pnt, pnbk) ? 1 : 0;
     }
+    // the flux kernel takes direction pairs for either closure
+    const int fluxPaired = opts->contraction == CL_CONTRACT_PAIRS ? 1 : 0;
     cudaError_t ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi,
                                         ang->eta, ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val,
-                                        ang->gaunt_nnz, paired);
+                                        ang->gaunt_nnz, paired, fluxPaired);
     if (ce != cudaSuccess) {
         ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
         return ctx_fail(ctx, CL_ERR_CUDA);
@@ -581,7 +610,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         ctx->B.release();
         if ((ce = build_device_basis(ctx->B, ang->n, ang->n2, ang->nq, gauntNewton, ang->w, ang->xi, ang->eta,
                                      ang->p, ang->gaunt_off, ang->gaunt_idx, ang->gaunt_val, ang->gaunt_nnz,
-                                     0)) != cudaSuccess) {
+                                     0, fluxPaired)) != cudaSuccess) {
             ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
             return ctx_fail(ctx, CL_ERR_CUDA);
         }
@@ -621,7 +650,10 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     f.cxw = ctx->B.cxw;
     f.cyw = ctx->B.cyw;
     f.n = ctx->n;
-    f.nb = round_up(ctx->n, 8);   // the flux basis keeps the moment order
+    f.nb = ctx->B.nbF;
+    f.paired = ctx->B.fluxPaired;
+    f.nbe = ctx->B.nbeF;
+    f.binv = ctx->B.fbinv;
     f.ldPf = ctx->B.ldPf;
     f.nqp = ctx->B.nqpF;
     f.NX = ctx->NX;

@@ -4,7 +4,8 @@
 // Replaces MomOptSolver::solveFlux (src/momopt/momopt_update.cpp:96-202) and
 // the stage updates (:316-336, :344-364, :367-377).  The reference loops q
 // outermost and streams a whole-grid ansatz array once per quadrature point;
-// here a CTA owns an 8 x 16 tile of interior cells and, per q-chunk:
+// here a CTA owns a 16 x 16 tile of interior cells and, per chunk of 16
+// directions:
 //   1. ansatz on the tile + 2-cell halo: S = alpha . P^T on the FP64 tensor
 //      cores (DMMA), then exp (Mn) or the PPn closure (computeAnsatz :38-69);
 //   2. the limited upwind stencil per (cell, q): slopefit / minmod with theta
@@ -50,6 +51,35 @@ __device__ __forceinline__ double slopefit(double l, double c, double r, double 
     return minmod3(th * (r - c), 0.5 * (r - l), th * (c - l));
 }
 
+// The closure of the ansatz (computeAnsatz, momopt_update.cpp:38-69) on K
+// kinetic values: exp for Mn, the positive-part closure for PPn.
+template <int K>
+__device__ __forceinline__ void closure_n(double (&v)[K], const double (&kin)[K], const FluxArgs &f,
+                                          const double *sExp)
+{
+    if (f.momentType == 0) {
+        fast_exp_n<K>(v, kin, sExp, f.ex.invL, f.ex.L1, f.ex.L2);
+    } else {
+        const double dl = f.deltaPPn;
+#pragma unroll
+        for (int h = 0; h < K; h++) {
+            const double x = kin[h];
+            if (x > 0)
+                v[h] = 0.5 * x + 0.5 * sqrt(x * x + 4 * dl);
+            else
+                v[h] = -dl / (0.5 * x - 0.5 * sqrt(x * x + 4 * dl));
+        }
+    }
+}
+
+// PAIR = 1: direction pairs.  Directions q and q + Q (phi and phi + pi) have
+// the same weight and p_l(q + Q) = (-1)^l p_l(q), so with the basis columns
+// grouped by degree parity one MMA chain per parity gives both exponents,
+// S(q) = S_even + S_odd and S(q + Q) = S_even - S_odd, and the projection
+// takes F(q) + F(q + Q) on the even columns and F(q) - F(q + Q) on the odd
+// ones: half the tensor-core work of one direction at a time.  The stencil
+// is per direction either way.
+template <int PAIR>
 __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_constant__ FluxArgs f)
 {
     extern __shared__ __align__(16) double sm[];
@@ -69,22 +99,25 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
     for (int i = tid; i < 64; i += kFluxThreads)
         sExp[i] = f.ex.tab[i];
 
-    // alpha of the halo region (zero outside the grid)
+    // alpha of the halo region in the basis's column order (zero outside
+    // the grid)
     for (int idx = tid; idx < HC * nb; idx += kFluxThreads) {
-        int h = idx / nb, k = idx % nb;
+        int h = idx / nb, c = idx % nb;
         int hi = h / HY, hj = h % HY;
         int i = i0 - 2 + hi, j = j0 - 2 + hj;
+        const int k = PAIR ? (int)f.binv[c] : c;
         double v = 0.0;
-        if (k < n && i < f.NX && j < f.NY)
+        if (k >= 0 && k < n && i < f.NX && j < f.NY)
             v = f.alpha[((size_t)i * f.NY + j) * n + k];
-        sAl[h * ldAl + k] = v;
+        sAl[h * ldAl + c] = v;
     }
 
-    const int nchunks = f.nqp / kq;
+    constexpr int kr = PAIR ? kQ / 2 : kQ;   // rows of P per chunk
+    const int nchunks = f.nqp / kr;
     auto load_chunk = [&](int c, int buf) {
-        const double *src = f.P + (size_t)c * kq * ldPf;
+        const double *src = f.P + (size_t)c * kr * ldPf;
         double *dst = sP + buf * kq * ldPf;
-        for (int i = tid; i < kq * ldPf / 2; i += kFluxThreads)
+        for (int i = tid; i < kr * ldPf / 2; i += kFluxThreads)
             cp_async16(dst + 2 * i, src + 2 * i);
         double *q = sQ + buf * 4 * kq;
         for (int i = tid; i < kq / 2; i += kFluxThreads) {
@@ -114,6 +147,35 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         const double *Pb = sP + buf * kq * ldPf;
         const double *Qb = sQ + buf * 4 * kq;
         // 1. ansatz on the halo tile
+        if (PAIR) {
+            const int nbe = f.nbe;
+            for (int mt = warp; mt < HC / 16; mt += kFluxWarps) {
+                double ce[4] = {0.0, 0.0, 0.0, 0.0}, co[4] = {0.0, 0.0, 0.0, 0.0};
+                const double *A0 = sAl + (mt * 16 + g) * ldAl;
+                const double *A1 = A0 + 8 * ldAl;
+                const double *B = Pb + g * ldPf;
+                for (int k0 = 0; k0 < nbe; k0 += 8)
+                    dmma16x8x8(ce, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
+                               B[k0 + t4 + 4]);
+                for (int k0 = nbe; k0 < nb; k0 += 8)
+                    dmma16x8x8(co, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
+                               B[k0 + t4 + 4]);
+                double kin[8], v[8];
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    kin[h] = ce[h] + co[h];
+                    kin[4 + h] = ce[h] - co[h];
+                }
+                closure_n<8>(v, kin, f, sExp);
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
+                    int q = 2 * t4 + (h & 1);
+                    sA[q * ldA + cell] = v[h];
+                    sA[(q + 8) * ldA + cell] = v[4 + h];
+                }
+            }
+        } else
         for (int ti = warp; ti < ntiles1; ti += kFluxWarps) {
             int mt = ti % (HC / 16), nt = ti / (HC / 16);
             double cs[4] = {0.0, 0.0, 0.0, 0.0};
@@ -124,19 +186,7 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
                            B[k0 + t4 + 4]);
             double v[4];
-            if (f.momentType == 0) {
-                fast_exp_n<4>(v, cs, sExp, f.ex.invL, f.ex.L1, f.ex.L2);
-            } else {
-                const double dl = f.deltaPPn;
-#pragma unroll
-                for (int h = 0; h < 4; h++) {
-                    const double kin = cs[h];
-                    if (kin > 0)
-                        v[h] = 0.5 * kin + 0.5 * sqrt(kin * kin + 4 * dl);
-                    else
-                        v[h] = -dl / (0.5 * kin - 0.5 * sqrt(kin * kin + 4 * dl));
-                }
-            }
+            closure_n<4>(v, cs, f, sExp);
 #pragma unroll
             for (int h = 0; h < 4; h++) {
                 int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
@@ -221,6 +271,27 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         }
         __syncthreads();
         // 3. projection on the basis: flux[ic][k] += F[ic][q] p[q][k]
+        if (PAIR) {
+            // k = the chunk's 8 pairs; rows t4, t4 + 4 of sF and their
+            // partners 8 rows further
+            const double *A0 = sF + t4 * ldF + warp * 16 + g;
+            const double *A8 = A0 + 8 * ldF;
+            const double f0 = A0[0], f1 = A0[8], f2 = A0[4 * ldF], f3 = A0[4 * ldF + 8];
+            const double p0 = A8[0], p1 = A8[8], p2 = A8[4 * ldF], p3 = A8[4 * ldF + 8];
+            const double s0 = f0 + p0, s1 = f1 + p1, s2 = f2 + p2, s3 = f3 + p3;
+            const double d0 = f0 - p0, d1 = f1 - p1, d2 = f2 - p2, d3 = f3 - p3;
+            const int nbe = f.nbe;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (j < NTf) {
+                    const double *B0 = Pb + t4 * ldPf + j * 8 + g;
+                    if (j * 8 < nbe)
+                        dmma16x8x8(acc[j], s0, s1, s2, s3, B0[0], B0[4 * ldPf]);
+                    else
+                        dmma16x8x8(acc[j], d0, d1, d2, d3, B0[0], B0[4 * ldPf]);
+                }
+            }
+        } else
         for (int k0 = 0; k0 < kq; k0 += 8) {
             const double *A0 = sF + (k0 + t4) * ldF + warp * 16 + g;
             double a0 = A0[0], a1 = A0[8], a2 = A0[4 * ldF], a3 = A0[4 * ldF + 8];
@@ -243,8 +314,10 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         for (int h = 0; h < 4; h++) {
             int ic = warp * 16 + g + ((h & 2) ? 8 : 0);
             int k = j * 8 + 2 * t4 + (h & 1);
+            if (PAIR)
+                k = f.binv[k];
             int i = i0 + ic / TY, jj = j0 + ic % TY;
-            if (k >= n || i >= f.NX - 2 || jj >= f.NY - 2)
+            if (k < 0 || k >= n || i >= f.NX - 2 || jj >= f.NY - 2)
                 continue;
             size_t cell = (size_t)i * f.NY + jj;
             double st = f.sigmaT[cell], ss = f.sigmaS[cell];
@@ -361,6 +434,8 @@ cudaError_t launch_halo(double *moments, int n, int NX, int NY, const HaloBuffer
 
 int plan_flux(FluxArgs &f)
 {
+    if (f.nb > 32 || f.nb % 8 != 0 || (f.paired && f.binv == nullptr))
+        return -1;   // the projection accumulators hold four column tiles
     f.kq = kQ;
     f.ldAl = f.nb + 4;
     f.ldA = HC + 2;      // ldA % 8 == 2: conflict-free fragment stores
@@ -386,12 +461,17 @@ int plan_flux(FluxArgs &f)
 
 cudaError_t prepare_flux(const FluxArgs &f)
 {
-    return cudaFuncSetAttribute(flux_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, f.smemBytes);
+    if (f.paired)
+        return cudaFuncSetAttribute(flux_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, f.smemBytes);
+    return cudaFuncSetAttribute(flux_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, f.smemBytes);
 }
 
 cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream)
 {
-    flux_kernel<<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
+    if (f.paired)
+        flux_kernel<1><<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
+    else
+        flux_kernel<0><<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
     return cudaGetLastError();
 }
 

@@ -12,10 +12,15 @@ struct FluxArgs {
     double *moments;            // [C][n], updated in place on interior cells
     const double *momentsOld;   // Heun average partner (stage 2) or null (stage 1)
     const double *sigmaT, *sigmaS;  // [C]
-    const double *P;            // [nqp][ldPf] basis, columns >= n zero
-    const double *xi, *eta;     // [nqp], zero on padded rows
-    const double *cxw, *cyw;    // xi*w, eta*w per q
+    const double *P;            // [nqp][ldPf] basis rows, padding columns zero
+    const double *xi, *eta;     // 16 per chunk, zero on padded directions
+    const double *cxw, *cyw;    // xi*w, eta*w per direction
     int n, nb, ldPf, nqp;
+    // direction pairs: a chunk's 8 rows of P serve directions q (0..7) and
+    // q + Q (8..15); columns are grouped by degree parity (nbe even ones
+    // first) and binv[c] is the moment of column c (-1 padding)
+    int paired, nbe;
+    const short *binv;
     int NX, NY;                 // grid with ghosts
     int momentType, initCond;
     double theta, deltaPPn;

@@ -92,9 +92,10 @@ typedef struct {
     int contraction;        /* CL_CONTRACT_PAIRS (default): the quadrature
                                directions phi and phi + pi share one
                                contraction through the degree parity of the
-                               basis, where supported (Mn, FP64);
-                               CL_CONTRACT_SINGLE: every direction on its own.
-                               The same sums in another order. */
+                               basis, in the kinetic flux (Mn and PPn) and in
+                               the Newton evaluation where supported (Mn,
+                               FP64); CL_CONTRACT_SINGLE: every direction on
+                               its own. The same sums in another order. */
 } cl_options;
 enum { CL_CONTRACT_PAIRS = 0, CL_CONTRACT_SINGLE = 1 };
 
