@@ -95,6 +95,7 @@ def lib():
             "cl_sync": (C.c_int, [vp]),
             "cl_get_state": (C.c_int, [vp, dp, dp]),
             "cl_set_state": (C.c_int, [vp, dp, dp]),
+            "cl_step_host": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp, dp]),
             "cl_get_stats": (C.c_int, [vp, C.POINTER(cl_stats)]),
             "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
@@ -316,6 +317,15 @@ class Context:
         m = np.ascontiguousarray(moments, dtype=np.float64)
         a = np.ascontiguousarray(alpha, dtype=np.float64)
         _check(lib().cl_set_state(self._ctx, _dp(m), _dp(a)), self._err)
+
+    def step_host(self, dt, dx, dy, moments, alpha):
+        """One RK2 step on host arrays ([NX*NY][n] float64, C-contiguous),
+        updated in place; page-locked arrays let the copies overlap the
+        kernels."""
+        for x in (moments, alpha):
+            if x.dtype != np.float64 or not x.flags.c_contiguous or x.size != self.NX * self.NY * self.n:
+                raise ValueError("step_host needs C-contiguous float64 arrays of NX*NY*n values")
+        _check(lib().cl_step_host(self._ctx, dt, dx, dy, _dp(moments), _dp(alpha)), self._err)
 
     def last_iterations(self):
         it = np.empty(self.NX * self.NY, np.int32)

@@ -36,6 +36,9 @@ namespace {
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// cl_step_host: bands of cells whose upload and first-stage solve overlap
+constexpr int kHostBands = 4;
+
 // Device copy of one moment order's angular data in the kernels' layouts.
 struct DeviceBasis {
     int n = 0, n2 = 0, nq = 0, nb = 0, K2p = 0, nqp = 0, ldP = 0, ldPf = 0, useGaunt = 0;
@@ -407,7 +410,7 @@ struct cl_ctx {
     long long C = 0;
     DeviceBasis B;
     double *dMom = nullptr, *dAlpha = nullptr, *dOld = nullptr, *dSigT = nullptr, *dSigS = nullptr;
-    unsigned int *dQueue = nullptr;   // [4]: stage 1, stage 2, batch, spare
+    unsigned int *dQueue = nullptr;   // [4 + kHostBands]: stage 1, stage 2, batch, spare, bands
     DevStats *dStats = nullptr;
     int *dErr = nullptr;
     int *hErr = nullptr;              // pinned [2]
@@ -423,6 +426,9 @@ struct cl_ctx {
     cudaGraphExec_t exec = nullptr;
     double gdt = 0, gdx = 0, gdy = 0;
     int graphKernels = 0;
+    // cl_step_host: copy stream and its events (created on first use)
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evStart = nullptr, evK1 = nullptr, evFlux = nullptr, evBand[8] = {};
     // batch scratch (grow only)
     double *bU = nullptr, *bA = nullptr, *bR = nullptr;
     int *bI = nullptr, *bS = nullptr;
@@ -559,7 +565,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     }
     if (cudaMalloc(&ctx->dMom, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dAlpha, C * n * 8) != cudaSuccess ||
         cudaMalloc(&ctx->dOld, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dSigT, C * 8) != cudaSuccess ||
-        cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&ctx->dStats, sizeof(DevStats)) != cudaSuccess || cudaMalloc(&ctx->dErr, 2 * sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dIters, C * sizeof(int)) != cudaSuccess) {
@@ -710,6 +716,16 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->bR);
     cudaFree(ctx->bI);
     cudaFree(ctx->bS);
+    if (ctx->copyStream) {
+        cudaStreamSynchronize(ctx->copyStream);
+        cudaStreamDestroy(ctx->copyStream);
+    }
+    for (cudaEvent_t ev : {ctx->evStart, ctx->evK1, ctx->evFlux})
+        if (ev)
+            cudaEventDestroy(ev);
+    for (cudaEvent_t ev : ctx->evBand)
+        if (ev)
+            cudaEventDestroy(ev);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1008,6 +1024,128 @@ int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha)
     if (alpha)
         CUDA_TRY(ctx, cudaMemcpy(ctx->dAlpha, alpha, bytes, cudaMemcpyHostToDevice));
     return CL_OK;
+}
+
+// One RK2 step on a state held in host memory, equal to cl_set_state,
+// cl_step and cl_get_state (the reference's solver keeps c_moments and
+// c_alpha on the host, momopt_update.cpp:279-378).  The copies run on a
+// second stream and overlap the kernels: the state goes up in kHostBands
+// bands of cells, each band's first-stage solve starting when its band has
+// arrived; the multipliers come back while the second-stage flux runs, and
+// the first part of the moments while the rest of that flux runs (its tiles
+// split in two launches at a whole number of waves).  With a periodic deck
+// or a learned warm start, whose first kernels read the whole grid, the
+// state goes up in one band.  Page-locked host buffers give the overlap;
+// others are still correct.
+int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, double *alpha)
+{
+    if (!ctx || !moments || !alpha)
+        return CL_ERR_ARG;
+    if (!ctx->copyStream) {
+        CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking));
+        for (cudaEvent_t *ev : {&ctx->evStart, &ctx->evK1, &ctx->evFlux})
+            CUDA_TRY(ctx, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+        for (int b = 0; b < kHostBands; b++)
+            CUDA_TRY(ctx, cudaEventCreateWithFlags(&ctx->evBand[b], cudaEventDisableTiming));
+    }
+    cudaStream_t S = ctx->stream, X = ctx->copyStream;
+    const size_t n = (size_t)ctx->n, C = (size_t)ctx->C, rowBytes = (size_t)ctx->NY * n * 8;
+    const bool periodic = ctx->grid.init_cond == 2;
+    const int bands = (periodic || ctx->warm) ? 1 : kHostBands;
+    int nk = 0;
+    cudaError_t e = cudaSuccess;
+    auto run = [&](cudaError_t r) {
+        if (e == cudaSuccess)
+            e = r;
+    };
+    // earlier work on the device state is done before the copies start
+    run(cudaEventRecord(ctx->evStart, S));
+    run(cudaStreamWaitEvent(X, ctx->evStart, 0));
+    run(cudaMemsetAsync(ctx->dQueue, 0, (4 + kHostBands) * sizeof(unsigned), S));
+    size_t band0[kHostBands + 1];
+    for (int b = 0; b <= bands; b++)
+        band0[b] = C * b / bands;
+    for (int b = 0; b < bands; b++) {
+        const size_t off = band0[b] * n, bytes = (band0[b + 1] - band0[b]) * n * 8;
+        run(cudaMemcpyAsync(ctx->dMom + off, moments + off, bytes, cudaMemcpyHostToDevice, X));
+        run(cudaMemcpyAsync(ctx->dAlpha + off, alpha + off, bytes, cudaMemcpyHostToDevice, X));
+        run(cudaEventRecord(ctx->evBand[b], X));
+    }
+    for (int stage = 0; stage < 2 && e == cudaSuccess; stage++) {
+        if (stage == 0 && bands == 1)
+            run(cudaStreamWaitEvent(S, ctx->evBand[0], 0));
+        if (periodic) {
+            run(launch_ghost_periodic(ctx->dMom, ctx->n, ctx->NX, ctx->NY, S));
+            nk += 2;
+        }
+        if (ctx->warm && e == cudaSuccess) {
+            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, S) != CL_OK)
+                run(cudaErrorLaunchFailure);
+            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+        }
+        NewtonArgs a = ctx->nargs;
+        a.prob[0].u = ctx->dMom;
+        a.prob[0].alpha = ctx->dAlpha;
+        a.prob[0].iters = ctx->dIters;
+        a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
+        a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
+        const int parts = (stage == 0) ? bands : 1;
+        for (int b = 0; b < parts; b++) {
+            if (stage == 0 && bands > 1)
+                run(cudaStreamWaitEvent(S, ctx->evBand[b], 0));
+            a.prob[0].first = (stage == 0) ? (int)band0[b] : 0;
+            a.prob[0].count = (stage == 0) ? (int)(band0[b + 1] - band0[b]) : (int)C;
+            a.prob[0].queue = ctx->dQueue + ((stage == 0 && bands > 1) ? 4 + b : stage);
+            if (e == cudaSuccess)
+                run(launch_newton(a, ctx->nCtas, S));
+            nk++;
+        }
+        FluxArgs f = ctx->fargs;
+        f.dt = dt;
+        f.dx = dx;
+        f.dy = dy;
+        f.momentsOld = (stage == 1) ? ctx->dOld : nullptr;
+        if (stage == 0) {
+            if (e == cudaSuccess)
+                run(launch_flux(f, S));
+            nk++;
+            continue;
+        }
+        // the multipliers are final: read them back under the flux
+        run(cudaEventRecord(ctx->evK1, S));
+        run(cudaStreamWaitEvent(X, ctx->evK1, 0));
+        run(cudaMemcpyAsync(alpha, ctx->dAlpha, C * n * 8, cudaMemcpyDeviceToHost, X));
+        // flux in two launches; the cell rows that the first completes go
+        // back while the second runs (each tile writes only its own cells)
+        const int tiles = f.tilesX * f.tilesY, sms = sm_count();
+        int tA = (tiles / 2) / sms * sms;
+        const int fullRows = tA / f.tilesY;
+        if (tA <= 0 || fullRows <= 0)
+            tA = 0;
+        size_t rowsA = 0;
+        if (tA > 0) {
+            if (e == cudaSuccess)
+                run(launch_flux_tiles(f, 0, tA, S));
+            nk++;
+            rowsA = 2 + (size_t)fullRows * flux_tile_rows(f);
+            run(cudaEventRecord(ctx->evFlux, S));
+            run(cudaStreamWaitEvent(X, ctx->evFlux, 0));
+            run(cudaMemcpyAsync(moments, ctx->dMom, rowsA * rowBytes, cudaMemcpyDeviceToHost, X));
+        }
+        if (e == cudaSuccess)
+            run(launch_flux_tiles(f, tA, tiles - tA, S));
+        nk++;
+        run(cudaMemcpyAsync(moments + rowsA * ctx->NY * n, ctx->dMom + rowsA * ctx->NY * n,
+                            C * n * 8 - rowsA * rowBytes, cudaMemcpyDeviceToHost, S));
+    }
+    g_launches += nk;
+    run(cudaStreamSynchronize(X));
+    run(cudaStreamSynchronize(S));
+    if (e != cudaSuccess) {
+        ctx->err = std::string("host-state step: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return read_device_error(ctx);
 }
 
 int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m)

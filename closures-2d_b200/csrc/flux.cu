@@ -85,7 +85,8 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
     extern __shared__ __align__(16) double sm[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
-    const int bx = blockIdx.x / f.tilesY, by = blockIdx.x % f.tilesY;
+    const int tile = blockIdx.x + f.tileBase;
+    const int bx = tile / f.tilesY, by = tile % f.tilesY;
     const int i0 = 2 + bx * TX, j0 = 2 + by * TY;     // first interior cell of the tile
     const int n = f.n, nb = f.nb, ldPf = f.ldPf;
     constexpr int kq = kQ;
@@ -466,14 +467,25 @@ cudaError_t prepare_flux(const FluxArgs &f)
     return cudaFuncSetAttribute(flux_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, f.smemBytes);
 }
 
-cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream)
+cudaError_t launch_flux_tiles(const FluxArgs &f, int first, int count, cudaStream_t stream)
 {
-    if (f.paired)
-        flux_kernel<1><<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
+    if (first < 0 || count <= 0 || first + count > f.tilesX * f.tilesY)
+        return cudaErrorInvalidValue;
+    FluxArgs g = f;
+    g.tileBase = first;
+    if (g.paired)
+        flux_kernel<1><<<count, kFluxThreads, g.smemBytes, stream>>>(g);
     else
-        flux_kernel<0><<<f.tilesX * f.tilesY, kFluxThreads, f.smemBytes, stream>>>(f);
+        flux_kernel<0><<<count, kFluxThreads, g.smemBytes, stream>>>(g);
     return cudaGetLastError();
 }
+
+cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream)
+{
+    return launch_flux_tiles(f, 0, f.tilesX * f.tilesY, stream);
+}
+
+int flux_tile_rows(const FluxArgs &) { return TX; }
 
 cudaError_t launch_ghost_periodic(double *moments, int n, int NX, int NY, cudaStream_t stream)
 {

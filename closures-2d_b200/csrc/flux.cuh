@@ -31,11 +31,15 @@ struct FluxArgs {
     ExpConsts ex;
     int smemBytes;
     int tilesX, tilesY;
+    int tileBase;               // first tile of the launch (row-major over tilesX x tilesY)
 };
 
 int plan_flux(FluxArgs &f);
 cudaError_t prepare_flux(const FluxArgs &f);
 cudaError_t launch_flux(const FluxArgs &f, cudaStream_t stream);
+// The tiles first .. first + count - 1 only (one launch of a split stage).
+cudaError_t launch_flux_tiles(const FluxArgs &f, int first, int count, cudaStream_t stream);
+int flux_tile_rows(const FluxArgs &f);   // interior cells per tile along x
 // duplicateBoundaries (momopt_boundaries.cpp:190-223) on device moments.
 cudaError_t launch_ghost_periodic(double *moments, int n, int NX, int NY, cudaStream_t stream);
 // Halo strips of a node's block: pack (1) the inner strips into p[side] or

@@ -57,6 +57,8 @@ struct NewtonProblem {
     double *regs;               // nullable [count]
     int *status;                // nullable [count]
     unsigned int *queue;        // work counter, zero before the launch
+    int first;                  // index of the first work item: the launch solves
+                                // items first .. first + count - 1 (a band of cells)
 };
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).

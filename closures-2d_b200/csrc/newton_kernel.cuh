@@ -1762,7 +1762,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                 int c = 0;
                 for (int s = 0; s < T && c < take; s++) {
                     if (L.ints[s * SI_N + SI_STATE] == S_IDLE) {
-                        L.ints[s * SI_N + SI_CELL] = (int)base + c;
+                        L.ints[s * SI_N + SI_CELL] = pb.first + (int)base + c;
                         L.ints[s * SI_N + SI_STATE] = S_NEW;
                         c++;
                     }

@@ -180,6 +180,15 @@ int cl_halo_unpack(cl_ctx *ctx, double *const bufs[4]);
 /* Copies the full state (all cells, ghosts included) to / from the host. */
 int cl_get_state(cl_ctx *ctx, double *moments, double *alpha);
 int cl_set_state(cl_ctx *ctx, const double *moments, const double *alpha);
+/* One RK2 step (MomOptSolver::update, momopt_update.cpp:279-378) on a state
+ * held in host memory, as the reference's solver holds c_moments and c_alpha:
+ * moments and alpha ([NX*NY][n], ghosts included) are read, stepped and
+ * overwritten with the new state.  The result equals cl_set_state, cl_step,
+ * cl_get_state; the copies overlap the kernels (bands of cells go up while
+ * earlier bands are solved, the multipliers and the first part of the
+ * moments come back under the second-stage flux), which needs page-locked
+ * host buffers to take effect.  Blocks until the step is done. */
+int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, double *alpha);
 /* Cumulative optimisation statistics (momopt_update.cpp:256-275). */
 int cl_get_stats(cl_ctx *ctx, cl_stats *s);
 /* outs.iter of every cell (ghosts included) in the last optimisation stage. */

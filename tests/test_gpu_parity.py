@@ -229,6 +229,14 @@ GRID_CASES = [
                           quad_order=20, tol=1e-8, moment_type="ppn", use_gaunt=0), 4),
     ("m6_pulse_q40", dict(num_cells_x=24, num_cells_y=24, gaussian_sigma=0.1, floor=1e-8,
                           moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1), 2),
+    # one direction at a time in the flux and the Newton evaluation
+    ("m4_lattice_q30_single", dict(num_cells_x=40, num_cells_y=40, a_x=-3.5, b_x=3.5, a_y=-3.5,
+                                   b_y=3.5, init_cond="lattice", floor=1e-10, moment_order=4,
+                                   quad_order=30, tol=1e-8, use_gaunt=1,
+                                   extra={"MOMOPT_GPU_CONTRACTION": "single"}), 4),
+    ("pp3_periodic_single", dict(num_cells_x=24, num_cells_y=20, init_cond="smooth", moment_order=3,
+                                 quad_order=20, tol=1e-8, moment_type="ppn", use_gaunt=0,
+                                 extra={"MOMOPT_GPU_CONTRACTION": "single"}), 4),
 ]
 
 
