@@ -62,7 +62,12 @@ struct NewtonProblem {
 };
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
-enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3 };
+// S_HELP: an idle slot lent, for one round, to a slot whose line search is
+// backtracking (plain Newton, work counter exhausted): it evaluates one of the
+// parent's next trial points (SI_CELL = parent slot, SI_ITER = k, the trial
+// t / 2^k), so that up to T - 1 halvings of linesearch.cpp:53-81 take one
+// round instead of one round each.
+enum SlotState { S_IDLE = 0, S_NEW = 1, S_NEWTON = 2, S_TRIAL = 3, S_HELP = 4 };
 enum { SC_T = 0, SC_FREF, SC_GD, SC_MAXF, SC_RTOL, SC_U0, SC_ASCALE, SC_DELTA, SC_R, SC_N };
 enum { SI_CELL = 0, SI_STATE, SI_ITER, SI_TOTAL, SI_REG, SI_MAXITER, SI_PRED, SI_CB, SI_BFGS, SI_N };
 

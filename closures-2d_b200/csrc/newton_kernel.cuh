@@ -512,6 +512,39 @@ __device__ __forceinline__ void hessian_from_contractions(const NewtonArgs &a, c
     }
 }
 
+// A helper slot's trial point: the parent's alpha_old + t_k d with t_k the
+// parent's t halved k times, formed as the backtracking loop forms it.
+__device__ void init_helper(const NewtonProblem &pb, Layout &L, int s, int lane, int ldv)
+{
+    const int par = L.ints[s * SI_N + SI_CELL], k = L.ints[s * SI_N + SI_ITER];
+    double t = L.scal[par * SC_N + SC_T];
+    for (int i = 0; i < k; i++)
+        t = 0.5 * t;
+    if (lane < ldv)
+        L.alpha[s * ldv + lane] =
+            (lane < pb.n) ? L.aold[par * ldv + lane] + t * L.d[par * ldv + lane] : 0.0;
+    if (lane == 0)
+        L.scal[s * SC_N + SC_DELTA] = L.scal[par * SC_N + SC_DELTA];
+}
+
+// The helper of slot s with index k (-1: none); slots are at most 32.
+__device__ __forceinline__ int find_helper(const Layout &L, int T, int s, int k, int lane)
+{
+    const int *hi = L.ints + lane * SI_N;
+    const unsigned m =
+        __ballot_sync(0xffffffffu, lane < T && hi[SI_STATE] == S_HELP && hi[SI_CELL] == s && hi[SI_ITER] == k);
+    return m ? __ffs(m) - 1 : -1;
+}
+
+__device__ __forceinline__ void release_helpers(Layout &L, int T, int s, int lane)
+{
+    __syncwarp();
+    int *hi = L.ints + lane * SI_N;
+    if (lane < T && hi[SI_STATE] == S_HELP && hi[SI_CELL] == s)
+        hi[SI_STATE] = S_IDLE;
+    __syncwarp();
+}
+
 // Newton logic for one slot after its evaluation (warp-wide).
 __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
                            int warp)
@@ -551,6 +584,35 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         if (!(fsum <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD])) {
             t = 0.5 * t;
             double ao = act ? L.aold[s * ldv + lane] : 0.0;
+            // the next trial points, evaluated this round by helper slots:
+            // take them in the backtracking order, stopping where the loop
+            // of linesearch.cpp:53-81 would stop
+            for (int k = 1; t * sc[SC_MAXF] > DBL_EPSILON / 2; k++) {
+                const int h = find_helper(L, a.T, s, k, lane);
+                if (h < 0)
+                    break;
+                const double ah = act ? L.alpha[h * ldv + lane] : 0.0;
+                double fp = 0.0;
+                for (int q = 0; q < a.ntq; q++)
+                    fp += L.fpart[h * a.ntq + q];
+                const double fh = fp - warp_sum(ah * ui);
+                if (fh <= sc[SC_FREF] + 1e-3 * t * sc[SC_GD]) {
+                    // accepted at t: the slot moves to this trial point, and
+                    // the next round's evaluation of it (bit for bit the
+                    // helper's) is taken, and counted, as the accepted trial
+                    if (act)
+                        L.alpha[s * ldv + lane] = ah;
+                    __syncwarp();
+                    if (lane == 0)
+                        sc[SC_T] = t;
+                    release_helpers(L, a.T, s, lane);
+                    return;
+                }
+                if (lane == 0)
+                    atomicAdd(&L.stat[kNumReg + 2], 1ull);
+                t = 0.5 * t;
+            }
+            release_helpers(L, a.T, s, lane);
             if (t * sc[SC_MAXF] > DBL_EPSILON / 2) {
                 if (act)
                     L.alpha[s * ldv + lane] = ao + t * L.d[s * ldv + lane];
@@ -1737,6 +1799,8 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
             int p = ctl[0];
             int nIdle = 0, nActive = 0;
             for (int s = 0; s < T; s++) {
+                if (L.ints[s * SI_N + SI_STATE] == S_HELP)   // helpers serve one round
+                    L.ints[s * SI_N + SI_STATE] = S_IDLE;
                 if (L.ints[s * SI_N + SI_STATE] == S_IDLE)
                     nIdle++;
                 else
@@ -1772,6 +1836,23 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                 if (nIdle > 0)
                     exhausted = true;
             }
+            // idle slots once the work counter is exhausted: lend them to
+            // slots whose line search is backtracking (plain Newton)
+            if (a.optType == 0 && exhausted && nIdle > 0) {
+                for (int s = 0; s < T && nIdle > 0; s++) {
+                    if (L.ints[s * SI_N + SI_STATE] != S_TRIAL || !(L.scal[s * SC_N + SC_T] < 1.0))
+                        continue;
+                    int k = 0;
+                    for (int h = 0; h < T && nIdle > 0; h++) {
+                        if (L.ints[h * SI_N + SI_STATE] == S_IDLE) {
+                            L.ints[h * SI_N + SI_STATE] = S_HELP;
+                            L.ints[h * SI_N + SI_CELL] = s;
+                            L.ints[h * SI_N + SI_ITER] = ++k;
+                            nIdle--;
+                        }
+                    }
+                }
+            }
             ctl[0] = p;
             ctl[2] = exhausted ? 1 : 0;
             ctl[1] = (nActive == 0) ? 1 : 0;
@@ -1794,9 +1875,13 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
                     L.ellOff[i] = pb.ellOff[i];
             }
         }
-        for (int s = warp; s < T; s += kWarps)
-            if (L.ints[s * SI_N + SI_STATE] == S_NEW)
+        for (int s = warp; s < T; s += kWarps) {
+            const int st = L.ints[s * SI_N + SI_STATE];
+            if (st == S_NEW)
                 (a.optType != 0) ? init_slot_cb(a, pb, L, s, lane, ldv) : init_slot(a, pb, L, s, lane, ldv);
+            else if (st == S_HELP)
+                init_helper(pb, L, s, lane, ldv);
+        }
         __syncthreads();
 
         // ---- phase A: evaluation contractions over the quadrature
