@@ -27,6 +27,19 @@ constexpr int TX = 16, TY = 16;            // interior tile (x slow, y fast)
 constexpr int HX = TX + 4, HY = TY + 4;    // with the 2-cell halo
 constexpr int HC = HX * HY;                // 400 halo cells (25 m16 tiles)
 constexpr int IC = TX * TY;                // 256 interior cells (16 m16 tiles)
+// The stencils never read the 2 x 2 halo corners: the ansatz runs on the
+// other 384 halo cells (24 m16 tiles), taken row by row.
+constexpr int kAnsatzTiles = (HC - 16) / 16;
+__device__ __forceinline__ int halo_cell(int r)
+{
+    if (r < 2 * TY)
+        return (r / TY) * HY + 2 + r % TY;
+    r -= 2 * TY;
+    if (r < TX * HY)
+        return (2 + r / HY) * HY + r % HY;
+    r -= TX * HY;
+    return (TX + 2 + r / TY) * HY + 2 + r % TY;
+}
 constexpr int kFluxThreads = 512;          // 16 warps: one interior m-tile each
 constexpr int kFluxWarps = kFluxThreads / 32;
 constexpr int kQ = 16;                     // directions per chunk
@@ -136,7 +149,7 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
     for (int j = 0; j < 4; j++)
         acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
     const int NTf = nb / 8;
-    const int ntiles1 = (HC / 16) * (kq / 8);
+    const int ntiles1 = kAnsatzTiles * (kq / 8);
 
     load_chunk(0, 0);
     for (int c = 0; c < nchunks; c++) {
@@ -150,10 +163,11 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         // 1. ansatz on the halo tile
         if (PAIR) {
             const int nbe = f.nbe;
-            for (int mt = warp; mt < HC / 16; mt += kFluxWarps) {
+            for (int mt = warp; mt < kAnsatzTiles; mt += kFluxWarps) {
                 double ce[4] = {0.0, 0.0, 0.0, 0.0}, co[4] = {0.0, 0.0, 0.0, 0.0};
-                const double *A0 = sAl + (mt * 16 + g) * ldAl;
-                const double *A1 = A0 + 8 * ldAl;
+                const int c0 = halo_cell(mt * 16 + g), c1 = halo_cell(mt * 16 + g + 8);
+                const double *A0 = sAl + c0 * ldAl;
+                const double *A1 = sAl + c1 * ldAl;
                 const double *B = Pb + g * ldPf;
                 for (int k0 = 0; k0 < nbe; k0 += 8)
                     dmma16x8x8(ce, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
@@ -170,7 +184,7 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 closure_n<8>(v, kin, f, sExp);
 #pragma unroll
                 for (int h = 0; h < 4; h++) {
-                    int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
+                    int cell = (h & 2) ? c1 : c0;
                     int q = 2 * t4 + (h & 1);
                     sA[q * ldA + cell] = v[h];
                     sA[(q + 8) * ldA + cell] = v[4 + h];
@@ -178,10 +192,11 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
             }
         } else
         for (int ti = warp; ti < ntiles1; ti += kFluxWarps) {
-            int mt = ti % (HC / 16), nt = ti / (HC / 16);
+            int mt = ti % kAnsatzTiles, nt = ti / kAnsatzTiles;
             double cs[4] = {0.0, 0.0, 0.0, 0.0};
-            const double *A0 = sAl + (mt * 16 + g) * ldAl;
-            const double *A1 = A0 + 8 * ldAl;
+            const int c0 = halo_cell(mt * 16 + g), c1 = halo_cell(mt * 16 + g + 8);
+            const double *A0 = sAl + c0 * ldAl;
+            const double *A1 = sAl + c1 * ldAl;
             const double *B = Pb + (nt * 8 + g) * ldPf;
             for (int k0 = 0; k0 < nb; k0 += 8)
                 dmma16x8x8(cs, A0[k0 + t4], A1[k0 + t4], A0[k0 + t4 + 4], A1[k0 + t4 + 4], B[k0 + t4],
@@ -190,7 +205,7 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
             closure_n<4>(v, cs, f, sExp);
 #pragma unroll
             for (int h = 0; h < 4; h++) {
-                int cell = mt * 16 + g + ((h & 2) ? 8 : 0);
+                int cell = (h & 2) ? c1 : c0;
                 int q = nt * 8 + 2 * t4 + (h & 1);
                 sA[q * ldA + cell] = v[h];
             }
