@@ -623,11 +623,16 @@ def pn_arm(args, world, rank, local):
     t1 = time.perf_counter()
     lib = cb.lib()
     for _ in range(e2e_steps):
-        solver.set_moments(hm)
-        solver.update(dt)
-        rc = lib.cl_solver_get_state(solver._s, cb._dp(hm))
-        if rc:
-            raise cb.ClosuresError(rc, lib.cl_solver_last_error(solver._s))
+        if world > 1:
+            # upload, the exchanged step of this node, read back
+            solver.set_moments(hm)
+            solver.update(dt)
+            rc = lib.cl_solver_get_state(solver._s, cb._dp(hm))
+            if rc:
+                raise cb.ClosuresError(rc, lib.cl_solver_last_error(solver._s))
+        else:
+            # the host-state step: bands of rows overlapped with the stages
+            solver.step_host(dt, hm)
     barrier()
     e2e_s = time.perf_counter() - t1
     if world > 1:
@@ -663,7 +668,9 @@ def pn_arm(args, world, rank, local):
                          "hbm_gbs_algorithmic": updates * (2.5 * n * 8 + 16) / (stage_ms * 1e-3) / 1e9},
             "cpu_baseline": cpu,
             "e2e": {"value": world * 2 * C_int * e2e_steps / e2e_s, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": C * n * 8, "d2h_bytes_per_step": C * n * 8, "steps": e2e_steps},
+                    "h2d_bytes_per_step": C * n * 8, "d2h_bytes_per_step": C * n * 8, "steps": e2e_steps,
+                    "call": "cl_solver_set_state + cl_solver_update + cl_solver_get_state" if world > 1
+                    else "cl_pn_step_host (page-locked buffer)"},
             "gpu_launches": int(launches), "clocks": clocks}), flush=True)
     solver.close()
     if world > 1:

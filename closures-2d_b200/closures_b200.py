@@ -170,6 +170,7 @@ def lib():
             "cl_pn_stage_timed": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double,
                                             C.POINTER(C.c_float)]),
             "cl_pn_last_error": (C.c_char_p, [vp]),
+            "cl_pn_step_host": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -470,6 +471,19 @@ class Solver:
     def set_moments(self, m):
         m = np.ascontiguousarray(m, dtype=np.float64)
         _check(lib().cl_solver_set_state(self._s, _dp(m)), self._err)
+
+    def step_host(self, dt, moments):
+        """SOLVER moment: one RK2 step on a host state ([NX*NY][n] float64,
+        C-contiguous), updated in place; page-locked arrays let the copies
+        overlap the stages."""
+        pn = lib().cl_solver_pn(self._s)
+        if not pn:
+            raise ValueError("step_host on a solver without a linear moment stage (use Context.step_host)")
+        if moments.dtype != np.float64 or not moments.flags.c_contiguous or \
+                moments.size != self.NX * self.NY * self.n:
+            raise ValueError("step_host needs a C-contiguous float64 array of NX*NY*n values")
+        _check(lib().cl_pn_step_host(pn, dt, self.dx, self.dy, _dp(moments)),
+               lambda: lib().cl_pn_last_error(pn))
 
     def context_state(self):
         """Moments and multipliers (momopt; zeros for the multipliers of the

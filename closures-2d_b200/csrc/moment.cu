@@ -34,6 +34,7 @@ namespace {
 
 constexpr int kPnWarps = 8;   // cells in flight per CTA, one warp each
 constexpr int kPnMaxN = 64;   // moments per cell (order <= 9)
+constexpr int kPnMaxBands = 16;   // row bands of cl_pn_step_host
 constexpr double kSqrtPiPn = 1.7724538509055160273;   // sqrt(M_PI) rounded to double
 
 struct PnArgs {
@@ -46,6 +47,7 @@ struct PnArgs {
     int n, NX, NY, initCond;
     int filteredGhosts;     // bit s: ghost strip of side s holds (filtered) interior values
     double dt, rdx, rdy, dx, dy, initX, initY;
+    int rowBegin, rowEnd;   // interior rows (x) of this launch; band starts are multiples of kTI
 };
 
 __device__ __forceinline__ bool filtered_cell(const PnArgs &a, int i, int j)
@@ -76,10 +78,10 @@ __global__ void __launch_bounds__(kPnWarps * 32) pn_stage_kernel(PnArgs a)
         ops[e] = a.opsT[e];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nx = a.NX - 4, ny = a.NY - 4;
-    const long long cells = (long long)nx * ny;
+    const int ny = a.NY - 4;
+    const long long cells = (long long)(a.rowEnd - a.rowBegin) * ny;
     for (long long c = (long long)blockIdx.x * kPnWarps + warp; c < cells; c += (long long)gridDim.x * kPnWarps) {
-        const int i = 2 + (int)(c / ny), j = 2 + (int)(c % ny);
+        const int i = 2 + a.rowBegin + (int)(c / ny), j = 2 + (int)(c % ny);
         double t[4][R], self[R];
         const size_t NY = a.NY;
 #pragma unroll
@@ -190,11 +192,12 @@ __global__ void __launch_bounds__(kTI * 32, 2) pn_tile_kernel(PnArgs a)
         ops[(o * NP + i) * OS + k] = (i < n && k < n) ? a.opsT[((size_t)o * n + i) * n + k] : 0.0;
     }
     const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
-    const int nx = a.NX - 4, ny = a.NY - 4;
-    const int tilesJ = (ny + kTJ - 1) / kTJ, tiles = ((nx + kTI - 1) / kTI) * tilesJ;
+    const int ny = a.NY - 4;
+    const int tilesJ = (ny + kTJ - 1) / kTJ;
+    const int tiles = ((a.rowEnd - a.rowBegin + kTI - 1) / kTI) * tilesJ;
     const size_t NY = a.NY;
     for (int tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
-        const int i0 = 2 + (tl / tilesJ) * kTI, j0 = 2 + (tl % tilesJ) * kTJ;
+        const int i0 = 2 + a.rowBegin + (tl / tilesJ) * kTI, j0 = 2 + (tl % tilesJ) * kTJ;
         __syncthreads();   // the previous tile's readers are done (and the operators staged)
         // staged in batches of 8 loads per thread, all issued before any is used
         constexpr int kTileElems = (kTI + 4) * RW * NP, kStep = kTI * 32, kBatch = 8;
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(kTI * 32, 2) pn_tile_kernel(PnArgs a)
                     dmma16x8x8(acc[o >> 1][kt], av[0], av[1], av[2], av[3], ob[kt * 8], ob[4 * OS + kt * 8]);
             }
         }
-        if (i >= a.NX - 2)
+        if (i >= 2 + a.rowEnd)
             continue;
         const double dt = a.dt;
 #pragma unroll
@@ -315,6 +318,9 @@ struct cl_pn {
     int exchanged = -1;    // sides whose ghosts hold neighbour values (-1: periodic or none)
     int nCtas = 0;
     std::string err;
+    // cl_pn_step_host: upload and readback streams and their events (created on first use)
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t evStart = nullptr, evUp[kPnMaxBands] = {}, evDone[kPnMaxBands] = {};
 };
 
 static int pn_fail(cl_pn *p, int rc)
@@ -333,9 +339,18 @@ static int pn_fail(cl_pn *p, int rc)
         }                                                                                      \
     } while (0)
 
-static cudaError_t pn_launch(cl_pn *p, int stage, double dt, double dx, double dy)
+// One stage over interior rows [rowBegin, rowEnd) (rowEnd < 0: all rows) on
+// `stream` (null: the solver's); reads p->cur.
+static cudaError_t pn_launch(cl_pn *p, int stage, double dt, double dx, double dy, int rowBegin = 0,
+                             int rowEnd = -1, cudaStream_t stream = nullptr)
 {
+    if (rowEnd < 0)
+        rowEnd = p->NX - 4;
+    if (!stream)
+        stream = p->stream;
     PnArgs a;
+    a.rowBegin = rowBegin;
+    a.rowEnd = rowEnd;
     a.in = p->cur;
     a.out = (stage == 1) ? p->V : p->U;
     a.old = (stage == 2) ? p->U : nullptr;
@@ -356,21 +371,27 @@ static cudaError_t pn_launch(cl_pn *p, int stage, double dt, double dx, double d
     a.initX = p->grid.init_x;
     a.initY = p->grid.init_y;
     const int np = (p->n + 7) / 8 * 8;
+    const long long rows = rowEnd - rowBegin, ny = p->NY - 4;
+    if (rows <= 0)
+        return cudaSuccess;
+    const long long units = (np <= 32) ? ((rows + kTI - 1) / kTI) * ((ny + kTJ - 1) / kTJ)
+                                       : (rows * ny + kPnWarps - 1) / kPnWarps;
+    const int ctas = (int)std::max<long long>(1, std::min<long long>(units, p->nCtas));
     switch (np) {
     case 8:
-        pn_tile_kernel<8><<<p->nCtas, kTI * 32, pn_tile_smem<8>(), p->stream>>>(a);
+        pn_tile_kernel<8><<<ctas, kTI * 32, pn_tile_smem<8>(), stream>>>(a);
         break;
     case 16:
-        pn_tile_kernel<16><<<p->nCtas, kTI * 32, pn_tile_smem<16>(), p->stream>>>(a);
+        pn_tile_kernel<16><<<ctas, kTI * 32, pn_tile_smem<16>(), stream>>>(a);
         break;
     case 24:
-        pn_tile_kernel<24><<<p->nCtas, kTI * 32, pn_tile_smem<24>(), p->stream>>>(a);
+        pn_tile_kernel<24><<<ctas, kTI * 32, pn_tile_smem<24>(), stream>>>(a);
         break;
     case 32:
-        pn_tile_kernel<32><<<p->nCtas, kTI * 32, pn_tile_smem<32>(), p->stream>>>(a);
+        pn_tile_kernel<32><<<ctas, kTI * 32, pn_tile_smem<32>(), stream>>>(a);
         break;
     default:
-        pn_stage_kernel<2><<<p->nCtas, kPnWarps * 32, (size_t)4 * p->n * p->n * sizeof(double), p->stream>>>(a);
+        pn_stage_kernel<2><<<ctas, kPnWarps * 32, (size_t)4 * p->n * p->n * sizeof(double), stream>>>(a);
     }
     clb_count_launches(1);
     return cudaGetLastError();
@@ -464,6 +485,19 @@ void cl_pn_destroy(cl_pn *p)
         return;
     if (p->stream)
         cudaStreamSynchronize(p->stream);
+    for (cudaStream_t st : {p->up, p->down})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    if (p->evStart)
+        cudaEventDestroy(p->evStart);
+    for (int b = 0; b < kPnMaxBands; b++) {
+        if (p->evUp[b])
+            cudaEventDestroy(p->evUp[b]);
+        if (p->evDone[b])
+            cudaEventDestroy(p->evDone[b]);
+    }
     cudaFree(p->U);
     cudaFree(p->V);
     cudaFree(p->opsT);
@@ -570,6 +604,96 @@ int cl_pn_set_state(cl_pn *p, const double *moments)
     // than a second upload
     PN_TRY(p, cudaMemcpyAsync(p->V, p->U, (size_t)p->C * p->n * 8, cudaMemcpyDeviceToDevice, p->stream));
     p->cur = p->U;
+    return CL_OK;
+}
+
+// One RK2 step on a state in host memory ([NX*NY][n], ghosts included, read
+// and overwritten), equal to cl_pn_set_state, cl_pn_step, cl_pn_get_state.
+// The grid goes up in bands of interior rows (multiples of the tile height)
+// on one stream and comes back on another; stage 1 of band b runs once band
+// b + 1 has arrived (its stencil reaches two rows into it), stage 2 of band
+// b after stage 1 of band b + 1, and band b goes back as soon as its stage 2
+// is done, while later bands are still going up.  Each band is also copied
+// to the second state buffer on the device, whose ghost cells must hold the
+// uploaded values.  Periodic and partitioned grids, whose ghost strips are
+// refilled from the whole grid, take the three calls one after the other.
+int cl_pn_step_host(cl_pn *p, double dt, double dx, double dy, double *moments)
+{
+    if (!p || !moments)
+        return CL_ERR_ARG;
+    if (p->grid.init_cond == 2 || p->exchanged > 0) {
+        int rc = cl_pn_set_state(p, moments);
+        if (rc == CL_OK)
+            rc = cl_pn_step(p, dt, dx, dy);
+        if (rc == CL_OK)
+            rc = cl_pn_get_state(p, moments);
+        return rc;
+    }
+    if (p->cur != p->U) {
+        p->err = "a step starts after stage 2";
+        return CL_ERR_STATE;
+    }
+    if (!p->up) {
+        PN_TRY(p, cudaStreamCreateWithFlags(&p->up, cudaStreamNonBlocking));
+        PN_TRY(p, cudaStreamCreateWithFlags(&p->down, cudaStreamNonBlocking));
+        PN_TRY(p, cudaEventCreateWithFlags(&p->evStart, cudaEventDisableTiming));
+        for (int b = 0; b < kPnMaxBands; b++) {
+            PN_TRY(p, cudaEventCreateWithFlags(&p->evUp[b], cudaEventDisableTiming));
+            PN_TRY(p, cudaEventCreateWithFlags(&p->evDone[b], cudaEventDisableTiming));
+        }
+    }
+    const int nx = p->NX - 4;
+    // about 12 bands of whole tile rows (the last one takes the remainder)
+    const int bandRows = std::max(kTI, (nx + 11) / 12 / kTI * kTI);
+    const int bands = std::min(kPnMaxBands, (nx + bandRows - 1) / bandRows);
+    int r0[kPnMaxBands + 1];
+    for (int b = 0; b < bands; b++)
+        r0[b] = b * bandRows;
+    r0[bands] = nx;
+    const size_t rowBytes = (size_t)p->NY * p->n * 8, rowElems = (size_t)p->NY * p->n;
+    // cell rows copied with band b: its interior rows, plus the ghost rows
+    // before the first band and after the last
+    auto first = [&](int b) { return (size_t)(b == 0 ? 0 : 2 + r0[b]); };
+    auto last = [&](int b) { return (size_t)(b == bands - 1 ? p->NX : 2 + r0[b + 1]); };
+    cudaError_t e = cudaSuccess;
+    auto run = [&](cudaError_t r) {
+        if (e == cudaSuccess)
+            e = r;
+    };
+    run(cudaEventRecord(p->evStart, p->stream));
+    run(cudaStreamWaitEvent(p->up, p->evStart, 0));
+    run(cudaStreamWaitEvent(p->down, p->evStart, 0));
+    for (int b = 0; b < bands; b++) {
+        const size_t off = first(b) * rowElems, bytes = (last(b) - first(b)) * rowBytes;
+        run(cudaMemcpyAsync(p->U + off, moments + off, bytes, cudaMemcpyHostToDevice, p->up));
+        run(cudaMemcpyAsync(p->V + off, p->U + off, bytes, cudaMemcpyDeviceToDevice, p->up));
+        run(cudaEventRecord(p->evUp[b], p->up));
+    }
+    auto stage2 = [&](int b) {
+        p->cur = p->V;
+        run(pn_launch(p, 2, dt, dx, dy, r0[b], r0[b + 1]));
+        run(cudaEventRecord(p->evDone[b], p->stream));
+        run(cudaStreamWaitEvent(p->down, p->evDone[b], 0));
+        const size_t off = first(b) * rowElems, bytes = (last(b) - first(b)) * rowBytes;
+        run(cudaMemcpyAsync(moments + off, p->U + off, bytes, cudaMemcpyDeviceToHost, p->down));
+    };
+    for (int b = 0; b < bands && e == cudaSuccess; b++) {
+        run(cudaStreamWaitEvent(p->stream, p->evUp[std::min(b + 1, bands - 1)], 0));
+        p->cur = p->U;
+        run(pn_launch(p, 1, dt, dx, dy, r0[b], r0[b + 1]));
+        if (b > 0)
+            stage2(b - 1);
+    }
+    if (e == cudaSuccess)
+        stage2(bands - 1);
+    p->cur = p->U;
+    run(cudaStreamSynchronize(p->down));
+    run(cudaStreamSynchronize(p->up));
+    run(cudaStreamSynchronize(p->stream));
+    if (e != cudaSuccess) {
+        p->err = std::string("host-state step: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
     return CL_OK;
 }
 

@@ -308,6 +308,13 @@ int cl_pn_stream(cl_pn *p, void **stream);
  * every stage, so the interior is the reference's). */
 int cl_pn_get_state(cl_pn *p, double *moments);
 int cl_pn_set_state(cl_pn *p, const double *moments);
+/* One RK2 step (MomentSolver::update, moment_update.cpp:151-247) on a state
+ * held in host memory ([NX*NY][n], ghosts included, read and overwritten),
+ * equal to cl_pn_set_state, cl_pn_step, cl_pn_get_state.  Bands of rows go
+ * up, are stepped and come back while later bands are still going up, which
+ * needs page-locked host memory to take effect.  Periodic or partitioned
+ * grids run the three calls in turn.  Blocks until the step is done. */
+int cl_pn_step_host(cl_pn *p, double dt, double dx, double dy, double *moments);
 /* As cl_halo_*, on the state the next stage reads (moment_boundaries.cpp). */
 int cl_pn_halo_counts(const cl_pn *p, long long counts[4]);
 int cl_pn_halo_pack(cl_pn *p, double *const bufs[4]);
