@@ -13,7 +13,13 @@ state (646,416 cells x 28 moments x {u, alpha}) is 290 MB, larger than L2,
 so no explicit L2 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
-                  [--workload m6_800|pp6_800|m4_lattice_200|m2_50]
+                  [--workload m6_800|pp6_800|m4_lattice_200|m2_50|pn6_800|batch_2e20]
+
+`value` is timed with CUDA events on the library's stream (kernels only,
+state resident on the device).  The `e2e` figure steps a state held in
+page-locked host memory through the host-state C ABI call (cl_step_host, or
+cl_pn_step_host for the linear solver), which copies it up and back every
+step with the copies overlapped with the kernels.
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle restatement, OpenMP over all host threads) on the same deck.
