@@ -88,6 +88,7 @@ def lib():
             "cl_destroy": (None, [vp]),
             "cl_last_error": (C.c_char_p, [vp]),
             "cl_global_error": (C.c_char_p, []),
+            "cl_error_text": (C.c_char_p, [C.c_int]),
             "cl_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "cl_step_async": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "cl_step_timed": (C.c_int, [vp, C.c_double, C.c_double, C.c_double,
@@ -196,6 +197,11 @@ def _check(rc, msg_fn):
 
 def global_error():
     return lib().cl_global_error().decode()
+
+
+def error_text(code):
+    """The library's message for a return code (cl_error_text)."""
+    return lib().cl_error_text(int(code)).decode()
 
 
 def launch_count():
@@ -753,11 +759,41 @@ def solve_batch_noalloc(angular, options, d_u, d_alpha, count, d_iters=None, d_r
     """Batched opt() on device arrays without any device allocation by the
     library (cl_solve_batch_noalloc): for callers whose device memory is owned
     by another allocator.  Arguments are torch tensors or raw addresses."""
+    n = angular.n
+    # torch tensors are checked here (the kernel would read and write past a
+    # short, strided, host or wrongly typed buffer); raw addresses are the
+    # caller's responsibility, as in the C ABI
+    _check_device_tensor(d_u, "d_u", "float64", count * n, required=True)
+    _check_device_tensor(d_alpha, "d_alpha", "float64", count * n, required=True)
+    _check_device_tensor(d_iters, "d_iters", "int32", count)
+    _check_device_tensor(d_reg, "d_reg", "float64", count)
+    _check_device_tensor(d_status, "d_status", "int32", count)
+    if stream is not None and hasattr(stream, "cuda_stream"):   # torch.cuda.Stream
+        stream = stream.cuda_stream
     ptr = lambda t: None if t is None else (t.data_ptr() if hasattr(t, "data_ptr") else int(t))
     _check(lib().cl_solve_batch_noalloc(C.byref(angular._a), C.byref(options), count, ptr(d_u),
                                         ptr(d_alpha), ptr(d_iters), ptr(d_reg), ptr(d_status),
-                                        ptr(stream)),
+                                        None if stream is None else int(stream)),
            lib().cl_noalloc_last_error)
+
+
+def _check_device_tensor(t, name, dtype, elements, required=False):
+    """Raises ValueError unless t is None (optional arguments), a raw address,
+    or a contiguous CUDA tensor of `dtype` with at least `elements` entries."""
+    if t is None:
+        if required:
+            raise ValueError("%s is required" % name)
+        return
+    if not hasattr(t, "data_ptr"):
+        return
+    if str(t.dtype) != "torch." + dtype:
+        raise ValueError("%s must be %s, got %s" % (name, dtype, t.dtype))
+    if not t.is_cuda:
+        raise ValueError("%s must be a CUDA tensor" % name)
+    if not t.is_contiguous():
+        raise ValueError("%s must be contiguous" % name)
+    if t.numel() < elements:
+        raise ValueError("%s holds %d elements, %d needed" % (name, t.numel(), elements))
 
 
 def _fp(a):

@@ -386,19 +386,7 @@ int sm_count()
     return sms;
 }
 
-const char *error_text(int code)
-{
-    switch (code) {
-    case CL_ERR_U0:
-        return "u[0] < 0";
-    case CL_ERR_MAXREG:
-        return "Max regularization achieved.";
-    case CL_ERR_TIMEOUT:
-        return "device wait timed out";
-    default:
-        return "device error";
-    }
-}
+const char *error_text(int code) { return cl_error_text(code); }
 
 }  // namespace
 
@@ -439,6 +427,28 @@ struct cl_ctx {
 extern "C" {
 
 const char *cl_global_error(void) { return g_global_err.c_str(); }
+
+const char *cl_error_text(int code)
+{
+    switch (code) {
+    case CL_OK:
+        return "no error";
+    case CL_ERR_ARG:
+        return "bad argument or unsupported configuration";
+    case CL_ERR_CUDA:
+        return "CUDA error or no usable device";
+    case CL_ERR_U0:
+        return "u[0] < 0";
+    case CL_ERR_MAXREG:
+        return "Max regularization achieved.";
+    case CL_ERR_TIMEOUT:
+        return "device wait timed out";
+    case CL_ERR_STATE:
+        return "call order or state error";
+    default:
+        return "device error";
+    }
+}
 
 int cl_angular_create(int order, int quad_order, int use_gaunt, cl_angular *out)
 {

@@ -226,8 +226,10 @@ extern "C" int cl_solve_batch_noalloc(const cl_angular *ang, const cl_options *o
     if (e != cudaSuccess)
         return fail(CL_ERR_CUDA, cudaGetErrorString(e));
     if (herr[0] != 0) {
-        std::snprintf(g_msg, sizeof(g_msg), "%s (vector %d)",
-                      herr[0] == CL_ERR_U0 ? "u[0] < 0" : "Max regularization achieved.", herr[1]);
+        if (herr[1] >= 0)
+            std::snprintf(g_msg, sizeof(g_msg), "%s (vector %d)", cl_error_text(herr[0]), herr[1]);
+        else
+            std::snprintf(g_msg, sizeof(g_msg), "%s", cl_error_text(herr[0]));
         return herr[0];
     }
     return CL_OK;

@@ -47,6 +47,12 @@ enum { CL_MN = 0, CL_PPN = 1 };            /* opt/opt.h:34-37 */
 enum { CL_FP64 = 0, CL_MIXED = 1 };        /* arithmetic of the Hessian assembly */
 #define CL_NUM_REG 5                       /* opt/opt.h:39-40 */
 
+/* Message of a return code (CL_OK and every CL_ERR_*; "device error" for
+ * anything else).  The texts of CL_ERR_U0 and CL_ERR_MAXREG are the
+ * reference's own abort messages (opt.cpp:97-101, opt.cpp:256-261).  Needs
+ * no device. */
+const char *cl_error_text(int code);
+
 /* Angular discretisation: momopt_init.cpp:88-259.  Arrays are owned by the
  * library and released by cl_angular_free(). */
 typedef struct {
@@ -366,7 +372,12 @@ int cl_run_deck(const char *deck_path, const char *out_dir, int max_steps);
  * holds until exit.  Configurations whose padded basis does not fit are
  * rejected with CL_ERR_ARG (message from cl_noalloc_last_error()); M6 at
  * Q = 40 with the Gaunt table fits.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
+ * array's device address, and the first call of each moment order and
+ * Gaunt/no-Gaunt combination loads that kernel instance; with CUDA's lazy
+ * module loading that load is where the array and the kernel image are
+ * placed in device memory, and it may synchronise the device.  So make one
+ * warm-up call per configuration at set-up, before any stream capture; later
+ * calls of that configuration allocate nothing.
  * All calls share the array, so calls that overlap on the GPU (several
  * streams or threads at once) race; the call waits for its own work on
  * `stream` (a cudaStream_t, null = legacy default stream) before returning.

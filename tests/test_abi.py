@@ -127,3 +127,30 @@ def test_wrong_solver_type(tmp_path):
     with pytest.raises(cb.ClosuresError) as e:
         cb.Solver(str(d), str(tmp_path))
     assert "Solver type does not exist" in str(e.value)
+
+
+def test_error_text_by_code():
+    """Each return code has its own message: a timed-out device wait is not
+    reported as an exhausted regularisation ladder (both the context and the
+    allocation-free entry point take their messages from cl_error_text)."""
+    assert cb.error_text(cb.CL_ERR_U0) == "u[0] < 0"
+    assert cb.error_text(cb.CL_ERR_MAXREG) == "Max regularization achieved."
+    assert cb.error_text(cb.CL_ERR_TIMEOUT) == "device wait timed out"
+    assert cb.error_text(-99) == "device error"
+    texts = {cb.error_text(c) for c in (cb.CL_OK, cb.CL_ERR_ARG, cb.CL_ERR_CUDA, cb.CL_ERR_U0,
+                                        cb.CL_ERR_MAXREG, cb.CL_ERR_TIMEOUT, cb.CL_ERR_STATE)}
+    assert len(texts) == 7
+
+
+def test_noalloc_wrapper_checks_tensors():
+    """solve_batch_noalloc refuses tensors the kernel would overrun or
+    misread, before anything reaches the library."""
+    a = cb.Angular(2, 8, 0)
+    o = cb.make_options()
+    u64 = torch.zeros((4, a.n), dtype=torch.float64)
+    with pytest.raises(ValueError, match="float64"):
+        cb.solve_batch_noalloc(a, o, u64.float(), u64, 4)
+    with pytest.raises(ValueError, match="CUDA"):
+        cb.solve_batch_noalloc(a, o, u64, u64, 4)
+    with pytest.raises(ValueError, match="required"):
+        cb.solve_batch_noalloc(a, o, None, u64, 4)

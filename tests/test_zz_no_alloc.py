@@ -65,6 +65,34 @@ def test_noalloc_matches_allocating_entry_point_twice():
     _check(ref2, got2)
 
 
+def test_noalloc_repeat_call_allocates_nothing():
+    """After one warm-up call of a configuration (which loads its kernel
+    instance and places the fixed array), a further call leaves the device's
+    free memory unchanged: the entry point itself allocates nothing."""
+    import torch
+
+    a = cb.Angular(3, 20, 1)
+    count = 400
+    u, _ = cb.sample_moment_vectors(a, count, seed=31, s_range=(0.1, 2.0))
+    opts = cb.make_options(tol=1e-8)
+    dev = torch.device("cuda", 0)
+    d_u0 = torch.from_numpy(u).to(dev)
+    d_a0 = torch.from_numpy(cb.isotropic_alpha(a.n, count)).to(dev)
+    d_u, d_a = d_u0.clone(), d_a0.clone()
+    d_it = torch.zeros(count, dtype=torch.int32, device=dev)
+    cb.solve_batch_noalloc(a, opts, d_u, d_a, count, d_it)   # warm-up call
+    first = d_u.clone()
+    d_u.copy_(d_u0)
+    d_a.copy_(d_a0)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(dev)[0]
+    cb.solve_batch_noalloc(a, opts, d_u, d_a, count, d_it, stream=torch.cuda.current_stream(dev))
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info(dev)[0]
+    assert free_after == free_before
+    assert torch.equal(d_u, first)
+
+
 def test_noalloc_rejects_oversized_configuration():
     import torch
 
