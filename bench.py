@@ -48,24 +48,7 @@ import decks  # noqa: E402
 
 METRIC = "Mn cell-solves/s at ||grad||<=1e-8 and steps/s: NN warm-start vs plain, 1 B200"
 
-WORKLOADS = {
-    # the M6 / PP6 800x800 pulse (configs of the headline)
-    "m6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
-                   gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
-                   moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
-                   moment_type="mn"),
-    "pp6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
-                    gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
-                    moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
-                    moment_type="ppn"),
-    # M4 lattice, 200x200 on [-3.5,3.5]^2, Q=30
-    "m4_lattice_200": dict(num_cells_x=200, num_cells_y=200, a_x=-3.5, b_x=3.5, a_y=-3.5,
-                           b_y=3.5, init_cond="lattice", floor=1e-10, moment_order=4,
-                           quad_order=30, tol=1e-8, use_gaunt=1, t_final=3.2),
-    # M2 50x50 Gaussian, Q=20 (the reference's CPU-runnable case)
-    "m2_50": dict(num_cells_x=50, num_cells_y=50, gaussian_sigma=0.4, floor=1e-4,
-                  moment_order=2, quad_order=20, tol=1e-8, use_gaunt=0, t_final=0.5),
-}
+WORKLOADS = decks.WORKLOADS
 
 
 def flops_per_iteration(n, n2, nq, use_gaunt, nnz):
@@ -147,7 +130,7 @@ def dist_setup():
     return world, rank, local
 
 
-def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1, contraction="pairs"):
+def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1, contraction="pairs", tune=True):
     """The workload's deck; with nodes > 1 the grid and domain are widened
     nodes times in x and split into nodes x 1 partitions, so every node holds
     the workload's grid."""
@@ -163,6 +146,8 @@ def write_deck(tmpdir, workload, precision="fp64", opt_type=0, nodes=1, contract
         kw["extra"]["MOMOPT_GPU_PRECISION"] = "mixed"
     if contraction == "single":
         kw["extra"]["MOMOPT_GPU_CONTRACTION"] = "single"
+    if not tune:
+        kw["extra"]["MOMOPT_GPU_TUNE"] = "0"
     decks.write_deck(path, decks.deck_text(**kw))
     return path
 
@@ -174,9 +159,10 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def run_oracle_steps(deck, max_steps, budget_s):
+def run_oracle_steps(deck, max_steps, budget_s, skip=0):
     """The reference algorithm on the host cores (oracle restatement):
-    full RK2 steps of the deck from t = 0.  Returns (steps, seconds, solves)."""
+    `skip` untimed RK2 steps of the deck from t = 0, then up to max_steps
+    timed ones within about budget_s.  Returns (steps, seconds, solves)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     threads = cpu_threads()
     os.environ["OMP_NUM_THREADS"] = str(threads)
@@ -184,6 +170,8 @@ def run_oracle_steps(deck, max_steps, budget_s):
     pyoracle.build()
     g = pyoracle.GridSolver(deck)
     C = g.NX * g.NY
+    if skip > 0:
+        g.steps(skip)
     done, t_total = 0, 0.0
     while done < max_steps:
         t0 = time.perf_counter()
@@ -230,14 +218,94 @@ def run_oracle_cb_sample(deck, w, opt_type, budget_s):
         count = int(count * min(8.0, max(2.0, budget_s / max(secs, 1e-3))))
 
 
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "closures_ref")
+
+
+def run_reference_build(w, side, steps, threads, moment=False):
+    """The reference's own program (oracle/_ref/closures_ref: its main.cpp,
+    solvers and OpenMP loops, compiled from its sources) on a centred
+    side x side sub-grid of the workload's deck -- the same cell size, time
+    step, closure and initial pulse -- timed as the difference of two runs
+    that stop at T_FINAL = 0.5 dt and (steps + 0.5) dt, so that start-up,
+    set-up and output cancel.  Returns (seconds for `steps` RK2 steps,
+    cells with ghosts)."""
+    nx = w["num_cells_x"]
+    dx = (w.get("b_x", 1.5) - w.get("a_x", -1.5)) / nx
+    cx = 0.5 * (w.get("b_x", 1.5) + w.get("a_x", -1.5))
+    cy = 0.5 * (w.get("b_y", 1.5) + w.get("a_y", -1.5))
+    half = 0.5 * side * dx
+    sub = dict(w, num_cells_x=side, num_cells_y=side, a_x=cx - half, b_x=cx + half, a_y=cy - half,
+               b_y=cy + half)
+    if moment:
+        # moment_init.cpp:69
+        dt = sub.get("cfl_factor", 0.9) * 0.5 * dx
+    else:
+        dt = decks.max_dt(sub)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+    secs = []
+    for k in (0.5, steps + 0.5):
+        with tempfile.TemporaryDirectory() as d:
+            kw = dict(sub, t_final=k * dt)
+            text = decks.moment_deck_text(**kw) if moment else decks.deck_text(**kw)
+            decks.write_deck(os.path.join(d, "input.deck"), text)
+            t0 = time.perf_counter()
+            r = subprocess.run([REF_BIN], cwd=d, env=env, stdout=subprocess.DEVNULL,
+                               stderr=subprocess.DEVNULL)
+            secs.append(time.perf_counter() - t0)
+            if r.returncode != 0:
+                raise RuntimeError("reference program exited with %d" % r.returncode)
+    return max(secs[1] - secs[0], 1e-9), (side + 4) ** 2
+
+
 def reference_arm(args, world, rank):
     if rank != 0:
         return 0
+    w = WORKLOADS[args.workload]
+    if os.path.exists(REF_BIN):
+        return reference_build_arm(args, world, w)
     with tempfile.TemporaryDirectory() as tmp:
         deck = write_deck(tmp, args.workload)
-        steps, secs, solves, threads = run_oracle_steps(deck, args.steps, budget_s=150.0)
+        # the native arm's headline window: --t-start, then W warm-up steps
+        dt = decks.max_dt(w)
+        skip = (int(round(args.t_start / dt)) if args.t_start > 0 else 0) + args.warmup
+        steps, secs, solves, threads = run_oracle_steps(deck, args.steps, budget_s=100.0, skip=skip)
     value = solves / secs
-    w = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-solves/s",
+        "n_gpus": world, "steps": steps, "warmup": skip, "ms_per_step": 1e3 * secs / steps,
+        "steps_per_s": steps / secs, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+                   "moment_order": w["moment_order"], "quad_order": w["quad_order"],
+                   "use_gaunt": w["use_gaunt"], "tol": w["tol"], "t_start": skip * dt},
+        "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "RK2 steps %d..%d of the deck (the native arm's headline window: "
+                                   "%d untimed steps from t=0 first), full grid"
+                                   % (skip + 1, skip + steps, skip)},
+        "e2e": {"value": value, "unit": "cell-solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def reference_build_arm(args, world, w):
+    """--impl reference with the compiled reference: its OpenMP program on
+    all host threads, on a bounded sample of the workload (a centred
+    sub-grid; see run_reference_build)."""
+    threads_all = cpu_threads()
+    side = REF_SAMPLE_SIDE.get(args.workload, 64)
+    steps = 1
+    tried = {}
+    for th in sorted({1, threads_all}):
+        secs_th, C = run_reference_build(w, side, steps, th)
+        tried[th] = secs_th
+    # the faster of one thread and all threads: the reference's per-cell
+    # dynamic schedule can make all threads slower than one
+    threads = min(tried, key=tried.get)
+    secs = tried[threads]
+    value = 2 * C * steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-solves/s",
         "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * secs / steps,
@@ -245,15 +313,27 @@ def reference_arm(args, world, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
                    "moment_order": w["moment_order"], "quad_order": w["quad_order"],
-                   "use_gaunt": w["use_gaunt"], "tol": w["tol"]},
-        "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads,
-                         "kind": "port",
-                         "sample": "first %d RK2 step(s) of the deck from t=0, full grid" % steps},
+                   "use_gaunt": w["use_gaunt"], "tol": w["tol"], "t_start": 0.0,
+                   "sample_grid": [side, side]},
+        "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads, "kind": "reference",
+                         "sample": "the reference's own program (its sources compiled -O3 -fopenmp "
+                                   "-DUSE_OPENMP with a GSL shim and OpenBLAS) on the centred %dx%d "
+                                   "sub-grid of the deck (same cell size, time step and pulse), "
+                                   "RK2 step 1 from t=0, %d OpenMP thread(s): the faster of 1 and all %d"
+                                   % (side, side, threads, threads_all),
+                         "by_threads": {str(k): 2 * C * steps / v for k, v in tried.items()}},
         "e2e": {"value": value, "unit": "cell-solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# The compiled reference spends most of a step in its flux loop, which
+# dispatches every cell of every direction separately (schedule(dynamic,1),
+# momopt_update.cpp:119-128), so a step of the full 800 x 800 grid takes tens
+# of minutes on the host; the bounded sample is a centred sub-grid.
+REF_SAMPLE_SIDE = {"m6_800": 96, "pp6_800": 96, "m4_lattice_200": 96, "m2_50": 50}
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
@@ -303,6 +383,340 @@ def train_grid_mlp(cb, torch, w, n, harvest, args):
             "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean())}
 
 
+def full_run_steps(t_final, dt):
+    """Steps of main.cpp:204-230 for one output interval: dt until t reaches
+    t_final, the last one shortened.  Returns (steps, dt of the last step)."""
+    t, k, last = 0.0, 0, dt
+    while t < t_final:
+        t += dt
+        k += 1
+        if t > t_final:
+            last = t_final - (t - dt)
+            t = t_final
+    return k, last
+
+
+def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
+    """One GPU, one domain: the headline window (W warm-up steps after
+    --t-start, then K timed steps), and unless --quick a window of K steps
+    near 0.9 t_final and the whole run to t_final (time to solution), all
+    on the same simulation."""
+    ctx = solver.context()
+    stream = ctx.stream()
+    dt, dx, dy = solver.max_dt, solver.dx, solver.dy
+    C = solver.NX * solver.NY
+    C_int = solver.nx * solver.ny
+    n = solver.n
+    nfull, last_dt = full_run_steps(solver.t_final, dt)
+    per_iter = flops_per_iteration(n, ang.n2, ang.nq, w["use_gaunt"], nnz)
+    if args.opt_type != 0:
+        # the change of basis adds the two triangular solves of
+        # H_P = T^-1 H_M T^-T and the basis update T <- T L (n^3 each)
+        per_iter += 3.0 * n ** 3
+    peak = cb.fp64_peak_tflops()
+    interior = np.zeros((solver.NX, solver.NY), bool)
+    interior[2:-2, 2:-2] = True
+
+    def advance(k):
+        """k captured-graph steps; device ms between events on the library stream."""
+        if k <= 0:
+            return 0.0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            ctx.step_async(dt, dx, dy)
+        e1.record(stream)
+        ctx.sync()
+        return e0.elapsed_time(e1)
+
+    def window(k, t_start):
+        """k steps kernel by kernel (CUDA events around every kernel)."""
+        s0 = solver.stats()
+        km = np.zeros(4)
+        for _ in range(k):
+            km += np.array(ctx.step_timed(dt, dx, dy))
+        s1 = solver.stats()
+        it = ctx.last_iterations()
+        solves = 2 * C * k
+        iters = s1["total_iter"] - s0["total_iter"]
+        trials = s1["total_trials"] - s0["total_trials"]
+        newton_ms = float(km[0] + km[2])
+        flux_ms = float(km[1] + km[3])
+        device_ms = float(km.sum())
+        f_newton = iters * per_iter + trials * flops_per_trial(n, ang.nq)
+        f_flux = 2 * k * flops_flux_stage(C, C_int, n, ang.nq)
+        return {
+            "t_start": t_start, "steps": k,
+            "value": solves / (device_ms * 1e-3),
+            "value_interior": 2 * C_int * k / (device_ms * 1e-3),
+            "ms_per_step": device_ms / k, "steps_per_s": 1e3 * k / device_ms,
+            "iter_mean": iters / solves, "trials_per_solve": trials / solves,
+            "fallback_restarts": s1["fallbacks"] - s0["fallbacks"],
+            "kernel_ms": {"newton": newton_ms, "flux": flux_ms},
+            "newton_tflops": f_newton / (newton_ms * 1e-3) / 1e12,
+            "flux_tflops": f_flux / (flux_ms * 1e-3) / 1e12,
+            "newton_frac": f_newton / (newton_ms * 1e-3) / 1e12 / peak,
+            "iter_hist_last_stage": np.bincount(np.minimum(it.ravel(), 20), minlength=21).tolist(),
+            "iter_hist_last_stage_interior": np.bincount(np.minimum(it[interior], 20), minlength=21).tolist(),
+            "_device_ms": device_ms,
+        }
+
+    step = 0
+    full_ms = 0.0
+    s_begin = solver.stats()
+    n_adv = int(round(args.t_start / dt)) if args.t_start > 0 else 0
+    full_ms += advance(n_adv)
+    step += n_adv
+    full_ms += advance(args.warmup)
+    step += args.warmup
+    # launch shapes: the autotuner times its candidates on this state
+    tuning = {"headline": ctx.tune() if not args.no_tune else ctx.tuning()}
+    head_state = ctx.get_state() if not args.no_cpu_baseline else None
+
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = cb.launch_count()
+    t0 = time.perf_counter()
+    head = window(args.steps, step * dt)
+    wall = time.perf_counter() - t0
+    launches = cb.launch_count() - launches0
+    clocks = sampler.stop()
+    full_ms += head["_device_ms"]
+    step += args.steps
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state from pinned host memory, runs the RK2 step and reads it back;
+    # the device state is put back afterwards so the run continues from the
+    # end of the headline window
+    e2e_steps = max(1, min(args.steps, 5))
+    saved_m, saved_a = ctx.get_state()
+    hm = torch.empty((C, n), dtype=torch.float64).pin_memory().numpy()
+    ha = torch.empty((C, n), dtype=torch.float64).pin_memory().numpy()
+    hm[:] = saved_m.reshape(C, n)
+    ha[:] = saved_a.reshape(C, n)
+    s_e2e0 = solver.stats()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.step_host(dt, dx, dy, hm, ha)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t1
+    s_e2e1 = solver.stats()
+    e2e_iters = s_e2e1["total_iter"] - s_e2e0["total_iter"]
+    e2e_trials = s_e2e1["total_trials"] - s_e2e0["total_trials"]
+    ctx.set_state(saved_m, saved_a)
+    state_bytes = 2 * C * n * 8
+
+    late, full, late_state, nn = None, None, None, None
+    if not args.quick:
+        n_late = max(step + 2, int(round(args.late_t * nfull)))
+        full_ms += advance(n_late - 2 - step)
+        # the learned start's training pairs: the two steps before the window
+        harvest = []
+        for _ in range(2):
+            full_ms += advance(1)
+            if args.newton_compare:
+                dm, da = cb_device_state_clone(ctx, torch, C, n)
+                harvest.append((dm, da))
+        step = n_late
+        if not args.no_tune:
+            tuning["late"] = ctx.tune()
+        late_state = ctx.get_state()
+        late = window(args.steps, step * dt)
+        full_ms += late["_device_ms"]
+        step += args.steps
+        if args.newton_compare and args.opt_type == 0 and args.precision == "fp64":
+            plain_end = ctx.get_state()
+            s_nn0 = solver.stats()
+            nn = nn_compare(args, cb, torch, ctx, w, n, harvest, late_state, plain_end, late, window,
+                            step * dt - args.steps * dt)
+            ctx.set_warm_start(None)
+            ctx.set_state(*plain_end)
+            s_nn1 = solver.stats()
+            # the comparison's windows are not part of the run
+            e2e_iters += s_nn1["total_iter"] - s_nn0["total_iter"]
+            e2e_trials += s_nn1["total_trials"] - s_nn0["total_trials"]
+        del harvest
+        full_ms += advance(nfull - 1 - step)
+        km_last = ctx.step_timed(last_dt, dx, dy)
+        full_ms += float(sum(km_last))
+        step = nfull
+        s_full1 = solver.stats()
+        solves = 2 * C * nfull
+        full = {"steps": nfull, "t_final": solver.t_final, "last_dt": last_dt,
+                "device_s": full_ms * 1e-3, "steps_per_s": nfull / (full_ms * 1e-3),
+                "value": solves / (full_ms * 1e-3), "value_interior": 2 * C_int * nfull / (full_ms * 1e-3),
+                "iter_mean": (s_full1["total_iter"] - s_begin["total_iter"] - e2e_iters) / solves,
+                "trials_per_solve": (s_full1["total_trials"] - s_begin["total_trials"] - e2e_trials) / solves,
+                "max_iter": s_full1["max_iter"],
+                "timing": "graph steps timed by CUDA events on the library stream, the two windows "
+                          "kernel by kernel; the e2e steps after the headline window are not part of "
+                          "it (the state is restored after them)"}
+
+    cpu = None
+    if not args.no_cpu_baseline and args.opt_type == 0:
+        cpu = cpu_window_sample(deck, head_state, "headline window (t = %.5f)" % head["t_start"])
+        if late_state is not None and late is not None:
+            cpu["late"] = cpu_window_sample(deck, late_state, "late window (t = %.5f)" % late["t_start"])
+    elif not args.no_cpu_baseline:
+        cells, secs, threads = run_oracle_cb_sample(deck, w, args.opt_type, budget_s=20.0)
+        cpu = {"value": cells / secs, "unit": "cell-solves/s", "cores": threads,
+               "kind": "port",
+               "sample": "%d random cells of the deck's first stage from t=0 (reference initial "
+                         "basis), %s on all %d host threads (oracle restatement, -O3 -fopenmp)"
+                         % (cells, "optcb" if args.opt_type == 1 else "optbfgs", threads)}
+
+    dominant = "newton" if head["kernel_ms"]["newton"] >= head["kernel_ms"]["flux"] else "flux"
+    achieved = head["newton_tflops"] if dominant == "newton" else head["flux_tflops"]
+    for win in (head, late):
+        if win is not None:
+            win.pop("_device_ms")
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": "cell-solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["ms_per_step"], "steps_per_s": head["steps_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64, Hessian-only tiles split tf32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
+                   "grid_per_gpu": [w["num_cells_x"], w["num_cells_y"]],
+                   "moment_order": w["moment_order"], "n": n, "quad_order": w["quad_order"],
+                   "nq": ang.nq, "use_gaunt": w["use_gaunt"], "tol": w["tol"],
+                   "moment_type": w.get("moment_type", "mn"),
+                   "newton": args.newton, "precision": args.precision, "opt_type": args.opt_type,
+                   "contraction": args.contraction, "t_start": head["t_start"],
+                   "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
+                   "parallelism": "single"},
+        "value_interior": head["value_interior"],
+        "iter_mean": head["iter_mean"], "trials_per_solve": head["trials_per_solve"],
+        "fallback_restarts": head["fallback_restarts"],
+        "kernel_ms": head["kernel_ms"],
+        "windows": {"headline": head, "late": late},
+        "full_run": full,
+        "nn": nn,
+        "tuning": tuning,
+        "roofline": {
+            "bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": NCU_TRAFFIC.get((args.workload, dominant)),
+            "peak_source": "FP64 DMMA m16n8k8 throughput measured live (cl_fp64_peak)",
+            "other": {"newton_tflops": head["newton_tflops"], "flux_tflops": head["flux_tflops"]},
+        },
+        "cpu_baseline": cpu,
+        "e2e": {"value": 2 * C * e2e_steps / e2e_s, "unit": "cell-solves/s",
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "steps": e2e_steps, "call": "cl_step_host (page-locked buffers)",
+                "ms_per_step": {"total": 1e3 * e2e_s / e2e_steps}},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    solver.close()
+    return 0
+
+
+def cb_device_state_clone(ctx, torch, C, n):
+    """Device copies of the context's moments and multipliers (through the
+    host; outside any timed region)."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    m, a = ctx.get_state()
+    return (torch.from_numpy(m.reshape(C, n)).to(dev), torch.from_numpy(a.reshape(C, n)).to(dev))
+
+
+def nn_compare(args, cb, torch, ctx, w, n, harvest, late_state, plain_end, plain_win, window, t_late):
+    """The learned warm start against the plain (previous-stage) start on the
+    late window: an n -> W -> W -> W -> n MLP (W = 512 for M6, 256 below)
+    trained by the library's own kernels on (u, alpha*) pairs from the two
+    steps before the window, each cell re-solved from its stored multipliers
+    so that the pair is consistent; then the same K steps from the same state
+    with the prediction for every cell and with the prediction only for the
+    cells whose previous stage took >= 3 iterations."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ang = cb.Angular(w["moment_order"], w["quad_order"], w["use_gaunt"])
+    bctx = cb.Context.for_batches(ang, cb.make_options(tol=w["tol"]))
+    t0 = time.perf_counter()
+    us, als = [], []
+    for du, da in harvest:
+        cnt = du.shape[0]
+        st = torch.zeros(cnt, dtype=torch.int32, device=dev)
+        rg = torch.zeros(cnt, dtype=torch.float64, device=dev)
+        bctx.solve_batch_device(du, da, None, rg, st, count=cnt)
+        torch.cuda.synchronize()
+        ok = (st == 0) & (rg == 0)
+        us.append(du[ok])
+        als.append(da[ok])
+    bctx.close()
+    u = torch.cat(us).contiguous()
+    al = torch.cat(als).contiguous()
+    harvest_s = time.perf_counter() - t0
+    sq = np.sqrt(np.pi)
+    x = (u / u[:, :1]).cpu().numpy()
+    tgt = al.cpu().numpy().copy()
+    tgt[:, 0] -= 2.0 * sq * np.log(u[:, 0].cpu().numpy())
+    lin = 2.0 * sq * x
+    lin[:, 0] = 2.0 * sq * np.log(0.5 / sq)
+    resid = tgt - lin
+    width = 512 if n >= 28 else 256
+    net = cb.MLP(n, width, seed=23)
+    net.set_output_scaling(resid.mean(axis=0), resid.std(axis=0) + 1e-3)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    losses = net.train(u, al, u.shape[0], steps=args.nn_steps, batch=4096, lr=1e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t1
+    pairs = int(u.shape[0])
+    del u, al, us, als
+    scale = np.abs(plain_end[0][:, :, :1])
+    out = {"network": "%d-%d-%d-%d-%d GELU, BF16 weights, FP32 accumulation" % (n, width, width, width, n),
+           "pairs": pairs, "pairs_from": "the 2 RK2 steps before the late window, re-solved",
+           "train_steps": args.nn_steps, "batch": 4096, "lr": 1e-3, "train_s": train_s, "harvest_s": harvest_s,
+           "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
+           "t_start": t_late,
+           "plain": {k: plain_win[k] for k in ("value", "iter_mean", "trials_per_solve", "ms_per_step",
+                                               "kernel_ms", "iter_hist_last_stage")},
+           "modes": {}}
+    for mode, min_it in (("every_cell", 0), ("cells_prev_iters_ge_3", 3)):
+        ctx.set_state(*late_state)
+        ctx.set_warm_start(net, min_prev_iters=min_it)
+        win = window(args.steps, t_late)
+        m_end, _ = ctx.get_state()
+        ctx.set_warm_start(None)
+        win.pop("_device_ms", None)
+        out["modes"][mode] = {
+            "value": win["value"], "speedup_vs_plain": win["value"] / plain_win["value"],
+            "iter_mean": win["iter_mean"], "trials_per_solve": win["trials_per_solve"],
+            "fallback_restarts": win["fallback_restarts"],
+            "fallback_rate": win["fallback_restarts"] / (2 * args.steps * m_end.shape[0] * m_end.shape[1]),
+            "ms_per_step": win["ms_per_step"], "kernel_ms": win["kernel_ms"],
+            "iter_hist_last_stage": win["iter_hist_last_stage"],
+            "max_rel_moment_diff_vs_plain": float(np.max(np.abs(m_end - plain_end[0]) / scale)),
+        }
+    return out
+
+
+def cpu_window_sample(deck, state, where):
+    """One RK2 step of the reference algorithm on the host cores (oracle
+    restatement, OpenMP over all threads) from the GPU run's state at the
+    start of a window: the CPU baseline on the same cells and time."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    threads = cpu_threads()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import pyoracle
+    pyoracle.build()
+    g = pyoracle.GridSolver(deck)
+    g.set_state(*state)
+    C = g.NX * g.NY
+    t0 = time.perf_counter()
+    g.steps(1)
+    secs = time.perf_counter() - t0
+    g.close()
+    return {"value": 2 * C / secs, "unit": "cell-solves/s", "cores": threads, "kind": "port",
+            "sample": "one RK2 step of the same deck from the GPU run's state at the %s, on all %d host "
+                      "threads (oracle restatement, -O3 -fopenmp)" % (where, threads)}
+
+
+
 def native_arm(args, world, rank, local):
     import torch
     import closures_b200 as cb
@@ -318,9 +732,11 @@ def native_arm(args, world, rank, local):
         dist.barrier()
     w = WORKLOADS[args.workload]
     tmp = tempfile.mkdtemp(prefix="bench_")
-    deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world,
-                      contraction=args.contraction)
     partitioned = world > 1 or args.partitioned
+    # one GPU: the bench runs the autotuner itself after the warm-up steps;
+    # partitioned nodes tune in their set-up (the deck default)
+    deck = write_deck(tmp, args.workload, args.precision, args.opt_type, nodes=world,
+                      contraction=args.contraction, tune=partitioned)
     if partitioned:
         solver = cb.NodeSolver(deck, tmp, node=rank, num_nodes=world)
     else:
@@ -344,6 +760,9 @@ def native_arm(args, world, rank, local):
             import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize()
+
+    if not partitioned:
+        return single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local)
 
     # warm-up (advances the simulation from t = 0)
     nn_info = None
@@ -847,9 +1266,22 @@ def main():
     ap.add_argument("--workload", default="m6_800",
                     choices=sorted(WORKLOADS) + ["batch_2e20"] + sorted(PN_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--t-start", type=float, default=0.0,
+                    help="grid workloads: advance to this time (untimed graph steps) before the "
+                         "warm-up steps and the headline window")
+    ap.add_argument("--late-t", type=float, default=0.9,
+                    help="single-GPU grid workloads: start of the second K-step window, as a "
+                         "fraction of the run's steps")
+    ap.add_argument("--quick", action="store_true",
+                    help="single-GPU grid workloads: the headline window only (no late window, "
+                         "no run to t_final, no learned-start comparison)")
     ap.add_argument("--newton", default="plain", choices=["plain", "nn"],
                     help="batch workload: start from the isotropic multiplier or a learned prediction")
-    ap.add_argument("--nn-steps", type=int, default=4000)
+    ap.add_argument("--nn-steps", type=int, default=20000)
+    ap.add_argument("--no-nn", dest="newton_compare", action="store_false",
+                    help="single-GPU grid workloads: skip the learned-start comparison on the late window")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (no autotuner)")
     ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1, 2],
                     help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton, "
                          "2: BFGS sub-iterations in the change of basis)")

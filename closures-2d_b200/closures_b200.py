@@ -68,6 +68,30 @@ class cl_stats(C.Structure):
                 ("total_trials", C.c_int64), ("fallbacks", C.c_int64)]
 
 
+class cl_tuning(C.Structure):
+    _fields_ = [("newton_warps", C.c_int), ("newton_ctas", C.c_int), ("newton_contraction", C.c_int),
+                ("flux_contraction", C.c_int), ("from_cache", C.c_int), ("ncand", C.c_int),
+                ("cand_kernel", C.c_int * 8), ("cand_warps", C.c_int * 8),
+                ("cand_contraction", C.c_int * 8), ("cand_ms", C.c_float * 8)]
+
+
+_CONTRACTION_NAMES = {0: "pairs", 1: "single"}
+
+
+def _tuning_dict(t):
+    cands = []
+    for i in range(t.ncand):
+        cands.append({"kernel": "newton" if t.cand_kernel[i] == 1 else "flux",
+                      "warps": t.cand_warps[i],
+                      "contraction": _CONTRACTION_NAMES.get(t.cand_contraction[i]),
+                      "ms": float(t.cand_ms[i])})
+    return {"newton_warps": t.newton_warps, "newton_cells_per_cta": 4 * t.newton_warps,
+            "newton_ctas": t.newton_ctas,
+            "newton_contraction": _CONTRACTION_NAMES.get(t.newton_contraction),
+            "flux_contraction": _CONTRACTION_NAMES.get(t.flux_contraction),
+            "from_cache": bool(t.from_cache), "candidates": cands}
+
+
 _lib = None
 
 
@@ -98,6 +122,9 @@ def lib():
             "cl_set_state": (C.c_int, [vp, dp, dp]),
             "cl_step_host": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, dp, dp]),
             "cl_get_stats": (C.c_int, [vp, C.POINTER(cl_stats)]),
+            "cl_tune": (C.c_int, [vp, C.c_int, C.POINTER(cl_tuning)]),
+            "cl_get_tuning": (C.c_int, [vp, C.POINTER(cl_tuning)]),
+            "cl_set_launch_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
             "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
@@ -141,6 +168,9 @@ def lib():
             "cl_mlp_set_params": (C.c_int, [vp, C.POINTER(C.POINTER(C.c_float)),
                                             C.POINTER(C.POINTER(C.c_float))]),
             "cl_set_warm_start": (C.c_int, [vp, vp]),
+            "cl_set_warm_start_selective": (C.c_int, [vp, vp, C.c_int]),
+            "cl_tc_gemm_bf16": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp]),
+            "cl_mlp_predict_selected": (C.c_int, [vp, vp, vp, C.c_int, vp, C.c_int, vp]),
             "cl_solve_batch_noalloc": (C.c_int, [C.POINTER(cl_angular), C.POINTER(cl_options),
                                                  C.c_int, vp, vp, vp, vp, vp, vp]),
             "cl_noalloc_last_error": (C.c_char_p, []),
@@ -378,12 +408,41 @@ class Context:
                                               ptr(d_alpha), ptr(d_iters), ptr(d_reg), ptr(d_status)),
                self._err)
 
-    def set_warm_start(self, mlp):
-        """Predict alpha with `mlp` before every optimisation stage (None: off).
-        The context borrows the network's device buffers, so it keeps a
-        reference to `mlp` until the warm start is replaced or removed."""
-        _check(lib().cl_set_warm_start(self._ctx, mlp._m if mlp is not None else None), self._err)
+    def set_warm_start(self, mlp, min_prev_iters=0):
+        """Predict alpha with `mlp` before every optimisation stage (None: off);
+        with min_prev_iters > 0 only for the cells whose previous stage took at
+        least that many iterations.  The context borrows the network's device
+        buffers, so it keeps a reference to `mlp` until the warm start is
+        replaced or removed."""
+        _check(lib().cl_set_warm_start_selective(self._ctx, mlp._m if mlp is not None else None,
+                                                 int(min_prev_iters)), self._err)
         self._warm = mlp
+
+    def tune(self, use_cache=False):
+        """Runs the launch-shape autotuner on the current state (cl_tune) and
+        returns what it chose and timed (with use_cache, a cached choice for
+        this configuration is applied without timing)."""
+        t = cl_tuning()
+        _check(lib().cl_tune(self._ctx, int(bool(use_cache)), C.byref(t)), self._err)
+        return _tuning_dict(t)
+
+    def tuning(self):
+        """The launch shapes in use (cl_get_tuning)."""
+        t = cl_tuning()
+        _check(lib().cl_get_tuning(self._ctx, C.byref(t)), self._err)
+        return _tuning_dict(t)
+
+    def set_launch_shape(self, newton_warps=8, newton_contraction=0, flux_contraction=0):
+        _check(lib().cl_set_launch_shape(self._ctx, newton_warps, newton_contraction, flux_contraction),
+               self._err)
+
+    def stream(self):
+        """The context's CUDA stream as a torch.cuda.ExternalStream (for
+        events and stream ordering with torch work)."""
+        import torch
+        st = C.c_void_p()
+        _check(lib().cl_stream(self._ctx, C.byref(st)), self._err)
+        return torch.cuda.ExternalStream(st.value, device=torch.device("cuda", torch.cuda.current_device()))
 
     def device_state(self):
         m, a = C.c_void_p(), C.c_void_p()
@@ -794,6 +853,21 @@ def _check_device_tensor(t, name, dtype, elements, required=False):
         raise ValueError("%s must be contiguous" % name)
     if t.numel() < elements:
         raise ValueError("%s holds %d elements, %d needed" % (name, t.numel(), elements))
+
+
+def tc_gemm_bf16(A, B):
+    """C = A . B^T (FP32) for BF16 CUDA tensors A [M x K], B [N x K] on the
+    tensor-memory GEMM of the network (cl_tc_gemm_bf16)."""
+    import torch
+    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16 and A.is_cuda and B.is_cuda
+    A, B = A.contiguous(), B.contiguous()
+    M, K = A.shape
+    N = B.shape[0]
+    assert B.shape[1] == K
+    C_ = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    torch.cuda.synchronize()
+    _check(lib().cl_tc_gemm_bf16(A.data_ptr(), B.data_ptr(), M, N, K, C_.data_ptr()), lib().cl_global_error)
+    return C_
 
 
 def _fp(a):

@@ -5,7 +5,12 @@
 // kernels want, one stream and the captured RK2 graph.
 #include "closures_gpu.h"
 
+#include <algorithm>
+#include <array>
 #include <atomic>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -404,6 +409,7 @@ struct cl_ctx {
     int *hErr = nullptr;              // pinned [2]
     int *dIters = nullptr;            // [C] iterations of each cell in the last stage
     cl_mlp *warm = nullptr;           // learned warm start (null: previous stage's alpha)
+    int warmMinIters = 0;             // > 0: predict only cells whose previous stage took this many iterations
     double *dAlphaPred = nullptr;     // [C][n] predicted starts when warm is set
     double *dP2M = nullptr, *dAlphaP = nullptr;   // change-of-basis state per cell (opt type 1)
     double *dCbScratch = nullptr;     // working basis per Newton slot (opt type 1)
@@ -421,6 +427,14 @@ struct cl_ctx {
     double *bU = nullptr, *bA = nullptr, *bR = nullptr;
     int *bI = nullptr, *bS = nullptr;
     long long bCap = 0;
+    // autotuner: the other contraction layout (built on first use) and the
+    // host angular data it is built from; which basis each kernel reads
+    DeviceBasis B2;
+    int newtonB2 = 0, fluxB2 = 0;
+    int angN = 0, angN2 = 0, angNq = 0, angGaunt = 0, angNnz = 0;
+    std::vector<double> aw, axi, aeta, ap, agval;
+    std::vector<int> agoff, agidx;
+    cl_tuning tuning{};
     std::string err;
 };
 
@@ -573,6 +587,20 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         ctx->err = std::string("basis upload: ") + cudaGetErrorString(ce);
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
+    ctx->angN = ang->n;
+    ctx->angN2 = ang->n2;
+    ctx->angNq = ang->nq;
+    ctx->angGaunt = gauntNewton;
+    ctx->angNnz = ang->gaunt_nnz;
+    ctx->aw.assign(ang->w, ang->w + ang->nq);
+    ctx->axi.assign(ang->xi, ang->xi + ang->nq);
+    ctx->aeta.assign(ang->eta, ang->eta + ang->nq);
+    ctx->ap.assign(ang->p, ang->p + (size_t)ang->nq * ang->n2);
+    if (gauntNewton && ang->gaunt_off) {
+        ctx->agoff.assign(ang->gaunt_off, ang->gaunt_off + ang->n * ang->n + 1);
+        ctx->agidx.assign(ang->gaunt_idx, ang->gaunt_idx + ang->gaunt_nnz);
+        ctx->agval.assign(ang->gaunt_val, ang->gaunt_val + ang->gaunt_nnz);
+    }
     if (cudaMalloc(&ctx->dMom, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dAlpha, C * n * 8) != cudaSuccess ||
         cudaMalloc(&ctx->dOld, C * n * 8) != cudaSuccess || cudaMalloc(&ctx->dSigT, C * 8) != cudaSuccess ||
         cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
@@ -589,6 +617,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     cudaMemcpy(ctx->dSigS, sigma_s, C * 8, cudaMemcpyHostToDevice);
     cudaMemset(ctx->dStats, 0, sizeof(DevStats));
     cudaMemset(ctx->dErr, 0, 2 * sizeof(int));
+    cudaMemset(ctx->dIters, 0, C * sizeof(int));
     ctx->hErr[0] = ctx->hErr[1] = 0;
 
     NewtonArgs &a = ctx->nargs;
@@ -692,6 +721,10 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         ctx->err = std::string("set-up: ") + cudaGetErrorString(cudaGetLastError());
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
+    ctx->tuning.newton_warps = a.nw;
+    ctx->tuning.newton_ctas = ctx->nCtas;
+    ctx->tuning.newton_contraction = ctx->B.paired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
+    ctx->tuning.flux_contraction = ctx->B.fluxPaired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
     *out = ctx;
     return CL_OK;
 }
@@ -707,6 +740,7 @@ void cl_destroy(cl_ctx *ctx)
     if (ctx->graph)
         cudaGraphDestroy(ctx->graph);
     ctx->B.release();
+    ctx->B2.release();
     cudaFree(ctx->dMom);
     cudaFree(ctx->dAlpha);
     cudaFree(ctx->dOld);
@@ -741,6 +775,23 @@ void cl_destroy(cl_ctx *ctx)
     delete ctx;
 }
 
+// The learned starts of a stage on `st`: every cell, or the cells whose
+// previous stage took at least warmMinIters iterations.  Returns the kernel
+// launches it issued (for the launch count) or -1.
+static int enqueue_prediction(cl_ctx *ctx, cudaStream_t st)
+{
+    const int chunks = (int)((ctx->C + (1 << 18) - 1) >> 18);
+    if (ctx->warmMinIters > 0) {
+        if (cl_mlp_predict_selected(ctx->warm, ctx->dMom, ctx->dIters, ctx->warmMinIters, ctx->dAlphaPred,
+                                    (int)ctx->C, st) != CL_OK)
+            return -1;
+        return 1 + 6 * chunks;
+    }
+    if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, st) != CL_OK)
+        return -1;
+    return 2 + 4 * chunks;
+}
+
 // Enqueues RK stage `stage` (0 or 1) on the context's stream: [periodic
 // ghost copy], [warm-start prediction], K1, K2+K3 (stage 1 also the Heun
 // average).  The stage's work counter must be zero when K1 starts.
@@ -754,9 +805,10 @@ static cudaError_t enqueue_stage(cl_ctx *ctx, int stage, double dt, double dx, d
         *nk += 2;
     }
     if (ctx->warm) {
-        if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
+        const int k = enqueue_prediction(ctx, ctx->stream);
+        if (k < 0)
             return cudaErrorLaunchFailure;
-        *nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+        *nk += k;
     }
     NewtonArgs a = ctx->nargs;
     a.prob[0].count = (int)ctx->C;
@@ -873,9 +925,10 @@ int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms)
             nk += 2;
         }
         if (ctx->warm && e == cudaSuccess) {
-            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, ctx->stream) != CL_OK)
+            const int k = enqueue_prediction(ctx, ctx->stream);
+            if (k < 0)
                 e = cudaErrorLaunchFailure;
-            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+            nk += k < 0 ? 0 : k;
         }
         NewtonArgs a = ctx->nargs;
         a.prob[0].count = (int)ctx->C;
@@ -1089,9 +1142,10 @@ int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, 
             nk += 2;
         }
         if (ctx->warm && e == cudaSuccess) {
-            if (cl_mlp_predict(ctx->warm, ctx->dMom, ctx->dAlphaPred, (int)ctx->C, 2, nullptr, S) != CL_OK)
+            const int k = enqueue_prediction(ctx, S);
+            if (k < 0)
                 run(cudaErrorLaunchFailure);
-            nk += 2 + 4 * ((int)((ctx->C + (1 << 18) - 1) >> 18));
+            nk += k < 0 ? 0 : k;
         }
         NewtonArgs a = ctx->nargs;
         a.prob[0].u = ctx->dMom;
@@ -1158,10 +1212,401 @@ int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, 
     return read_device_error(ctx);
 }
 
-int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m)
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner of the launch shapes (cl_tune): K1 cells per CTA / warps and the
+// Hessian tile layout, K2+K3 tile layout.  Candidates run on copies of the
+// context's state; the median of three timed launches decides.
+
+static void invalidate_graph(cl_ctx *ctx)
+{
+    if (ctx->exec) {
+        cudaGraphExecDestroy(ctx->exec);
+        ctx->exec = nullptr;
+    }
+    if (ctx->graph) {
+        cudaGraphDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+}
+
+// Builds the other contraction layout (both kernels) into ctx->B2 once.
+static int ensure_alt_basis(cl_ctx *ctx)
+{
+    if (ctx->B2.P)
+        return CL_OK;
+    int paired = 0;
+    if (ctx->opt.moment_type == CL_MN && ctx->opt.precision == CL_FP64 && !ctx->B.paired) {
+        int pnt = 0, pnbk = 0;
+        paired_counts(ctx->angN, ctx->angN2, ctx->angGaunt, pnt, pnbk);
+        paired = newton_pair_supported(pnt, pnbk) ? 1 : 0;
+    }
+    const int fluxPaired = ctx->B.fluxPaired ? 0 : 1;
+    cudaError_t e = build_device_basis(ctx->B2, ctx->angN, ctx->angN2, ctx->angNq, ctx->angGaunt, ctx->aw.data(),
+                                       ctx->axi.data(), ctx->aeta.data(), ctx->ap.data(),
+                                       ctx->agoff.empty() ? nullptr : ctx->agoff.data(),
+                                       ctx->agidx.empty() ? nullptr : ctx->agidx.data(),
+                                       ctx->agval.empty() ? nullptr : ctx->agval.data(), ctx->angNnz, paired,
+                                       fluxPaired);
+    if (e != cudaSuccess) {
+        ctx->B2.release();
+        ctx->err = std::string("tuner basis: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return CL_OK;
+}
+
+// Newton arguments of the context with the basis `B` and `nw` warps per
+// CTA; returns false where that shape has no instance.
+static bool newton_shape(const cl_ctx *ctx, const DeviceBasis &B, int nw, NewtonArgs &a)
+{
+    a = ctx->nargs;
+    NewtonProblem keep = a.prob[0];
+    a.prob[0] = make_problem(B);
+    a.prob[0].P2M = keep.P2M;
+    a.prob[0].alphaP = keep.alphaP;
+    a.nw = nw;
+    if (plan_newton(a) != 0 || a.ntf == 0 || (B.paired && a.ntExact == 0))
+        return false;
+    return prepare_newton(a) == cudaSuccess;
+}
+
+static void flux_basis(FluxArgs &f, const DeviceBasis &B)
+{
+    f.P = B.Pf;
+    f.xi = B.xi;
+    f.eta = B.eta;
+    f.cxw = B.cxw;
+    f.cyw = B.cyw;
+    f.nb = B.nbF;
+    f.paired = B.fluxPaired;
+    f.nbe = B.nbeF;
+    f.binv = B.fbinv;
+    f.ldPf = B.ldPf;
+    f.nqp = B.nqpF;
+}
+
+static float median3(float *v)
+{
+    std::sort(v, v + 3);
+    return v[1];
+}
+
+struct TuneScratch {
+    double *u = nullptr, *a = nullptr;
+    int *it = nullptr, *err = nullptr;
+    unsigned *q = nullptr;
+    DevStats *st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~TuneScratch()
+    {
+        cudaFree(u);
+        cudaFree(a);
+        cudaFree(it);
+        cudaFree(err);
+        cudaFree(q);
+        cudaFree(st);
+        if (e0)
+            cudaEventDestroy(e0);
+        if (e1)
+            cudaEventDestroy(e1);
+    }
+};
+
+// Median K1 time (ms) of `a` over the context's state (copies); < 0 if a
+// launch failed or reported an error.
+static float time_newton(cl_ctx *ctx, NewtonArgs a, TuneScratch &S)
+{
+    const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
+    a.prob[0].count = (int)C;
+    a.prob[0].u = S.u;
+    a.prob[0].alpha = S.a;
+    a.prob[0].iters = S.it;
+    a.prob[0].regs = nullptr;
+    a.prob[0].status = nullptr;
+    a.prob[0].alphaStart = nullptr;
+    a.prob[0].queue = S.q;
+    a.prob[0].first = 0;
+    a.momentsOld = nullptr;
+    a.stats = S.st;
+    a.err = S.err;
+    const int grid = sm_count() * newton_ctas_per_sm(a);
+    float ms[3] = {0, 0, 0};
+    cudaStream_t st = ctx->stream;
+    for (int r = 0; r < 4; r++) {
+        if (cudaMemcpyAsync(S.u, ctx->dMom, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(S.a, ctx->dAlpha, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemsetAsync(S.q, 0, sizeof(unsigned), st) != cudaSuccess ||
+            cudaMemsetAsync(S.err, 0, 2 * sizeof(int), st) != cudaSuccess)
+            return -1.0f;
+        cudaEventRecord(S.e0, st);
+        if (launch_newton(a, grid, st) != cudaSuccess)
+            return -1.0f;
+        g_launches++;
+        cudaEventRecord(S.e1, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess)
+            return -1.0f;
+        int herr[2] = {0, 0};
+        cudaMemcpy(herr, S.err, sizeof(herr), cudaMemcpyDeviceToHost);
+        if (herr[0] != 0)
+            return -1.0f;
+        if (r > 0)
+            cudaEventElapsedTime(&ms[r - 1], S.e0, S.e1);
+    }
+    return median3(ms);
+}
+
+static float time_flux(cl_ctx *ctx, FluxArgs f, TuneScratch &S)
+{
+    const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
+    f.moments = S.u;
+    f.alpha = ctx->dAlpha;
+    f.momentsOld = nullptr;
+    f.dt = 1e-6;
+    f.dx = f.dy = 1.0;
+    if (plan_flux(f) != 0 || prepare_flux(f) != cudaSuccess)
+        return -1.0f;
+    float ms[3] = {0, 0, 0};
+    cudaStream_t st = ctx->stream;
+    for (int r = 0; r < 4; r++) {
+        if (cudaMemcpyAsync(S.u, ctx->dMom, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return -1.0f;
+        cudaEventRecord(S.e0, st);
+        if (launch_flux(f, st) != cudaSuccess)
+            return -1.0f;
+        g_launches++;
+        cudaEventRecord(S.e1, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess)
+            return -1.0f;
+        if (r > 0)
+            cudaEventElapsedTime(&ms[r - 1], S.e0, S.e1);
+    }
+    return median3(ms);
+}
+
+// Makes the shapes current: K1 with `nw` warps on the Newton layout
+// `ncontr`, K2+K3 on the flux layout `fcontr`.
+static int apply_shape(cl_ctx *ctx, int nw, int ncontr, int fcontr)
+{
+    const int wantNP = ncontr == CL_CONTRACT_PAIRS, wantFP = fcontr == CL_CONTRACT_PAIRS;
+    if ((wantNP != ctx->B.paired || wantFP != ctx->B.fluxPaired) && ensure_alt_basis(ctx) != CL_OK)
+        return CL_ERR_CUDA;
+    const DeviceBasis *bn = (wantNP == ctx->B.paired) ? &ctx->B : (ctx->B2.P && ctx->B2.paired == wantNP) ? &ctx->B2 : nullptr;
+    const DeviceBasis *bf = (wantFP == ctx->B.fluxPaired) ? &ctx->B
+                            : (ctx->B2.Pf && ctx->B2.fluxPaired == wantFP) ? &ctx->B2 : nullptr;
+    if (!bn || !bf) {
+        ctx->err = "launch shape: that contraction layout does not exist for this configuration";
+        return CL_ERR_ARG;
+    }
+    NewtonArgs a;
+    if (!newton_shape(ctx, *bn, nw, a)) {
+        ctx->err = "launch shape: no Newton instance for that shape";
+        return CL_ERR_ARG;
+    }
+    FluxArgs f = ctx->fargs;
+    flux_basis(f, *bf);
+    if (plan_flux(f) != 0 || prepare_flux(f) != cudaSuccess) {
+        ctx->err = "launch shape: flux layout";
+        return CL_ERR_ARG;
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->nargs = a;
+    ctx->nCtas = sm_count() * newton_ctas_per_sm(a);
+    ctx->fargs = f;
+    ctx->newtonB2 = (bn == &ctx->B2);
+    ctx->fluxB2 = (bf == &ctx->B2);
+    if (!ctx->newtonB2 && !ctx->fluxB2)
+        ctx->B2.release();
+    invalidate_graph(ctx);
+    ctx->tuning.newton_warps = nw;
+    ctx->tuning.newton_ctas = ctx->nCtas;
+    ctx->tuning.newton_contraction = ncontr;
+    ctx->tuning.flux_contraction = fcontr;
+    return CL_OK;
+}
+
+// Cache of tuned shapes: key -> (nw, Newton contraction, flux contraction).
+static std::mutex g_tune_mutex;
+static std::map<std::string, std::array<int, 3>> g_tune_cache;
+static bool g_tune_file_read = false;
+
+static std::string tune_key(const cl_ctx *ctx)
+{
+    char buf[160];
+    snprintf(buf, sizeof(buf), "n%d_n2%d_nq%d_gaunt%d_mt%d_prec%d_opt%d", ctx->angN, ctx->angN2, ctx->angNq,
+             ctx->angGaunt, ctx->opt.moment_type, ctx->opt.precision, ctx->opt.opt_type);
+    return buf;
+}
+
+static void tune_cache_load()
+{
+    if (g_tune_file_read)
+        return;
+    g_tune_file_read = true;
+    const char *path = getenv("CL_TUNE_CACHE");
+    if (!path || !*path)
+        return;
+    FILE *fp = fopen(path, "r");
+    if (!fp)
+        return;
+    char key[160];
+    int v[3];
+    while (fscanf(fp, "%159s %d %d %d", key, &v[0], &v[1], &v[2]) == 4)
+        g_tune_cache[key] = {v[0], v[1], v[2]};
+    fclose(fp);
+}
+
+static void tune_cache_store(const std::string &key, const std::array<int, 3> &v)
+{
+    g_tune_cache[key] = v;
+    const char *path = getenv("CL_TUNE_CACHE");
+    if (!path || !*path)
+        return;
+    FILE *fp = fopen(path, "a");
+    if (!fp)
+        return;
+    fprintf(fp, "%s %d %d %d\n", key.c_str(), v[0], v[1], v[2]);
+    fclose(fp);
+}
+
+extern "C" {
+
+int cl_get_tuning(cl_ctx *ctx, cl_tuning *out)
+{
+    if (!ctx || !out)
+        return CL_ERR_ARG;
+    *out = ctx->tuning;
+    return CL_OK;
+}
+
+int cl_set_launch_shape(cl_ctx *ctx, int newton_warps, int newton_contraction, int flux_contraction)
+{
+    if (!ctx || (newton_warps != 8 && newton_warps != 4) ||
+        (newton_contraction != CL_CONTRACT_PAIRS && newton_contraction != CL_CONTRACT_SINGLE) ||
+        (flux_contraction != CL_CONTRACT_PAIRS && flux_contraction != CL_CONTRACT_SINGLE))
+        return CL_ERR_ARG;
+    int rc = apply_shape(ctx, newton_warps, newton_contraction, flux_contraction);
+    if (rc == CL_OK) {
+        ctx->tuning.from_cache = 0;
+        ctx->tuning.ncand = 0;
+    }
+    return rc;
+}
+
+int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out)
 {
     if (!ctx)
         return CL_ERR_ARG;
+    const long long kMinCells = 16384;
+    if (ctx->C < kMinCells || ctx->nargs.optType != 0) {
+        // too small to time meaningfully, or a change-of-basis type: defaults
+        if (out)
+            *out = ctx->tuning;
+        return CL_OK;
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    tune_cache_load();
+    const std::string key = tune_key(ctx);
+    auto hit = g_tune_cache.find(key);
+    if (use_cache && hit != g_tune_cache.end()) {
+        int rc = apply_shape(ctx, hit->second[0], hit->second[1], hit->second[2]);
+        if (rc != CL_OK)
+            return rc;
+        ctx->tuning.from_cache = 1;
+        ctx->tuning.ncand = 0;
+        if (out)
+            *out = ctx->tuning;
+        return CL_OK;
+    }
+    int rc = ensure_alt_basis(ctx);
+    if (rc != CL_OK)
+        return rc;
+    const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
+    TuneScratch S;
+    if (cudaMalloc(&S.u, C * n * 8) != cudaSuccess || cudaMalloc(&S.a, C * n * 8) != cudaSuccess ||
+        cudaMalloc(&S.it, C * sizeof(int)) != cudaSuccess || cudaMalloc(&S.err, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&S.q, sizeof(unsigned)) != cudaSuccess || cudaMalloc(&S.st, sizeof(DevStats)) != cudaSuccess ||
+        cudaEventCreate(&S.e0) != cudaSuccess || cudaEventCreate(&S.e1) != cudaSuccess) {
+        ctx->err = "tuner scratch";
+        return CL_ERR_CUDA;
+    }
+    cl_tuning T = ctx->tuning;
+    T.ncand = 0;
+    T.from_cache = 0;
+    // K1 candidates: each existing Newton layout in each launch shape
+    float bestN = 1e30f;
+    int bestNw = ctx->tuning.newton_warps, bestNc = ctx->tuning.newton_contraction;
+    for (const DeviceBasis *B : {&ctx->B, &ctx->B2}) {
+        if (!B->P || (B == &ctx->B2 && B->paired == ctx->B.paired))
+            continue;
+        for (int nw : {8, 4}) {
+            NewtonArgs a;
+            if (!newton_shape(ctx, *B, nw, a))
+                continue;
+            const float ms = time_newton(ctx, a, S);
+            if (ms < 0 || T.ncand >= CL_TUNE_MAX)
+                continue;
+            const int contr = B->paired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
+            T.cand_kernel[T.ncand] = 1;
+            T.cand_warps[T.ncand] = nw;
+            T.cand_contraction[T.ncand] = contr;
+            T.cand_ms[T.ncand] = ms;
+            T.ncand++;
+            if (ms < bestN) {
+                bestN = ms;
+                bestNw = nw;
+                bestNc = contr;
+            }
+        }
+    }
+    // K2+K3 candidates: the two flux layouts
+    float bestF = 1e30f;
+    int bestFc = ctx->tuning.flux_contraction;
+    for (const DeviceBasis *B : {&ctx->B, &ctx->B2}) {
+        if (!B->Pf || (B == &ctx->B2 && B->fluxPaired == ctx->B.fluxPaired))
+            continue;
+        FluxArgs f = ctx->fargs;
+        flux_basis(f, *B);
+        const float ms = time_flux(ctx, f, S);
+        if (ms < 0 || T.ncand >= CL_TUNE_MAX)
+            continue;
+        const int contr = B->fluxPaired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
+        T.cand_kernel[T.ncand] = 2;
+        T.cand_warps[T.ncand] = 16;
+        T.cand_contraction[T.ncand] = contr;
+        T.cand_ms[T.ncand] = ms;
+        T.ncand++;
+        if (ms < bestF) {
+            bestF = ms;
+            bestFc = contr;
+        }
+    }
+    rc = apply_shape(ctx, bestNw, bestNc, bestFc);
+    if (rc != CL_OK)
+        return rc;
+    T.newton_warps = ctx->tuning.newton_warps;
+    T.newton_ctas = ctx->tuning.newton_ctas;
+    T.newton_contraction = bestNc;
+    T.flux_contraction = bestFc;
+    ctx->tuning = T;
+    tune_cache_store(key, {bestNw, bestNc, bestFc});
+    if (out)
+        *out = T;
+    return CL_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m) { return cl_set_warm_start_selective(ctx, m, 0); }
+
+int cl_set_warm_start_selective(cl_ctx *ctx, cl_mlp *m, int min_prev_iters)
+{
+    if (!ctx || min_prev_iters < 0)
+        return CL_ERR_ARG;
+    ctx->warmMinIters = m ? min_prev_iters : 0;
     if (m) {
         int rc = clb_mlp_reserve_for(m, (size_t)ctx->C);
         if (rc) {
@@ -1176,14 +1621,7 @@ int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m)
     }
     ctx->warm = m;
     // the captured step changes: re-capture at the next cl_step
-    if (ctx->exec) {
-        cudaGraphExecDestroy(ctx->exec);
-        ctx->exec = nullptr;
-    }
-    if (ctx->graph) {
-        cudaGraphDestroy(ctx->graph);
-        ctx->graph = nullptr;
-    }
+    invalidate_graph(ctx);
     return CL_OK;
 }
 

@@ -16,6 +16,9 @@
 #include "closures_gpu.h"
 
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include "tc_gemm.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -55,17 +58,26 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], unsigned a0, unsigned a1
 // [K x M] (TA = 1); B is [K x N] row-major (TB = 0) or [N x K] (TB = 1).
 // Epilogues: FP32 store; bias + GELU (pre-activation FP32, activation BF16);
 // bias (FP32).  Tiles 64 x 64 x 32, four warps of 32 x 32.
+// Mdev (nullable): the rows come from a device count, M = min(M, *Mdev - moff)
+// (a compacted selection whose size the host does not know); tiles past it
+// return at once.
 template <int TA, int TB, int EPI>
 __global__ void __launch_bounds__(128) gemm_kernel(const __nv_bfloat16 *__restrict__ A,
                                                    const __nv_bfloat16 *__restrict__ B, int M, int N, int K,
                                                    float *__restrict__ C, const float *__restrict__ bias,
-                                                   __nv_bfloat16 *__restrict__ Act)
+                                                   __nv_bfloat16 *__restrict__ Act, const int *Mdev, int moff)
 {
     __shared__ __align__(16) __nv_bfloat16 As[BM][BK + KPAD];
     __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + KPAD];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    if (Mdev) {
+        const int rem = *Mdev - moff;
+        M = rem < M ? (rem > 0 ? rem : 0) : M;
+        if (m0 >= M)
+            return;
+    }
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     float acc[2][4][4];
 #pragma unroll
@@ -263,19 +275,25 @@ __global__ void prep_kernel(const double *u, const double *alpha, int count, int
 // the fallback multipliers.  fallbackKind: 0 = keep alpha as given (previous
 // stage), 1 = isotropic alpha for this u0, 2 = write NaN so that the Newton
 // kernel's start falls back to its own multipliers.
+// With idx (nullable), row r of Y is cell idx[off + r] (rows past *cnt - off
+// are not there).
 __global__ void predict_out_kernel(const float *Y, const double *u, double *alpha, int count, int n,
                                    int momentType, double delta, const float *mean, const float *stdv,
-                                   int fallbackKind, int *fallbacks)
+                                   int fallbackKind, int *fallbacks, const int *idx = nullptr,
+                                   const int *cnt = nullptr, int off = 0)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= count)
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= count || (idx && off + r >= *cnt))
         return;
+    // Y row r; u and alpha rows of cell c (with an index list) or r
+    const int c = idx ? idx[off + r] : r;
+    const float *Yr = Y + (size_t)r * n;
     double u0 = u[(size_t)c * n];
     bool ok = u0 > 0.0;
     double a[32];
     for (int k = 0; k < n && ok; k++) {
         double x = u[(size_t)c * n + k] / u0;
-        double v = (double)Y[(size_t)c * n + k] * stdv[k] + mean[k] + alpha_linear(k, x, momentType);
+        double v = (double)Yr[k] * stdv[k] + mean[k] + alpha_linear(k, x, momentType);
         if (!isfinite(v))
             ok = false;
         a[k] = v;
@@ -306,14 +324,130 @@ __global__ void predict_out_kernel(const float *Y, const double *u, double *alph
 
 template <int TA, int TB, int EPI>
 cudaError_t gemm(const __nv_bfloat16 *A, const __nv_bfloat16 *B, int M, int N, int K, float *C, const float *bias,
-                 __nv_bfloat16 *Act, cudaStream_t s)
+                 __nv_bfloat16 *Act, cudaStream_t s, const int *Mdev = nullptr, int moff = 0)
 {
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    gemm_kernel<TA, TB, EPI><<<grid, 128, 0, s>>>(A, B, M, N, K, C, bias, Act);
+    gemm_kernel<TA, TB, EPI><<<grid, 128, 0, s>>>(A, B, M, N, K, C, bias, Act, Mdev, moff);
     return cudaGetLastError();
 }
 
+// Cells whose last optimisation took at least minIters iterations are listed
+// in idx (count in *cnt, order arbitrary); the others get a NaN start, so the
+// Newton kernel starts them from their own (previous-stage) multipliers.
+__global__ void select_kernel(const int *iters, int count, int minIters, int *idx, int *cnt, double *alpha, int n)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= count)
+        return;
+    if (iters[c] >= minIters)
+        idx[atomicAdd(cnt, 1)] = c;
+    else
+        alpha[(size_t)c * n] = __longlong_as_double(0x7ff8000000000000ll);
+}
+
+// Inputs x = u/u0 of the listed cells idx[off + r], r < min(rows, *cnt - off).
+__global__ void prep_idx_kernel(const double *u, const int *idx, const int *cnt, int off, int rows, int n,
+                                __nv_bfloat16 *X)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = i / n, k = i % n;
+    if (r >= rows || off + r >= *cnt)
+        return;
+    const size_t c = (size_t)idx[off + r];
+    X[i] = __float2bfloat16((float)(u[c * n + k] / u[c * n]));
+}
+
 int blocks(size_t n, int t = 256) { return (int)((n + t - 1) / t); }
+
+int round8(int x) { return (x + 7) / 8 * 8; }
+
+// x [rows x n] -> xp [rows x np] with zero columns n..np-1 (a row stride of a
+// multiple of 16 bytes, as the tensor-memory GEMM's TMA loads need)
+__global__ void pad_cols_kernel(const __nv_bfloat16 *x, int rows, int n, int np, __nv_bfloat16 *xp)
+{
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= (size_t)rows * np)
+        return;
+    const int r = (int)(i / np), k = (int)(i % np);
+    xp[i] = k < n ? x[(size_t)r * n + k] : __float2bfloat16(0.0f);
+}
+
+// W [K x N] FP32 row-major -> Wt [N x Kp] BF16 (the K-major B operand), zero
+// columns K..Kp-1
+__global__ void transpose_cast_kernel(const float *W, int K, int N, int Kp, __nv_bfloat16 *Wt)
+{
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= (size_t)N * Kp)
+        return;
+    const int c = (int)(i / Kp), k = (int)(i % Kp);
+    Wt[i] = k < K ? __float2bfloat16(W[(size_t)k * N + c]) : __float2bfloat16(0.0f);
+}
+
+// The driver's tensor-map encoder, through the runtime's entry-point query
+// (no link against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 2-D map of a row-major BF16 [rows x cols] matrix (cols a multiple of 8,
+// base 16-byte aligned) in boxes of boxRows x 64 with the 128 B swizzle;
+// reads past the matrix are zero.
+bool bf16_map(CUtensorMap *map, const __nv_bfloat16 *base, int rows, int cols, int boxRows)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || cols % 8 != 0 || ((uintptr_t)base & 15) != 0)
+        return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)clb::tc::BK, (cuuint32_t)boxRows};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int EPI>
+cudaError_t tc_gemm_bn(const CUtensorMap &ma, const CUtensorMap &mb, int M, int N, int K, float *Z, const float *bias,
+                       __nv_bfloat16 *Act, const int *Mdev, int moff, int *err, cudaStream_t s)
+{
+    static bool attr = false;
+    auto *k = clb::tc::tc_gemm_kernel<BN, EPI>;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, clb::tc::smem_bytes(BN));
+        if (e != cudaSuccess)
+            return e;
+        attr = true;
+    }
+    dim3 grid((N + BN - 1) / BN, (M + clb::tc::BM - 1) / clb::tc::BM);
+    k<<<grid, 128, clb::tc::smem_bytes(BN), s>>>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err);
+    return cudaGetLastError();
+}
+
+// Z (nullable) / Act (nullable) [M x N] = epilogue(A [M x K] . B [N x K]^T):
+// the tensor-memory GEMM (tc_gemm.cuh); K a multiple of 8.
+template <int EPI>
+cudaError_t tc_gemm(const __nv_bfloat16 *A, const __nv_bfloat16 *B, int M, int N, int K, float *Z, const float *bias,
+                    __nv_bfloat16 *Act, const int *Mdev, int moff, int *err, cudaStream_t s)
+{
+    const int bn = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+    CUtensorMap ma, mb;
+    if (!bf16_map(&ma, A, M, K, clb::tc::BM) || !bf16_map(&mb, B, N, K, bn))
+        return cudaErrorInvalidValue;
+    if (bn == 32)
+        return tc_gemm_bn<32, EPI>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err, s);
+    if (bn == 64)
+        return tc_gemm_bn<64, EPI>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err, s);
+    return tc_gemm_bn<128, EPI>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err, s);
+}
 
 }  // namespace
 
@@ -324,14 +458,19 @@ struct cl_mlp {
     float *W[kLayers] = {}, *b[kLayers] = {}, *mW[kLayers] = {}, *vW[kLayers] = {}, *mb[kLayers] = {},
           *vb[kLayers] = {}, *gW[kLayers] = {}, *gb[kLayers] = {};
     __nv_bfloat16 *W16[kLayers] = {};
+    __nv_bfloat16 *Wt16[kLayers] = {};   // [out x round8(in)] BF16, the K-major operand of the forward GEMMs
     float *mean = nullptr, *stdv = nullptr;  // device [n]
     std::vector<float> hmean, hstd;
     int adamStep = 0;
     // work buffers (grow only)
     size_t cap = 0;
-    __nv_bfloat16 *X = nullptr, *Act[kLayers] = {}, *dZ16 = nullptr;
+    __nv_bfloat16 *X = nullptr, *Xp = nullptr, *Act[kLayers] = {}, *dZ16 = nullptr;   // Xp: X padded to round8(n)
+    int *tcErr = nullptr;       // error word of the tensor-memory GEMM's bounded waits
+    bool keepZ = true;          // forward keeps the hidden pre-activations (training)
     float *Z[kLayers] = {}, *T = nullptr, *dA = nullptr, *dZ = nullptr, *loss = nullptr;
     int *fallbacks = nullptr;
+    int *sel = nullptr;         // selected cells (+ their count) of cl_mlp_predict_selected
+    size_t selCap = 0;
     cudaStream_t stream = nullptr;
     std::string err;
 };
@@ -341,6 +480,7 @@ static int mlp_reserve(cl_mlp *m, size_t rows)
     if (rows <= m->cap)
         return CL_OK;
     cudaFree(m->X);
+    cudaFree(m->Xp);
     cudaFree(m->dZ16);
     cudaFree(m->T);
     cudaFree(m->dA);
@@ -352,6 +492,7 @@ static int mlp_reserve(cl_mlp *m, size_t rows)
     }
     size_t w = (size_t)(m->width > m->n ? m->width : m->n);
     bool ok = cudaMalloc(&m->X, rows * m->n * sizeof(__nv_bfloat16)) == cudaSuccess &&
+              cudaMalloc(&m->Xp, rows * round8(m->n) * sizeof(__nv_bfloat16)) == cudaSuccess &&
               cudaMalloc(&m->dZ16, rows * w * sizeof(__nv_bfloat16)) == cudaSuccess &&
               cudaMalloc(&m->T, rows * m->n * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&m->dA, rows * w * sizeof(float)) == cudaSuccess &&
@@ -369,17 +510,25 @@ static int mlp_reserve(cl_mlp *m, size_t rows)
     return CL_OK;
 }
 
-// forward over `rows` inputs already in m->X; output pre-activations in Z[3]
-static cudaError_t mlp_forward(cl_mlp *m, int rows)
+// forward over `rows` inputs already in m->X (with Mdev: min(rows, *Mdev -
+// moff) of them); output pre-activations in Z[3]
+//
+// The layer GEMMs run on the tensor-memory path (tcgen05, tc_gemm.cuh): the
+// input padded to round8(n) columns, the weights as K-major BF16 copies.
+static cudaError_t mlp_forward(cl_mlp *m, int rows, const int *Mdev = nullptr, int moff = 0)
 {
-    cudaError_t e = cudaSuccess;
-    const __nv_bfloat16 *in = m->X;
+    const int np = round8(m->n);
+    pad_cols_kernel<<<blocks((size_t)rows * np), 256, 0, m->stream>>>(m->X, rows, m->n, np, m->Xp);
+    cudaError_t e = cudaGetLastError();
+    const __nv_bfloat16 *in = m->Xp;
     for (int l = 0; l < kLayers && e == cudaSuccess; l++) {
-        int K = m->dims[l], N = m->dims[l + 1];
+        const int K = round8(m->dims[l]), N = m->dims[l + 1];
         if (l < kLayers - 1)
-            e = gemm<0, 0, EPI_BIAS_GELU>(in, m->W16[l], rows, N, K, m->Z[l], m->b[l], m->Act[l], m->stream);
+            e = tc_gemm<clb::tc::EPI_BIAS_GELU>(in, m->Wt16[l], rows, N, K, m->keepZ ? m->Z[l] : nullptr, m->b[l],
+                                                 m->Act[l], Mdev, moff, m->tcErr, m->stream);
         else
-            e = gemm<0, 0, EPI_BIAS>(in, m->W16[l], rows, N, K, m->Z[l], m->b[l], nullptr, m->stream);
+            e = tc_gemm<clb::tc::EPI_BIAS>(in, m->Wt16[l], rows, N, K, m->Z[l], m->b[l], nullptr, Mdev, moff,
+                                            m->tcErr, m->stream);
         in = m->Act[l];
     }
     return e;
@@ -390,6 +539,8 @@ static cudaError_t mlp_sync_weights(cl_mlp *m)
     for (int l = 0; l < kLayers; l++) {
         size_t cnt = (size_t)m->dims[l] * m->dims[l + 1];
         cast_bf16_kernel<<<blocks(cnt), 256, 0, m->stream>>>(m->W[l], m->W16[l], cnt);
+        const int K = m->dims[l], N = m->dims[l + 1], Kp = round8(K);
+        transpose_cast_kernel<<<blocks((size_t)N * Kp), 256, 0, m->stream>>>(m->W[l], K, N, Kp, m->Wt16[l]);
     }
     return cudaGetLastError();
 }
@@ -429,6 +580,21 @@ static cudaError_t mlp_backward(cl_mlp *m, int rows, float *lossOut)
     return e;
 }
 
+// The tensor-memory GEMM's error word (a bounded wait that gave up), read
+// after the stream has been synchronised, and cleared.
+static int tc_error(cl_mlp *m)
+{
+    int h = 0;
+    if (cudaMemcpy(&h, m->tcErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return CL_ERR_CUDA;
+    if (h != 0) {
+        cudaMemset(m->tcErr, 0, sizeof(int));
+        m->err = "tensor-memory GEMM: a bounded wait timed out";
+        return CL_ERR_TIMEOUT;
+    }
+    return CL_OK;
+}
+
 extern "C" {
 
 int cl_mlp_create(int n, int width, int moment_type, double delta_ppn, unsigned long long seed, cl_mlp **out)
@@ -461,7 +627,9 @@ int cl_mlp_create(int n, int width, int moment_type, double delta_ppn, unsigned 
             v = U(rng) * sc;
         ok = cudaMalloc(&m->W[l], cnt * 4) == cudaSuccess && cudaMalloc(&m->mW[l], cnt * 4) == cudaSuccess &&
              cudaMalloc(&m->vW[l], cnt * 4) == cudaSuccess && cudaMalloc(&m->gW[l], cnt * 4) == cudaSuccess &&
-             cudaMalloc(&m->W16[l], cnt * 2) == cudaSuccess && cudaMalloc(&m->b[l], N * 4) == cudaSuccess &&
+             cudaMalloc(&m->W16[l], cnt * 2) == cudaSuccess &&
+             cudaMalloc(&m->Wt16[l], (size_t)N * round8(m->dims[l]) * 2) == cudaSuccess &&
+             cudaMalloc(&m->b[l], N * 4) == cudaSuccess &&
              cudaMalloc(&m->mb[l], N * 4) == cudaSuccess && cudaMalloc(&m->vb[l], N * 4) == cudaSuccess &&
              cudaMalloc(&m->gb[l], N * 4) == cudaSuccess;
         if (ok) {
@@ -474,7 +642,8 @@ int cl_mlp_create(int n, int width, int moment_type, double delta_ppn, unsigned 
         }
     }
     ok = ok && cudaMalloc(&m->mean, n * 4) == cudaSuccess && cudaMalloc(&m->stdv, n * 4) == cudaSuccess &&
-         cudaMalloc(&m->fallbacks, sizeof(int)) == cudaSuccess;
+         cudaMalloc(&m->fallbacks, sizeof(int)) == cudaSuccess && cudaMalloc(&m->tcErr, sizeof(int)) == cudaSuccess &&
+         cudaMemset(m->tcErr, 0, sizeof(int)) == cudaSuccess;
     if (!ok) {
         cl_mlp_destroy(m);
         return CL_ERR_CUDA;
@@ -505,6 +674,7 @@ void cl_mlp_destroy(cl_mlp *m)
         cudaFree(m->gW[l]);
         cudaFree(m->gb[l]);
         cudaFree(m->W16[l]);
+        cudaFree(m->Wt16[l]);
         cudaFree(m->Act[l]);
         cudaFree(m->Z[l]);
     }
@@ -517,6 +687,8 @@ void cl_mlp_destroy(cl_mlp *m)
     cudaFree(m->dZ);
     cudaFree(m->loss);
     cudaFree(m->fallbacks);
+    cudaFree(m->tcErr);
+    cudaFree(m->sel);
     if (m->stream)
         cudaStreamDestroy(m->stream);
     delete m;
@@ -607,7 +779,7 @@ int cl_mlp_train(cl_mlp *m, const double *d_u, const double *d_alpha, int count,
         m->err = std::string("training: ") + cudaGetErrorString(e);
         return CL_ERR_CUDA;
     }
-    return CL_OK;
+    return tc_error(m);
 }
 
 // Predicted multipliers for count vectors d_u (device, [count x n]) written to
@@ -633,7 +805,9 @@ int cl_mlp_predict(cl_mlp *m, const double *d_u, double *d_alpha, int count, int
         int rows = count - c0 < chunk ? count - c0 : chunk;
         prep_kernel<<<blocks((size_t)rows * m->n), 256, 0, st>>>(d_u + (size_t)c0 * m->n, nullptr, rows, m->n,
                                                                 m->momentType, m->mean, m->stdv, m->X, nullptr);
+        m->keepZ = false;
         e = mlp_forward(m, rows);
+        m->keepZ = true;
         predict_out_kernel<<<blocks(rows), 256, 0, st>>>(m->Z[kLayers - 1], d_u + (size_t)c0 * m->n,
                                                          d_alpha + (size_t)c0 * m->n, rows, m->n, m->momentType,
                                                          m->delta, m->mean, m->stdv, fallback_kind, m->fallbacks);
@@ -651,6 +825,84 @@ int cl_mlp_predict(cl_mlp *m, const double *d_u, double *d_alpha, int count, int
         return CL_ERR_CUDA;
     }
     return CL_OK;
+}
+
+// Predicted starts only for the cells whose last optimisation took at least
+// min_iters iterations (d_iters, device [count]); the other cells' starts are
+// NaN, so the Newton kernel starts them from their previous-stage
+// multipliers.  The selection is compacted on the device and the network runs
+// over it in chunks whose row counts the GEMMs read from device memory, so
+// the call needs no host synchronisation and can be captured in a graph.
+int cl_mlp_predict_selected(cl_mlp *m, const double *d_u, const int *d_iters, int min_iters, double *d_alpha,
+                            int count, void *stream)
+{
+    if (!m || !d_u || !d_iters || !d_alpha || count < 0 || min_iters < 1)
+        return CL_ERR_ARG;
+    if (count == 0)
+        return CL_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : m->stream;
+    const int chunk = 1 << 18;
+    int rc = mlp_reserve(m, count < chunk ? count : chunk);
+    if (rc)
+        return rc;
+    if (!m->sel || m->selCap < (size_t)count) {
+        cudaFree(m->sel);
+        m->sel = nullptr;
+        if (cudaMalloc(&m->sel, ((size_t)count + 1) * sizeof(int)) != cudaSuccess) {
+            m->err = "selection buffer";
+            return CL_ERR_CUDA;
+        }
+        m->selCap = count;
+    }
+    int *cnt = m->sel + count;
+    cudaStream_t keep = m->stream;
+    m->stream = st;
+    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(int), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(m->fallbacks, 0, sizeof(int), st);
+    select_kernel<<<blocks(count), 256, 0, st>>>(d_iters, count, min_iters, m->sel, cnt, d_alpha, m->n);
+    for (int c0 = 0; c0 < count && e == cudaSuccess; c0 += chunk) {
+        const int rows = count - c0 < chunk ? count - c0 : chunk;
+        prep_idx_kernel<<<blocks((size_t)rows * m->n), 256, 0, st>>>(d_u, m->sel, cnt, c0, rows, m->n, m->X);
+        m->keepZ = false;
+        e = mlp_forward(m, rows, cnt, c0);
+        m->keepZ = true;
+        predict_out_kernel<<<blocks(rows), 256, 0, st>>>(m->Z[kLayers - 1], d_u, d_alpha, rows, m->n, m->momentType,
+                                                         m->delta, m->mean, m->stdv, 2, m->fallbacks, m->sel, cnt,
+                                                         c0);
+    }
+    m->stream = keep;
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        m->err = std::string("selected predict: ") + cudaGetErrorString(e);
+        return CL_ERR_CUDA;
+    }
+    return CL_OK;
+}
+
+// The network's GEMM on its own (device pointers): C [M x N] FP32 = A [M x K]
+// . B [N x K]^T with BF16 A, B (row-major, K a multiple of 8).  Waits for the
+// result; for the numerics test of the tensor-memory path.
+int cl_tc_gemm_bf16(const void *d_A, const void *d_B, int M, int N, int K, float *d_C)
+{
+    if (!d_A || !d_B || !d_C || M < 1 || N < 1 || K < 8 || K % 8 != 0)
+        return CL_ERR_ARG;
+    int *err = nullptr;
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess)
+        return CL_ERR_CUDA;
+    cudaMemset(err, 0, sizeof(int));
+    cudaError_t e = tc_gemm<clb::tc::EPI_STORE>((const __nv_bfloat16 *)d_A, (const __nv_bfloat16 *)d_B, M, N, K, d_C,
+                                                 nullptr, nullptr, nullptr, 0, err, nullptr);
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    int h = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(err);
+    if (e != cudaSuccess)
+        return CL_ERR_CUDA;
+    return h ? CL_ERR_TIMEOUT : CL_OK;
 }
 
 // Gradient check support: loss and parameter gradients of one batch (host
@@ -687,7 +939,7 @@ int cl_mlp_loss_and_grads(cl_mlp *m, const double *u, const double *alpha, int r
         m->err = std::string("loss/grad: ") + cudaGetErrorString(e);
         return CL_ERR_CUDA;
     }
-    return CL_OK;
+    return tc_error(m);
 }
 
 // Parameters: W_l is [in x out] row-major (y = x W + b).  get/set copy FP32

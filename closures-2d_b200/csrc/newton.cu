@@ -20,7 +20,12 @@ int plan_newton(NewtonArgs &a)
         K2tot = kt > K2tot ? kt : K2tot;
         nMax = pb.n > nMax ? pb.n : nMax;
     }
-    a.T = 32;
+    if (a.nw == 0)
+        a.nw = kWarps;
+    if (a.nw != kWarps && a.nw != 4)
+        return -1;
+    const int nw = a.nw;
+    a.T = 4 * nw;   // 16-slot m-tiles x four q-groups of 8 directions = warps
     a.kq = 32;
     a.ntq = a.kq / 8;
     a.ldv = nbMax + 4;
@@ -42,6 +47,10 @@ int plan_newton(NewtonArgs &a)
     a.offInt = take((T * SI_N + 1) / 2);
     a.offFpart = take(T * a.ntq);
     a.offStat = take(kStatU64 + 1);
+    // the 4-warp shape reads the Gaunt table through L1 so that two CTAs fit
+    a.stageEll = (nw == kWarps) ? 1 : 0;
+    if (!a.stageEll)
+        ellRows = ellChunks = 0;
     a.offEllVal = take(ellRows * 32);
     a.offEllIdx = take((ellRows * 32 + 3) / 4);
     a.offEllPair = take((ellChunks * 32 + 3) / 4);
@@ -52,7 +61,7 @@ int plan_newton(NewtonArgs &a)
     exp_consts_init(a.ex);
     const int unionBase = off;
     const int ntiles2 = (T / 16) * (K2tot / 8);
-    a.tpw = (ntiles2 + kWarps - 1) / kWarps;
+    a.tpw = (ntiles2 + nw - 1) / nw;
     // fused contractions when every problem's G fits in 16 column tiles
     // (one warp per 16 slots x 8 quadrature rows of a 32-row chunk)
     const int nt2 = K2tot / 8;
@@ -61,16 +70,20 @@ int plan_newton(NewtonArgs &a)
     a.nbk = (a.ntf > 0 && a.nprob == 1) ? a.prob[0].nb / 8 : 0;
     if (a.mixed && a.ntExact == 0)
         return -2;
+    if (nw != kWarps && (a.ntExact == 0 || a.nprob != 1 || !a.prob[0].paired || a.mixed || a.optType != 0 ||
+                         !newton_pair4_supported(a.ntExact, a.nbk)))
+        return -1;   // the 4-warp shape: single-order direction-pair Newton only
     // phase-B region
     int offG = unionBase;
     int offH = offG + ((T * a.ldG + 1) & ~1);
-    int offVec = offH + ((kWarps * kMaxN * a.ldh + 1) & ~1);
-    int endB = offVec + kWarps * 64;
+    int offVec = offH + ((nw * kMaxN * a.ldh + 1) & ~1);
+    int endB = offVec + nw * 64;
 
     // phase-A region
     const int maxDoubles = (232448 - 1024) / 8;   // opt-in limit minus static shared
     if (a.ntf > 0) {
-        const int endA = unionBase + 3 * (a.kq * ldPMax + a.kq);   // three chunks
+        const int depth = (nw == kWarps) ? 3 : 2;
+        const int endA = unionBase + depth * (a.kq * ldPMax + a.kq);   // staged chunks
         const int end = endA > endB ? endA : endB;
         if (end <= maxDoubles) {
             a.doubleBuffer = 1;
@@ -86,6 +99,8 @@ int plan_newton(NewtonArgs &a)
         a.ntExact = a.nbk = 0;
         if (a.mixed)
             return -2;
+        if (nw != kWarps)
+            return -1;
     }
     for (int db = 1; db >= 0; db--) {
         int offP = unionBase;
@@ -122,10 +137,16 @@ static cudaError_t run(const NewtonArgs &a, int grid, cudaStream_t stream, int m
     }
     if (a.nprob == 1 && a.prob[0].paired) {
         // the direction-pair layout runs only its own fused instances
+        if (a.nw == 4)
+            return (a.ntf > 0 && a.ntExact > 0 && newton_run_exact_pair4(a, grid, stream, mode, occ, &e))
+                       ? e
+                       : cudaErrorInvalidValue;
         if (a.ntf > 0 && a.ntExact > 0 && newton_run_exact_pair(a, grid, stream, mode, occ, &e))
             return e;
         return cudaErrorInvalidValue;
     }
+    if (a.nw != kWarps)
+        return cudaErrorInvalidValue;
     if (a.ntf > 0 && a.ntExact > 0) {
         if (newton_run_exact_mn_a(a, grid, stream, mode, occ, &e) ||
             newton_run_exact_mn_b(a, grid, stream, mode, occ, &e) ||

@@ -100,6 +100,12 @@ struct NewtonArgs {
     double condHMaxBfgs;        // optType 2: MOMOPT_COND_H_MAX_BFGS
     int cbStride;               // doubles per slot of cbScratch (kCbSlotDoubles or kBfgsSlotDoubles)
     double *cbScratch;          // optType 1, 2: per-slot working state, [grid][T][cbStride]
+    // launch shape, set before plan_newton(): warps per CTA (0 or 8: 32
+    // slots, three staged chunks, one CTA per SM; 4: 16 slots, two staged
+    // chunks, the Gaunt table read through L1, two CTAs per SM -- fused
+    // direction-pair instances only)
+    int nw;
+    int stageEll;               // filled by plan_newton(): Gaunt table staged in shared memory
 };
 
 // Fills the layout fields from the problems' sizes; returns 0, -1 when the
@@ -110,6 +116,8 @@ int plan_newton(NewtonArgs &a);
 cudaError_t prepare_newton(const NewtonArgs &a);
 // A fused instance exists for the direction-pair layout with these counts.
 bool newton_pair_supported(int nt, int nbk);
+// ... and in the 4-warp launch shape.
+bool newton_pair4_supported(int nt, int nbk);
 // Launches the persistent kernel on `stream` over `grid` CTAs.
 cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream);
 int newton_ctas_per_sm(const NewtonArgs &a);
@@ -120,6 +128,7 @@ int newton_ctas_per_sm(const NewtonArgs &a);
 bool newton_run_generic(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_mn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_pair(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
+bool newton_run_exact_pair4(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_mn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_a(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);
 bool newton_run_exact_ppn_b(const NewtonArgs &a, int grid, cudaStream_t s, int mode, int *occ, cudaError_t *err);

@@ -1493,11 +1493,21 @@ constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on any wait for
 // are p(q) with the odd ones negated), and GEMM2 takes their weighted sum as
 // the A operand of the even column tiles and their difference for the odd
 // ones.  Each MMA so serves two directions.
-template <int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0>
+//
+// NW (warps per CTA) sets the launch shape: NW = 8 runs T = 32 slots (two
+// 16-slot m-tiles, q-group = warp / 2) with three chunk buffers, one CTA per
+// SM; NW = 4 runs T = 16 slots (one m-tile, q-group = warp) with two chunk
+// buffers, small enough for two CTAs per SM, so that one CTA's phase B runs
+// while the other's phase A keeps the tensor pipe busy.  Each slot's sums
+// are the same MMAs in the same order in both shapes.
+template <int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0, int NW = 8>
 __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int tid,
                                               int lane, int warp, unsigned &mbPhase)
 {
     static_assert(!PAIR || (PPN == 0 && MIX == 0), "direction pairs: Mn in FP64");
+    static_assert(NW == 8 || NW == 4, "launch shapes: 8 warps (32 slots) or 4 warps (16 slots)");
+    constexpr int MT = NW / 4;                  // 16-slot m-tiles: T = 16 MT
+    constexpr int DEPTH = (NW == 8) ? 3 : 2;    // staged chunk buffers
     const int g = lane >> 2, t4 = lane & 3;
     const int kq = a.kq, ldv = a.ldv, ldG = a.ldG;
     const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
@@ -1509,7 +1519,7 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     const int NT2 = (NT > 0) ? NT : NTH + (PPN ? nb / 8 : 0);
     const int nchunks = pb.nqp / kq;
     const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
-    const int mt = warp & 1, qg = warp >> 1;
+    const int mt = warp % MT, qg = warp / MT;
     const int r0 = mt * 16 + g, r1 = r0 + 8;
     const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
     const double *A0 = L.alpha + r0 * ldv + t4, *A1 = L.alpha + r1 * ldv + t4;
@@ -1552,7 +1562,7 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     auto abandon = [&]() {
         if (tid == 0)
             record_error(a.err, -5, -1);
-        for (int b = 0; b < 3; b++)
+        for (int b = 0; b < DEPTH; b++)
             if (pending & (1u << b))
                 wait_chunk(b);
         return false;
@@ -1701,19 +1711,39 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
         }
     };
     int bc = 0;   // buffer of chunk c
-    for (int c = 0; c + 1 < nchunks; c++) {
-        const int bn = (bc == 2) ? 0 : bc + 1, bf = (bn == 2) ? 0 : bn + 1;
-        const bool okWait = wait_chunk(bn);
-        // chunk c + 1 visible to all; every warp is done with chunk c - 1 (buffer bf)
-        if (__syncthreads_or(!okWait))
-            return abandon();
-        if (c + 2 < nchunks)
-            load_chunk(c + 2, bf);
-        double cs[4], co[4];
-        gemm1(L.P + bn * chunkDoubles, cs, co);
-        gemm2(L.P + bc * chunkDoubles);
-        weights(L.P + bn * chunkDoubles, cs, co, e, eg);
-        bc = bn;
+    if constexpr (DEPTH == 3) {
+        for (int c = 0; c + 1 < nchunks; c++) {
+            const int bn = (bc == 2) ? 0 : bc + 1, bf = (bn == 2) ? 0 : bn + 1;
+            const bool okWait = wait_chunk(bn);
+            // chunk c + 1 visible to all; every warp is done with chunk c - 1 (buffer bf)
+            if (__syncthreads_or(!okWait))
+                return abandon();
+            if (c + 2 < nchunks)
+                load_chunk(c + 2, bf);
+            double cs[4], co[4];
+            gemm1(L.P + bn * chunkDoubles, cs, co);
+            gemm2(L.P + bc * chunkDoubles);
+            weights(L.P + bn * chunkDoubles, cs, co, e, eg);
+            bc = bn;
+        }
+    } else {
+        // two buffers: chunk c + 2 goes into chunk c's buffer once every
+        // warp has finished its GEMM2 on chunk c
+        for (int c = 0; c + 1 < nchunks; c++) {
+            const int bn = bc ^ 1;
+            const bool okWait = wait_chunk(bn);
+            if (__syncthreads_or(!okWait))
+                return abandon();
+            double cs[4], co[4];
+            gemm1(L.P + bn * chunkDoubles, cs, co);
+            gemm2(L.P + bc * chunkDoubles);
+            weights(L.P + bn * chunkDoubles, cs, co, e, eg);
+            if (c + 2 < nchunks) {
+                __syncthreads();
+                load_chunk(c + 2, bc);
+            }
+            bc = bn;
+        }
     }
     gemm2(L.P + bc * chunkDoubles);   // the last chunk (waited for by the last iteration)
     if constexpr (MIX) {
@@ -1759,9 +1789,11 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     return true;
 }
 
-template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0>
-__global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_constant__ NewtonArgs a)
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX, int PAIR = 0, int NW = 8>
+__global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const __grid_constant__ NewtonArgs a)
 {
+    static_assert(NW == 8 || NTF > 0, "the 4-warp shape runs the fused contractions only");
+    constexpr int kThreads = NW * 32, kWarps = NW;
     extern __shared__ __align__(16) double sm[];
     __shared__ int ctl[4];   // [0] problem, [1] done, [2] exhausted
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1863,8 +1895,15 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
         const NewtonProblem &pb = a.prob[ctl[0]];
         if (ctl[0] != loadedProb) {
             // stage this order's Gaunt contraction table in shared memory
+            // (or read it from global memory through L1 where the launch
+            // shape leaves no room for it)
             loadedProb = ctl[0];
-            if (a.useGaunt) {
+            if (a.useGaunt && !a.stageEll) {
+                L.ellVal = const_cast<double *>(pb.ellVal);
+                L.ellIdx = const_cast<unsigned short *>(pb.ellIdx);
+                L.ellPair = const_cast<unsigned short *>(pb.ellPair);
+                L.ellOff = const_cast<int *>(pb.ellOff);
+            } else if (a.useGaunt) {
                 for (int i = tid; i < pb.ellRows * 32; i += kThreads) {
                     L.ellVal[i] = pb.ellVal[i];
                     L.ellIdx[i] = pb.ellIdx[i];
@@ -1886,7 +1925,7 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
         // ---- phase A: evaluation contractions over the quadrature
         if constexpr (NTF > 0) {
-            if (!phase_a_fused<NTF, PPN, NT, NBK, MIX, PAIR>(a, pb, L, tid, lane, warp, mbPhase))
+            if (!phase_a_fused<NTF, PPN, NT, NBK, MIX, PAIR, NW>(a, pb, L, tid, lane, warp, mbPhase))
                 return;   // a staged chunk never arrived (error recorded)
         } else {
         const int nb = pb.nb, ldP = pb.ldP, K2p = pb.K2p;
@@ -2046,19 +2085,19 @@ __global__ void __launch_bounds__(kThreads, 1) newton_kernel(const __grid_consta
 
 // One kernel instance: mode 0 launches it, 1 sets its shared-memory limit,
 // 2 writes its resident CTAs per SM to *occ.
-template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX = 0, int PAIR = 0>
+template <int TPW, int NTF, int PPN, int NT, int NBK, int MIX = 0, int PAIR = 0, int NW = 8>
 cudaError_t newton_run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
 {
-    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK, MIX, PAIR>;
+    auto *k = newton_kernel<TPW, NTF, PPN, NT, NBK, MIX, PAIR, NW>;
     if (mode == 1)
         return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smemBytes);
     if (mode == 2) {
         int b = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kThreads, a.smemBytes);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, NW * 32, a.smemBytes);
         *occ = b < 1 ? 1 : b;
         return e;
     }
-    k<<<grid, kThreads, a.smemBytes, stream>>>(a);
+    k<<<grid, NW * 32, a.smemBytes, stream>>>(a);
     return cudaGetLastError();
 }
 

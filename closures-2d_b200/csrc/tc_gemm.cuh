@@ -1,0 +1,217 @@
+// tc_gemm.cuh -- BF16 GEMM on the 5th-generation tensor cores (sm_100a) for
+// the learned warm start's network: C = A . B^T with A [M x K] and B [N x K]
+// both K-major (row-major with K contiguous), FP32 accumulation in tensor
+// memory, and a fused epilogue (bias, GELU, FP32 and/or BF16 stores).
+//
+// One CTA (4 warps) computes a 128 x BN tile:
+//   warp 0, one lane   TMA producer: cp.async.bulk.tensor 2-D loads of the
+//                      A and B k-blocks (128 B swizzle, 64 BF16 of K per
+//                      row) into a STAGES-deep ring, completion counted in
+//                      bytes on the stage's "full" mbarrier; no multicast;
+//   warp 1, one lane   MMA issuer: tcgen05.mma.cta_group::1.kind::f16,
+//                      M = 128, N = BN, K = 16 per instruction, accumulating
+//                      in BN columns of tensor memory; tcgen05.commit on the
+//                      stage's "empty" mbarrier hands the stage back to the
+//                      producer, a last commit signals the epilogue;
+//   all four warps     epilogue: warp w reads TMEM lanes 32w..32w+31 (rows of
+//                      the tile) with tcgen05.ld.32x32b, 16 columns at a time.
+// Every wait is bounded (2 s of %globaltimer); a wait that gives up records
+// an error in *err and the CTA still releases its tensor memory.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "closures_gpu.h"
+#include "common.cuh"
+
+namespace clb {
+namespace tc {
+
+constexpr int BM = 128;                 // tile rows = TMEM lanes
+constexpr int BK = 64;                  // BF16 of K per k-block: one 128 B swizzle row
+constexpr int kStages = 4;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+enum Epi { EPI_STORE = 0, EPI_BIAS = 1, EPI_BIAS_GELU = 2 };
+
+__device__ __forceinline__ float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+// Shared-memory matrix descriptor of a K-major tile in the 128 B swizzle
+// layout: rows of 128 B, 8-row groups 1024 B apart (stride byte offset),
+// leading byte offset unused (1), descriptor version 1, layout type 2.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (16 B units)
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+    d |= (uint64_t)1 << 46;                 // version
+    d |= (uint64_t)2 << 61;                 // 128 B swizzle
+    return d;
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 accumulator, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, unsigned long long *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int acc)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(unsigned long long *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Z (nullable) [M x N] FP32 = A B^T (+ bias); Act (nullable) [M x N] BF16 =
+// GELU(Z) (EPI_BIAS_GELU) or Z.  With Mdev, M = min(M, *Mdev - moff).
+template <int BN, int EPI>
+__global__ void __launch_bounds__(128, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int N,
+                   int K, float *Z, const float *bias, __nv_bfloat16 *Act, const int *Mdev, int moff, int *err)
+{
+    static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM columns: a power of two >= 32");
+    constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE = A_BYTES + B_BYTES;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long full[kStages], empty[kStages], accum;
+    __shared__ uint32_t tmemBase;
+    __shared__ int failed;
+    // stage tiles on 1024 B boundaries (the swizzle pattern's period)
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    if (Mdev) {
+        const int rem = *Mdev - moff;
+        M = rem < M ? (rem > 0 ? rem : 0) : M;
+    }
+    if (m0 >= M)
+        return;   // uniform over the CTA, before any allocation
+    const int nk = (K + BK - 1) / BK;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accum, 1);
+        mbar_init_fence();
+        failed = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmemBase)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmemBase;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % kStages;
+            if (kb >= kStages && !mbar_wait_bounded(&empty[s], ((kb / kStages) - 1) & 1, kWaitNs)) {
+                failed = 1;
+                break;
+            }
+            unsigned char *sa = smem + s * STAGE;
+            mbar_expect_tx(&full[s], STAGE);
+            tma_load_2d(sa, &mapA, kb * BK, m0, &full[s]);
+            tma_load_2d(sa + A_BYTES, &mapB, kb * BK, n0, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        constexpr uint32_t idesc = idesc_bf16(BN);
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % kStages;
+            if (!mbar_wait_bounded(&full[s], (kb / kStages) & 1, kWaitNs)) {
+                failed = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
+            const int ksteps = min(BK / 16, (K - kb * BK + 15) / 16);
+            for (int kk = 0; kk < ksteps; kk++)
+                umma_bf16(tmem, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32), idesc,
+                          (kb > 0 || kk > 0) ? 1 : 0);
+            umma_commit(&empty[s]);
+        }
+        umma_commit(&accum);
+    }
+    __syncwarp();
+    // epilogue: every warp waits for the accumulator
+    const bool ok = mbar_wait_bounded(&accum, 0, kWaitNs);
+    __syncthreads();   // the producer's and issuer's failure flag
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (ok && !failed) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            if (n0 + c0 >= N)
+                break;   // uniform over the warp
+            uint32_t r[16];
+            tmem_ld16(tl + c0, r);
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) {
+                        float v = __uint_as_float(r[j]);
+                        if (EPI != EPI_STORE)
+                            v += bias[col];
+                        if (Z)
+                            Z[(size_t)row * N + col] = v;
+                        if (Act)
+                            Act[(size_t)row * N + col] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v) : v);
+                    }
+                }
+            }
+        }
+    } else if (tid == 0 && err) {
+        atomicExch(err, CL_ERR_TIMEOUT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+// Dynamic shared memory of a BN instance: the stage ring and 1 KB for the
+// alignment of its start.
+constexpr int smem_bytes(int bn) { return kStages * (BM * BK * 2 + bn * BK * 2) + 1024; }
+
+}  // namespace tc
+}  // namespace clb

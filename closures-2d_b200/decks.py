@@ -99,3 +99,34 @@ def regression_deck(init_cond, moment_type, **kw):
 def write_deck(path, text):
     with open(path, "w") as f:
         f.write(text)
+
+
+def max_dt(kw):
+    """The time step a deck written by deck_text(**kw) runs at:
+    CFL * (2 / (2 + theta)) * dx dy / (dx + dy) (momopt_init.cpp:72)."""
+    nx, ny = kw.get("num_cells_x", 50), kw.get("num_cells_y", 50)
+    dx = (kw.get("b_x", 1.5) - kw.get("a_x", -1.5)) / nx
+    dy = (kw.get("b_y", 1.5) - kw.get("a_y", -1.5)) / ny
+    cfl, theta = kw.get("cfl_factor", 0.9), kw.get("theta", 2.0)
+    return cfl * (2.0 / (2.0 + theta)) * dx * dy / (dx + dy)
+
+
+# The benchmark workloads (deck_text keyword sets).
+WORKLOADS = {
+    # the M6 / PP6 800x800 pulse (configs of the headline)
+    "m6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
+                   gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
+                   moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
+                   moment_type="mn"),
+    "pp6_800": dict(num_cells_x=800, num_cells_y=800, a_x=-1.5, b_x=1.5, a_y=-1.5, b_y=1.5,
+                    gaussian_sigma=0.03, floor=1e-8, sigma=1.0, init_cond="gaussian",
+                    moment_order=6, quad_order=40, tol=1e-8, use_gaunt=1, t_final=1.0,
+                    moment_type="ppn"),
+    # M4 lattice, 200x200 on [-3.5,3.5]^2, Q=30
+    "m4_lattice_200": dict(num_cells_x=200, num_cells_y=200, a_x=-3.5, b_x=3.5, a_y=-3.5,
+                           b_y=3.5, init_cond="lattice", floor=1e-10, moment_order=4,
+                           quad_order=30, tol=1e-8, use_gaunt=1, t_final=3.2),
+    # M2 50x50 Gaussian, Q=20 (the reference's CPU-runnable case)
+    "m2_50": dict(num_cells_x=50, num_cells_y=50, gaussian_sigma=0.4, floor=1e-4,
+                  moment_order=2, quad_order=20, tol=1e-8, use_gaunt=0, t_final=0.5),
+}

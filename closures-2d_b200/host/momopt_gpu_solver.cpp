@@ -67,6 +67,10 @@ int MomOptGpuSolver::tryInit(double dx, double dy, double *maxDtOut)
         m_opt.precision = CL_MIXED;
     std::string contraction;
     m_opt.contraction = CL_CONTRACT_PAIRS;
+    int tune = 1;
+    if (!d.get("MOMOPT_GPU_TUNE", &tune))
+        tune = 1;
+    m_tune = tune != 0;
     if (d.get("MOMOPT_GPU_CONTRACTION", contraction) && contraction == "single")
         m_opt.contraction = CL_CONTRACT_SINGLE;
 
@@ -108,6 +112,10 @@ int MomOptGpuSolver::tryInit(double dx, double dy, double *maxDtOut)
         lastError = cl_global_error();
         return rc;
     }
+    // launch shapes chosen by the autotuner on the initial state (or taken
+    // from its cache); grids too small to time keep the defaults
+    if (m_tune)
+        return ctxError(cl_tune(m_ctx, 1, nullptr));
     return CL_OK;
 }
 

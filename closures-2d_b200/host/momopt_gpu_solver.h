@@ -34,6 +34,7 @@ private:
     double m_maxDt = 0;
     cl_ctx *m_ctx = nullptr;
     cl_options m_opt{};
+    bool m_tune = true;   // MOMOPT_GPU_TUNE (default 1): cl_tune once the state is on the device
 };
 
 }  // namespace clb

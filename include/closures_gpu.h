@@ -200,6 +200,46 @@ int cl_get_stats(cl_ctx *ctx, cl_stats *s);
 /* outs.iter of every cell (ghosts included) in the last optimisation stage. */
 int cl_get_last_iterations(cl_ctx *ctx, int *iters);
 
+/* Autotuner of the launch shapes -- no counterpart in the reference, whose
+ * per-cell loop is an OpenMP schedule(dynamic,1) over cells
+ * (momopt_update.cpp:208-277, :214).  Candidates, each run on copies of the
+ * context's current state (the real state is untouched):
+ *   K1 (Newton):  cells per CTA and warps -- 32 cells / 8 warps / one CTA
+ *                 per SM, or 16 cells / 4 warps / two CTAs per SM (the
+ *                 direction-pair layout) -- and the Hessian tile layout:
+ *                 direction pairs (even/odd degree column tiles) or one
+ *                 direction at a time, where both exist (Mn, FP64);
+ *   K2+K3 (flux): the same two tile layouts.
+ * Every candidate is launched once untimed, then timed three times with
+ * CUDA events on the context's stream; the median decides.  The choice is
+ * applied to the context and cached per (order, quadrature, Gaunt, closure,
+ * precision, optimisation type) in the process, and in the file named by
+ * the environment variable CL_TUNE_CACHE when set; with use_cache = 1 a
+ * cached choice is applied without timing.  Grids below 16384 cells, batch-only
+ * contexts and the change-of-basis types keep the default shape (nothing is
+ * timed; out->ncand = 0).  Every candidate computes the same per-cell sums:
+ * the two K1 launch shapes give bit-identical results, the two tile layouts
+ * the same sums in another order. */
+#define CL_TUNE_MAX 8
+typedef struct {
+    int newton_warps;         /* K1 warps per CTA: 8 (32 cells per CTA) or 4 (16) */
+    int newton_ctas;          /* K1 persistent CTAs per launch */
+    int newton_contraction;   /* K1 Hessian tile layout: CL_CONTRACT_PAIRS or _SINGLE */
+    int flux_contraction;     /* K2+K3 tile layout */
+    int from_cache;           /* 1: taken from the cache, nothing timed */
+    int ncand;                /* candidates timed */
+    int cand_kernel[CL_TUNE_MAX];        /* 1: K1, 2: K2+K3 */
+    int cand_warps[CL_TUNE_MAX];
+    int cand_contraction[CL_TUNE_MAX];
+    float cand_ms[CL_TUNE_MAX];          /* median launch time */
+} cl_tuning;
+int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out);   /* use_cache 0: always time */
+/* The shapes in use (after cl_tune, cl_set_launch_shape or the defaults). */
+int cl_get_tuning(cl_ctx *ctx, cl_tuning *out);
+/* Forces the shapes (CL_ERR_ARG where the configuration has no such
+ * instance): newton_warps 8 or 4, contractions CL_CONTRACT_PAIRS/_SINGLE. */
+int cl_set_launch_shape(cl_ctx *ctx, int newton_warps, int newton_contraction, int flux_contraction);
+
 /* Batched per-vector operator: the GPU equivalent of calling
  * opt(n, n2, nq, u, alpha, options, w, p, &outs) (opt.cpp:82-148) on `count`
  * vectors, in place on u and alpha (host arrays, [count*n] each, the order of
@@ -412,6 +452,17 @@ int cl_mlp_train(cl_mlp *m, const double *d_u, const double *d_alpha, int count,
  * stream null = the network's own stream. */
 int cl_mlp_predict(cl_mlp *m, const double *d_u, double *d_alpha, int count, int fallback_kind, int *fallbacks,
                    void *stream);
+/* Predictions only for the vectors whose last solve took at least min_iters
+ * iterations (d_iters [count], device); the others get a NaN start (the
+ * Newton kernel then starts them from their own multipliers).  The selection
+ * stays on the device (no host synchronisation). */
+int cl_mlp_predict_selected(cl_mlp *m, const double *d_u, const int *d_iters, int min_iters, double *d_alpha,
+                            int count, void *stream);
+/* The network's GEMM alone: C [M x N] FP32 = A [M x K] . B [N x K]^T with BF16
+ * A and B (device, row-major, K a multiple of 8), on the tensor-memory path
+ * (tcgen05.mma kind::f16 with TMA-staged operands) the forward pass uses.
+ * Waits for the result. */
+int cl_tc_gemm_bf16(const void *d_A, const void *d_B, int M, int N, int K, float *d_C);
 /* Loss and gradients of one host batch (gradient checks). */
 int cl_mlp_loss_and_grads(cl_mlp *m, const double *u, const double *alpha, int rows, float *loss,
                           float *const *gW, float *const *gb);
@@ -422,6 +473,11 @@ int cl_mlp_set_params(cl_mlp *m, float *const *W, float *const *b);
  * NULL to return to the reference's plain warm start.  The network must
  * outlive its use by the context. */
 int cl_set_warm_start(cl_ctx *ctx, cl_mlp *m);
+/* Same, predicting only for the cells whose previous optimisation stage took
+ * at least min_prev_iters iterations (the cells the previous-stage start
+ * served worst); every other cell keeps the reference's previous-stage
+ * start.  min_prev_iters 0 predicts every cell, as cl_set_warm_start. */
+int cl_set_warm_start_selective(cl_ctx *ctx, cl_mlp *m, int min_prev_iters);
 
 /* Kernel launches issued by the library since load (for the bench). */
 int64_t cl_launch_count(void);

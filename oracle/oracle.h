@@ -90,6 +90,10 @@ void orc_gauss_legendre(int n, double *x, double *w);
 /* Normalised associated Legendre with Condon-Shortley phase
  * (the quantity gsl_sf_legendre_sphPlm returns). */
 double orc_sphPlm(int l, int m, double x);
+/* Householder QR of a row-major rows x cols matrix in place, and the least
+ * squares solve with it (momopt_init.cpp:233-243 uses GSL's). */
+void orc_householder_qr(int rows, int cols, double *A, double *tau);
+void orc_householder_lssolve(int rows, int cols, const double *QR, const double *tau, double *b, double *beta);
 
 /* Per-cell operator: opt.cpp:82-148 (in-place on u, alpha). */
 int orc_opt(int n, int n2, int nq, double *u, double *alpha, orc_options opts,

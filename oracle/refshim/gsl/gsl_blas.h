@@ -1,0 +1,2 @@
+/* see gsl_shim.h */
+#include "gsl_shim.h"

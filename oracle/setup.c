@@ -94,7 +94,7 @@ double orc_sphPlm(int l, int m, double x)
 /* Householder QR of A (rows x cols, row-major, rows >= cols), in place:
  * R in the upper triangle, v_k below the diagonal with v_k[k]=1 implied,
  * tau[k] the reflector scale. */
-static void householder_qr(int rows, int cols, double *A, double *tau)
+void orc_householder_qr(int rows, int cols, double *A, double *tau)
 {
     for (int k = 0; k < cols; k++) {
         double norm = 0.0;
@@ -125,7 +125,7 @@ static void householder_qr(int rows, int cols, double *A, double *tau)
 }
 
 /* min ||A beta - b|| given the factorisation above; b is overwritten. */
-static void householder_lssolve(int rows, int cols, const double *QR, const double *tau,
+void orc_householder_lssolve(int rows, int cols, const double *QR, const double *tau,
                                 double *b, double *beta)
 {
     for (int k = 0; k < cols; k++) {
@@ -212,7 +212,7 @@ int orc_setup_create(int order, int Q, int useGaunt, orc_setup *s)
         double *b = (double *)malloc(sizeof(double) * nq);
         double *beta = (double *)malloc(sizeof(double) * n2);
         memcpy(A, s->p, sizeof(double) * nq * n2);
-        householder_qr(nq, n2, A, tau);
+        orc_householder_qr(nq, n2, A, tau);
         int cap = n * n * n2;
         s->gaunt.n = n;
         s->gaunt.off = (int *)malloc(sizeof(int) * (n * n + 1));
@@ -223,7 +223,7 @@ int orc_setup_create(int order, int Q, int useGaunt, orc_setup *s)
             for (int j = 0; j < n; j++) {
                 for (int q = 0; q < nq; q++)
                     b[q] = s->p[q * n2 + i] * s->p[q * n2 + j];
-                householder_lssolve(nq, n2, A, tau, b, beta);
+                orc_householder_lssolve(nq, n2, A, tau, b, beta);
                 s->gaunt.off[i * n + j] = nnz;
                 for (int k = 0; k < n2; k++) {
                     if (fabs(beta[k]) > 10e-10) {

@@ -74,3 +74,37 @@ def run_oracle(deck_text, workdir, max_steps=-1, threads=None):
     subprocess.run([exe, deck, workdir, str(max_steps)], check=True, env=env,
                    stdout=subprocess.DEVNULL)
     return workdir
+
+
+def per_cell_parity(m_g, m_o, m_f, tol=1e-10, factor=3.0, newton_tol=1e-8, max_flip_frac=0.01):
+    """Grid parity cell by cell, of m_g against the oracle m_o and the oracle
+    built with FMA contraction m_f ([NX][NY][n] each; moments scaled by the
+    oracle's |u_0| of the cell).  Each cell falls in one class:
+      exact     the two oracle builds agree to tol (rounding decides nothing
+                in the cell's history) and m_g agrees to tol;
+      envelope  the oracle builds differ (an Armijo, condition or stopping
+                decision taken on values equal to the last ulp, and the cells
+                its flux reached) and m_g is within factor x that spread + tol;
+      flip      neither, but within the stopping test's own resolution
+                2 newton_tol ||u/u0|| (opt.cpp:286-293): a third rounding
+                (another summation order, another LAPACK) ends one more or
+                one fewer Newton iteration where the oracle builds agree;
+      bad       anything else.
+    Passes when no cell is bad and at most max_flip_frac of the cells (and
+    at least 5 allowed) are flips.  Returns (passed, report)."""
+    scale = np.abs(m_o[:, :, :1])
+    err = np.max(np.abs(m_g - m_o) / scale, axis=2)
+    env = np.max(np.abs(m_f - m_o) / scale, axis=2)
+    unorm = np.linalg.norm(m_o / m_o[:, :, :1], axis=2)
+    stable = env <= tol
+    exact = stable & (err <= tol)
+    envelope = ~stable & (err <= factor * env + tol)
+    flip = ~exact & ~envelope & (err <= 2.0 * newton_tol * unorm)
+    bad = ~exact & ~envelope & ~flip
+    allowed = max(5, int(max_flip_frac * err.size))
+    report = {"cells": int(err.size), "exact": int(exact.sum()), "envelope": int(envelope.sum()),
+              "flip": int(flip.sum()), "bad": int(bad.sum()), "flip_allowed": allowed,
+              "max_err": float(err.max()), "max_env": float(env.max()),
+              "max_err_where_stable": float(err[stable].max()) if stable.any() else 0.0,
+              "bad_cells": np.argwhere(bad)[:10].tolist()}
+    return (not bad.any()) and int(flip.sum()) <= allowed, report

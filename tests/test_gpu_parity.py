@@ -260,15 +260,12 @@ def test_grid_steps_match_oracle(tmp_path, name, kw, steps):
     m_f, _ = fma.state()
     m_g, a_g = s.context_state()
     scale = np.abs(m_o[:, :, :1])
-    err = float(np.max(np.abs(m_g - m_o) / scale))
     env = float(np.max(np.abs(m_f - m_o) / scale))
-    if env < TOL:
-        assert err < TOL, "gpu %.3e (decisions are rounding-stable here)" % err
-    else:
-        # Rounding decides some regularisation steps on this deck (the two
-        # oracle builds already differ): a flipped first rung changes a cell's
-        # moments by r = 1e-3 relative, which is the scale of the envelope.
-        assert err <= max(3.0 * env, 2e-3), "gpu %.3e vs envelope %.3e" % (err, env)
+    # cell by cell: 1e-10 wherever the two oracle builds agree, their spread
+    # where rounding decided a regularisation or Armijo step (the flipped
+    # cell and the cells its flux reached), a few stopping-test flips
+    ok, rep = helpers.per_cell_parity(m_g, m_o, m_f)
+    assert ok, rep
     so, sg = orc.stats(), s.stats()
     assert sg["num_solves"] == so["num_solves"]
     if env < TOL:

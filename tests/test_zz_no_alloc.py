@@ -71,9 +71,9 @@ def test_noalloc_repeat_call_allocates_nothing():
     free memory unchanged: the entry point itself allocates nothing."""
     import torch
 
-    a = cb.Angular(3, 20, 1)
-    count = 400
-    u, _ = cb.sample_moment_vectors(a, count, seed=31, s_range=(0.1, 2.0))
+    a = cb.Angular(4, 30, 1)
+    count = 900
+    u, _ = cb.sample_moment_vectors(a, count, seed=21, s_range=(0.1, 2.0))
     opts = cb.make_options(tol=1e-8)
     dev = torch.device("cuda", 0)
     d_u0 = torch.from_numpy(u).to(dev)
