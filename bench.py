@@ -523,14 +523,15 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         if not args.no_tune:
             tuning["late"] = ctx.tune()
         late_state = ctx.get_state()
+        late_iters = ctx.last_iterations()
         late = window(args.steps, step * dt)
         full_ms += late["_device_ms"]
         step += args.steps
         if args.newton_compare and args.opt_type == 0 and args.precision == "fp64":
             plain_end = ctx.get_state()
             s_nn0 = solver.stats()
-            nn = nn_compare(args, cb, torch, ctx, w, n, harvest, late_state, plain_end, late, window,
-                            step * dt - args.steps * dt)
+            nn = nn_compare(args, cb, torch, ctx, w, n, harvest, (late_state, late_iters), plain_end, late,
+                            window, step * dt - args.steps * dt)
             ctx.set_warm_start(None)
             ctx.set_state(*plain_end)
             s_nn1 = solver.stats()
@@ -666,18 +667,38 @@ def nn_compare(args, cb, torch, ctx, w, n, harvest, late_state, plain_end, plain
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t1
     pairs = int(u.shape[0])
-    del u, al, us, als
+    # inference throughput of the network (its forward GEMMs on the tensor
+    # memory path): a prediction for every cell of the window's state
+    dm = torch.from_numpy(late_state[0][0].reshape(-1, n).copy()).to(dev)
+    dpred = torch.empty_like(dm)
+    net.predict(dm, dpred, dm.shape[0], fallback_kind=1)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        net.predict(dm, dpred, dm.shape[0], fallback_kind=1)
+    torch.cuda.synchronize()
+    pred_ms = 1e3 * (time.perf_counter() - t2) / reps
+    flops_cell = 2.0 * (n * width + 2 * width * width + width * n)
+    train_flops = 3.0 * flops_cell * 4096 * args.nn_steps
+    del u, al, us, als, dm, dpred
     scale = np.abs(plain_end[0][:, :, :1])
     out = {"network": "%d-%d-%d-%d-%d GELU, BF16 weights, FP32 accumulation" % (n, width, width, width, n),
            "pairs": pairs, "pairs_from": "the 2 RK2 steps before the late window, re-solved",
            "train_steps": args.nn_steps, "batch": 4096, "lr": 1e-3, "train_s": train_s, "harvest_s": harvest_s,
            "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
+           "train_tflops": train_flops / train_s / 1e12,
+           "predict_ms_all_cells": pred_ms,
+           "predict_tflops": flops_cell * late_state[0][0].reshape(-1, n).shape[0] / (pred_ms * 1e-3) / 1e12,
            "t_start": t_late,
            "plain": {k: plain_win[k] for k in ("value", "iter_mean", "trials_per_solve", "ms_per_step",
                                                "kernel_ms", "iter_hist_last_stage")},
            "modes": {}}
+    late_state, late_iters = late_state
     for mode, min_it in (("every_cell", 0), ("cells_prev_iters_ge_3", 3)):
+        # the window's starting point, per-cell iteration counts included
         ctx.set_state(*late_state)
+        ctx.set_last_iterations(late_iters)
         ctx.set_warm_start(net, min_prev_iters=min_it)
         win = window(args.steps, t_late)
         m_end, _ = ctx.get_state()

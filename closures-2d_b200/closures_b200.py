@@ -170,6 +170,7 @@ def lib():
             "cl_set_warm_start": (C.c_int, [vp, vp]),
             "cl_set_warm_start_selective": (C.c_int, [vp, vp, C.c_int]),
             "cl_tc_gemm_bf16": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp]),
+            "cl_set_last_iterations": (C.c_int, [vp, vp]),
             "cl_mlp_predict_selected": (C.c_int, [vp, vp, vp, C.c_int, vp, C.c_int, vp]),
             "cl_solve_batch_noalloc": (C.c_int, [C.POINTER(cl_angular), C.POINTER(cl_options),
                                                  C.c_int, vp, vp, vp, vp, vp, vp]),
@@ -368,6 +369,11 @@ class Context:
         it = np.empty(self.NX * self.NY, np.int32)
         _check(lib().cl_get_last_iterations(self._ctx, _ip(it)), self._err)
         return it.reshape(self.NX, self.NY)
+
+    def set_last_iterations(self, iters):
+        it = np.ascontiguousarray(iters, dtype=np.int32).reshape(-1)
+        assert it.size == self.NX * self.NY
+        _check(lib().cl_set_last_iterations(self._ctx, _ip(it)), self._err)
 
     def stats(self):
         s = cl_stats()

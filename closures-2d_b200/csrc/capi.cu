@@ -1634,6 +1634,15 @@ int cl_get_last_iterations(cl_ctx *ctx, int *iters)
     return CL_OK;
 }
 
+int cl_set_last_iterations(cl_ctx *ctx, const int *iters)
+{
+    if (!ctx || !iters)
+        return CL_ERR_ARG;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dIters, iters, (size_t)ctx->C * sizeof(int), cudaMemcpyHostToDevice));
+    return CL_OK;
+}
+
 int cl_device_state(cl_ctx *ctx, double **d_moments, double **d_alpha)
 {
     if (!ctx)

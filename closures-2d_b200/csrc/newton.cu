@@ -48,7 +48,7 @@ int plan_newton(NewtonArgs &a)
     a.offFpart = take(T * a.ntq);
     a.offStat = take(kStatU64 + 1);
     // the 4-warp shape reads the Gaunt table through L1 so that two CTAs fit
-    a.stageEll = (nw == kWarps) ? 1 : 0;
+    a.stageEll = (nw == kWarps) ? 1 : 0;   // matches the kernel's compile-time choice
     if (!a.stageEll)
         ellRows = ellChunks = 0;
     a.offEllVal = take(ellRows * 32);

@@ -1519,7 +1519,7 @@ __device__ __forceinline__ bool phase_a_fused(const NewtonArgs &a, const NewtonP
     const int NT2 = (NT > 0) ? NT : NTH + (PPN ? nb / 8 : 0);
     const int nchunks = pb.nqp / kq;
     const int chunkDoubles = kq * ldP + kq;   // rows of a chunk, gaps included (basis_row)
-    const int mt = warp % MT, qg = warp / MT;
+    const int mt = (int)((unsigned)warp % MT), qg = (int)((unsigned)warp / MT);
     const int r0 = mt * 16 + g, r1 = r0 + 8;
     const double dl0 = L.scal[r0 * SC_N + SC_DELTA], dl1 = L.scal[r1 * SC_N + SC_DELTA];
     const double *A0 = L.alpha + r0 * ldv + t4, *A1 = L.alpha + r1 * ldv + t4;
@@ -1898,11 +1898,15 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
             // (or read it from global memory through L1 where the launch
             // shape leaves no room for it)
             loadedProb = ctl[0];
-            if (a.useGaunt && !a.stageEll) {
-                L.ellVal = const_cast<double *>(pb.ellVal);
-                L.ellIdx = const_cast<unsigned short *>(pb.ellIdx);
-                L.ellPair = const_cast<unsigned short *>(pb.ellPair);
-                L.ellOff = const_cast<int *>(pb.ellOff);
+            // (a compile-time choice: the 8-warp shape's table pointers stay
+            // shared-memory pointers, which the loads in phase B rely on)
+            if constexpr (NW != 8) {
+                if (a.useGaunt) {
+                    L.ellVal = const_cast<double *>(pb.ellVal);
+                    L.ellIdx = const_cast<unsigned short *>(pb.ellIdx);
+                    L.ellPair = const_cast<unsigned short *>(pb.ellPair);
+                    L.ellOff = const_cast<int *>(pb.ellOff);
+                }
             } else if (a.useGaunt) {
                 for (int i = tid; i < pb.ellRows * 32; i += kThreads) {
                     L.ellVal[i] = pb.ellVal[i];

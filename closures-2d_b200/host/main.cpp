@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <string>
 
+#include "closures_gpu.h"
 #include "solver.h"
 
 int main(int argc, char **argv)
@@ -18,7 +19,8 @@ int main(int argc, char **argv)
     std::string err;
     int rc = clb::run_deck(deck, dir, maxSteps, err);
     if (rc != 0) {
-        std::printf("%s\n", err.c_str());
+        std::printf("%s\n", err.empty() ? cl_error_text(rc) : err.c_str());
+        std::fflush(stdout);   // abort() does not flush
         std::abort();
     }
     return 0;

@@ -199,6 +199,9 @@ int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, 
 int cl_get_stats(cl_ctx *ctx, cl_stats *s);
 /* outs.iter of every cell (ghosts included) in the last optimisation stage. */
 int cl_get_last_iterations(cl_ctx *ctx, int *iters);
+/* Sets those counts (host [NX*NY]), e.g. with a state put back by
+ * cl_set_state, for the selective learned start that reads them. */
+int cl_set_last_iterations(cl_ctx *ctx, const int *iters);
 
 /* Autotuner of the launch shapes -- no counterpart in the reference, whose
  * per-cell loop is an OpenMP schedule(dynamic,1) over cells

@@ -108,3 +108,41 @@ def per_cell_parity(m_g, m_o, m_f, tol=1e-10, factor=3.0, newton_tol=1e-8, max_f
               "max_err_where_stable": float(err[stable].max()) if stable.any() else 0.0,
               "bad_cells": np.argwhere(bad)[:10].tolist()}
     return (not bad.any()) and int(flip.sum()) <= allowed, report
+
+
+REF_OPT = os.path.join(REPO, "oracle", "_ref", "ref_opt")
+
+
+def ref_opt_batch(order, Q, use_gaunt, u, alpha, moment_type=0, tol=1e-8, max_iter=100, cond_h_max=1e10,
+                  delta_ppn=1e-10, threads=1):
+    """The reference's own opt() (oracle/_ref/ref_opt: opt.cpp, fobj.cpp,
+    linesearch.cpp and its set-up, compiled from the reference's sources) on
+    each row of u/alpha, in place.  Returns iters, regs, status (0, or -2 where
+    the regularisation ladder ran out).  Needs the reference build."""
+    import tempfile
+    import decks
+    n = u.shape[1]
+    with tempfile.TemporaryDirectory() as d:
+        decks.write_deck(os.path.join(d, "input.deck"),
+                         decks.deck_text(num_cells_x=2, num_cells_y=2, moment_order=order, quad_order=Q,
+                                         use_gaunt=use_gaunt, moment_type=moment_type, tol=tol,
+                                         max_iter=max_iter, cond_h_max=cond_h_max, delta_ppn=delta_ppn))
+        with open(os.path.join(d, "in.bin"), "wb") as f:
+            f.write(np.array([u.shape[0], n], np.int32).tobytes())
+            f.write(np.ascontiguousarray(u, np.float64).tobytes())
+            f.write(np.ascontiguousarray(alpha, np.float64).tobytes())
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
+        subprocess.run([REF_OPT, "in.bin", "out.bin"], cwd=d, env=env, check=True, stdout=subprocess.DEVNULL)
+        raw = open(os.path.join(d, "out.bin"), "rb").read()
+    count = u.shape[0]
+    off = 0
+    u[:] = np.frombuffer(raw, np.float64, count * n, off).reshape(count, n)
+    off += 8 * count * n
+    alpha[:] = np.frombuffer(raw, np.float64, count * n, off).reshape(count, n)
+    off += 8 * count * n
+    iters = np.frombuffer(raw, np.int32, count, off).copy()
+    off += 4 * count
+    regs = np.frombuffer(raw, np.float64, count, off).copy()
+    off += 8 * count
+    status = np.frombuffer(raw, np.int32, count, off).copy()
+    return iters, regs, status

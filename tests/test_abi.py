@@ -154,3 +154,20 @@ def test_noalloc_wrapper_checks_tensors():
         cb.solve_batch_noalloc(a, o, u64, u64, 4)
     with pytest.raises(ValueError, match="required"):
         cb.solve_batch_noalloc(a, o, None, u64, 4)
+
+
+BIN = os.path.join(helpers.PKG_DIR, "bin", "closures_gpu")
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_driver_binary_fails_cleanly_without_device(tmp_path):
+    """The drop-in executable (host/main.cpp, the reference's main.cpp loop)
+    stops with the library's message and abort(), as utils_abort() does, when
+    there is no device -- no CPU fallback."""
+    import subprocess
+    deck = tmp_path / "input.deck"
+    decks.write_deck(str(deck), decks.deck_text(num_cells_x=8, num_cells_y=8, moment_order=2, quad_order=8))
+    r = subprocess.run([BIN, str(deck), str(tmp_path)], capture_output=True, text=True, cwd=str(tmp_path))
+    assert r.returncode != 0
+    assert "device" in (r.stdout + r.stderr).lower()
+    assert not any(f.endswith(".pn") for f in os.listdir(str(tmp_path)))

@@ -73,3 +73,43 @@ def test_mixed_rejected_where_not_provided():
     a = cb.Angular(6, 40, 0)
     with pytest.raises(cb.ClosuresError):
         cb.Context.for_batches(a, cb.make_options(precision=cb.CL_MIXED))
+
+
+def test_mixed_cfg2_lattice_against_fp64_and_oracle(tmp_path):
+    """The M4 lattice at 200 x 200, Q = 30 (the mixed-precision configuration
+    of the north star) for three RK2 steps, cell by cell: mixed against the
+    FP64 GPU path and against the FP64 oracle, to the north star's 1e-6
+    relative for the mixed path.  The comparison with the oracle is made on
+    the cells whose result rounding does not decide (the two oracle builds and
+    the FP64 GPU path agree to 1e-10), which must be nearly all of them."""
+    import pyoracle
+    kw = dict(decks.WORKLOADS["m4_lattice_200"])
+    steps = 3
+    out = {}
+    for prec in ("fp64", "mixed"):
+        d = tmp_path / prec
+        d.mkdir()
+        extra = {"MOMOPT_GPU_PRECISION": "mixed"} if prec == "mixed" else None
+        deck = str(d / "input.deck")
+        decks.write_deck(deck, decks.deck_text(extra=extra, **kw))
+        s = cb.Solver(deck, str(d))
+        for _ in range(steps):
+            s.update(s.max_dt)
+        out[prec] = s.context_state()[0]
+        s.close()
+    ref = {}
+    for name, fma in (("oracle", False), ("fma", True)):
+        g = pyoracle.GridSolver(str(tmp_path / "fp64" / "input.deck"), fma=fma)
+        g.steps(steps)
+        ref[name] = g.state()[0]
+        g.close()
+    m64, m32, m_o, m_f = out["fp64"], out["mixed"], ref["oracle"], ref["fma"]
+    scale = np.abs(m_o[:, :, :1])
+    cell = lambda a, b: np.max(np.abs(a - b) / scale, axis=2)
+    e64, e32, env, e3264 = cell(m64, m_o), cell(m32, m_o), cell(m_f, m_o), cell(m32, m64)
+    stable = (env <= 1e-10) & (e64 <= 1e-10)
+    print("cells %d, decision-stable %d; mixed vs oracle there %.3e, mixed vs fp64 (all) %.3e"
+          % (stable.size, stable.sum(), e32[stable].max(), e3264.max()))
+    assert stable.mean() >= 0.95
+    assert e32[stable].max() <= 1e-6
+    assert (e3264 <= 1e-6).mean() >= 0.99

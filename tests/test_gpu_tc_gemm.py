@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("M,N,K", [(4096, 512, 512), (1000, 28, 512), (777, 512, 32), (130, 64, 200),
-                                   (262144, 256, 256), (5, 32, 8)])
+                                   (131072, 512, 512), (262144, 256, 256), (5, 32, 8)])
 def test_tc_gemm_matches_fp32_reference(M, N, K):
     import torch
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
