@@ -31,7 +31,8 @@ namespace tc {
 
 constexpr int BM = 128;                 // tile rows = TMEM lanes
 constexpr int BK = 64;                  // BF16 of K per k-block: one 128 B swizzle row
-constexpr int kStages = 4;
+constexpr int kStages = 3;               // 97 KB at BN = 128: two CTAs per SM, one's epilogue
+                                        // under the other's main loop
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 enum Epi { EPI_STORE = 0, EPI_BIAS = 1, EPI_BIAS_GELU = 2 };
@@ -96,7 +97,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 // Z (nullable) [M x N] FP32 = A B^T (+ bias); Act (nullable) [M x N] BF16 =
 // GELU(Z) (EPI_BIAS_GELU) or Z.  With Mdev, M = min(M, *Mdev - moff).
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int N,
                    int K, float *Z, const float *bias, __nv_bfloat16 *Act, const int *Mdev, int moff, int *err)
 {
@@ -185,17 +186,43 @@ __global__ void __launch_bounds__(128, 1)
             uint32_t r[16];
             tmem_ld16(tl + c0, r);
             if (row < M) {
+                const int col0 = n0 + c0;
+                float v[16];
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
-                    const int col = n0 + c0 + j;
-                    if (col < N) {
-                        float v = __uint_as_float(r[j]);
-                        if (EPI != EPI_STORE)
-                            v += bias[col];
-                        if (Z)
-                            Z[(size_t)row * N + col] = v;
-                        if (Act)
-                            Act[(size_t)row * N + col] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v) : v);
+                    v[j] = __uint_as_float(r[j]);
+                    if (EPI != EPI_STORE && col0 + j < N)
+                        v[j] += bias[col0 + j];
+                }
+                if (col0 + 16 <= N && (N & 7) == 0) {
+                    // whole 16-column chunk: 16-byte stores (rows start on
+                    // 16-byte boundaries when N is a multiple of 8)
+                    if (Z) {
+                        float4 *z = reinterpret_cast<float4 *>(Z + (size_t)row * N + col0);
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            z[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    }
+                    if (Act) {
+                        __align__(16) __nv_bfloat16 b[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            b[j] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
+                        uint4 *a = reinterpret_cast<uint4 *>(Act + (size_t)row * N + col0);
+                        a[0] = reinterpret_cast<const uint4 *>(b)[0];
+                        a[1] = reinterpret_cast<const uint4 *>(b)[1];
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const int col = col0 + j;
+                        if (col < N) {
+                            if (Z)
+                                Z[(size_t)row * N + col] = v[j];
+                            if (Act)
+                                Act[(size_t)row * N + col] =
+                                    __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
+                        }
                     }
                 }
             }
@@ -210,7 +237,7 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 // Dynamic shared memory of a BN instance: the stage ring and 1 KB for the
-// alignment of its start.
+// alignment of its start (97 KB at BN = 128).
 constexpr int smem_bytes(int bn) { return kStages * (BM * BK * 2 + bn * BK * 2) + 1024; }
 
 }  // namespace tc
