@@ -415,20 +415,36 @@ bool bf16_map(CUtensorMap *map, const __nv_bfloat16 *base, int rows, int cols, i
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+int sm_count_dev()
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms < 1)
+            sms = 1;
+    }
+    return sms;
+}
+
+// The persistent tensor-memory GEMM: one CTA per SM (or per tile, if fewer).
 template <int BN, int EPI>
 cudaError_t tc_gemm_bn(const CUtensorMap &ma, const CUtensorMap &mb, int M, int N, int K, float *Z, const float *bias,
                        __nv_bfloat16 *Act, const int *Mdev, int moff, int *err, cudaStream_t s)
 {
     static bool attr = false;
-    auto *k = clb::tc::tc_gemm_kernel<BN, EPI>;
+    auto *k = clb::tc::tc_gemm_persistent_kernel<BN, EPI>;
+    const int smem = clb::tc::smem_bytes_persistent(BN);
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, clb::tc::smem_bytes(BN));
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess)
             return e;
         attr = true;
     }
-    dim3 grid((N + BN - 1) / BN, (M + clb::tc::BM - 1) / clb::tc::BM);
-    k<<<grid, 128, clb::tc::smem_bytes(BN), s>>>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err);
+    const int tiles = ((N + BN - 1) / BN) * ((M + clb::tc::BM - 1) / clb::tc::BM);
+    const int grid = tiles < sm_count_dev() ? tiles : sm_count_dev();
+    k<<<grid, 192, smem, s>>>(ma, mb, M, N, K, Z, bias, Act, Mdev, moff, err);
     return cudaGetLastError();
 }
 

@@ -3,18 +3,21 @@
 // both K-major (row-major with K contiguous), FP32 accumulation in tensor
 // memory, and a fused epilogue (bias, GELU, FP32 and/or BF16 stores).
 //
-// One CTA (4 warps) computes a 128 x BN tile:
+// A persistent CTA per SM takes 128 x BN tiles in turn:
 //   warp 0, one lane   TMA producer: cp.async.bulk.tensor 2-D loads of the
 //                      A and B k-blocks (128 B swizzle, 64 BF16 of K per
-//                      row) into a STAGES-deep ring, completion counted in
+//                      row) into a four-stage ring, completion counted in
 //                      bytes on the stage's "full" mbarrier; no multicast;
 //   warp 1, one lane   MMA issuer: tcgen05.mma.cta_group::1.kind::f16,
-//                      M = 128, N = BN, K = 16 per instruction, accumulating
-//                      in BN columns of tensor memory; tcgen05.commit on the
-//                      stage's "empty" mbarrier hands the stage back to the
-//                      producer, a last commit signals the epilogue;
-//   all four warps     epilogue: warp w reads TMEM lanes 32w..32w+31 (rows of
-//                      the tile) with tcgen05.ld.32x32b, 16 columns at a time.
+//                      M = 128, N = BN, K = 16 per instruction, into one of
+//                      two BN-column accumulators in tensor memory;
+//                      tcgen05.commit on the stage's "empty" mbarrier hands
+//                      the stage back, a commit per tile hands the
+//                      accumulator to the epilogue;
+//   warps 2-5          epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
+//                      (rows of the tile) with tcgen05.ld.32x32b, 16 columns
+//                      at a time, and frees the accumulator, so one tile's
+//                      epilogue overlaps the next tile's MMAs.
 // Every wait is bounded (2 s of %globaltimer); a wait that gives up records
 // an error in *err and the CTA still releases its tensor memory.
 #pragma once
@@ -31,8 +34,6 @@ namespace tc {
 
 constexpr int BM = 128;                 // tile rows = TMEM lanes
 constexpr int BK = 64;                  // BF16 of K per k-block: one 128 B swizzle row
-constexpr int kStages = 3;               // 97 KB at BN = 128: two CTAs per SM, one's epilogue
-                                        // under the other's main loop
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 enum Epi { EPI_STORE = 0, EPI_BIAS = 1, EPI_BIAS_GELU = 2 };
@@ -95,42 +96,109 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 }
 
 // Z (nullable) [M x N] FP32 = A B^T (+ bias); Act (nullable) [M x N] BF16 =
-// GELU(Z) (EPI_BIAS_GELU) or Z.  With Mdev, M = min(M, *Mdev - moff).
+// GELU(Z) (EPI_BIAS_GELU) or Z; with Mdev, M = min(M, *Mdev - moff).
+// Persistent (one CTA per SM, tiles taken in turn), six warps:
+//   warp 0 (one lane)  TMA producer over the tiles' k-blocks, kPStages deep;
+//   warp 1 (one lane)  MMA issuer into one of two BN-column accumulators in
+//                      tensor memory, alternating per tile;
+//   warps 2-5          epilogue of the other accumulator: warp w reads TMEM
+//                      lanes 32 (w % 4) .. +31, then frees the buffer.
+// So a tile's epilogue runs while the next tile's MMAs accumulate.  Barriers:
+// full/empty per stage (TMA / MMA), tfull/tempty per accumulator (MMA /
+// epilogue), all waits bounded.
+constexpr int kPStages = 4;
+constexpr int smem_bytes_persistent(int bn) { return kPStages * (BM * BK * 2 + bn * BK * 2) + 1024; }
+
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 2)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int N,
-                   int K, float *Z, const float *bias, __nv_bfloat16 *Act, const int *Mdev, int moff, int *err)
+__device__ __forceinline__ void epilogue_rows(uint32_t tl, int row, int M, int N, int n0, float *Z,
+                                              const float *bias, __nv_bfloat16 *Act)
 {
-    static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM columns: a power of two >= 32");
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        if (n0 + c0 >= N)
+            break;   // uniform over the warp
+        uint32_t r[16];
+        tmem_ld16(tl + c0, r);
+        if (row >= M)
+            continue;
+        const int col0 = n0 + c0;
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            v[j] = __uint_as_float(r[j]);
+            if (EPI != EPI_STORE && col0 + j < N)
+                v[j] += bias[col0 + j];
+        }
+        if (col0 + 16 <= N && (N & 7) == 0) {
+            if (Z) {
+                float4 *z = reinterpret_cast<float4 *>(Z + (size_t)row * N + col0);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    z[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+            if (Act) {
+                __align__(16) __nv_bfloat16 b[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    b[j] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
+                uint4 *a = reinterpret_cast<uint4 *>(Act + (size_t)row * N + col0);
+                a[0] = reinterpret_cast<const uint4 *>(b)[0];
+                a[1] = reinterpret_cast<const uint4 *>(b)[1];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const int col = col0 + j;
+                if (col < N) {
+                    if (Z)
+                        Z[(size_t)row * N + col] = v[j];
+                    if (Act)
+                        Act[(size_t)row * N + col] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
+                }
+            }
+        }
+    }
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(192, 1)
+    tc_gemm_persistent_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                              int M, int N, int K, float *Z, const float *bias, __nv_bfloat16 *Act, const int *Mdev,
+                              int moff, int *err)
+{
+    static_assert(BN == 32 || BN == 64 || BN == 128, "two accumulators of BN columns (power of two)");
     constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE = A_BYTES + B_BYTES;
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) unsigned long long full[kStages], empty[kStages], accum;
+    __shared__ __align__(8) unsigned long long full[kPStages], empty[kPStages], tfull[2], tempty[2];
     __shared__ uint32_t tmemBase;
     __shared__ int failed;
-    // stage tiles on 1024 B boundaries (the swizzle pattern's period)
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (Mdev) {
         const int rem = *Mdev - moff;
         M = rem < M ? (rem > 0 ? rem : 0) : M;
     }
-    if (m0 >= M)
+    const int tilesN = (N + BN - 1) / BN, tilesM = (M + BM - 1) / BM;
+    const int ntiles = tilesM * tilesN;
+    if ((int)blockIdx.x >= ntiles)
         return;   // uniform over the CTA, before any allocation
     const int nk = (K + BK - 1) / BK;
 
     if (tid == 0) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < kPStages; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&accum, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);   // one arrival per epilogue warp
+        }
         mbar_init_fence();
         failed = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmemBase)),
-                     "r"(BN)
+                     "r"(2 * BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
@@ -139,106 +207,85 @@ __global__ void __launch_bounds__(128, 2)
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmemBase;
 
-    if (warp == 0 && lane == 0) {
-        // producer
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % kStages;
-            if (kb >= kStages && !mbar_wait_bounded(&empty[s], ((kb / kStages) - 1) & 1, kWaitNs)) {
-                failed = 1;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            int kbAll = 0;   // k-blocks issued so far (ring position)
+            for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+                const int m0 = (t / tilesN) * BM, n0 = (t % tilesN) * BN;
+                for (int kb = 0; kb < nk; kb++, kbAll++) {
+                    const int s = kbAll % kPStages;
+                    if (kbAll >= kPStages &&
+                        !mbar_wait_bounded(&empty[s], ((kbAll / kPStages) - 1) & 1, kWaitNs)) {
+                        failed = 1;
+                        break;
+                    }
+                    unsigned char *sa = smem + s * STAGE;
+                    mbar_expect_tx(&full[s], STAGE);
+                    tma_load_2d(sa, &mapA, kb * BK, m0, &full[s]);
+                    tma_load_2d(sa + A_BYTES, &mapB, kb * BK, n0, &full[s]);
+                }
             }
-            unsigned char *sa = smem + s * STAGE;
-            mbar_expect_tx(&full[s], STAGE);
-            tma_load_2d(sa, &mapA, kb * BK, m0, &full[s]);
-            tma_load_2d(sa + A_BYTES, &mapB, kb * BK, n0, &full[s]);
         }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        constexpr uint32_t idesc = idesc_bf16(BN);
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % kStages;
-            if (!mbar_wait_bounded(&full[s], (kb / kStages) & 1, kWaitNs)) {
-                failed = 1;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(BN);
+            int kbAll = 0, it = 0;
+            for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x, it++) {
+                const int b = it & 1;
+                // the epilogue has freed this accumulator (its previous use)
+                if (it >= 2 && !mbar_wait_bounded(&tempty[b], ((it >> 1) - 1) & 1, kWaitNs)) {
+                    failed = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                for (int kb = 0; kb < nk; kb++, kbAll++) {
+                    const int s = kbAll % kPStages;
+                    if (!mbar_wait_bounded(&full[s], (kbAll / kPStages) & 1, kWaitNs)) {
+                        failed = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
+                    const int ksteps = min(BK / 16, (K - kb * BK + 15) / 16);
+                    for (int kk = 0; kk < ksteps; kk++)
+                        umma_bf16(acc, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32), idesc,
+                                  (kb > 0 || kk > 0) ? 1 : 0);
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&tfull[b]);
+                if (failed)
+                    break;
+            }
+        }
+    } else {
+        // epilogue warps 2..5: TMEM lane quarter w % 4
+        const int quarter = warp & 3;
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+            const int b = it & 1;
+            if (!mbar_wait_bounded(&tfull[b], (it >> 1) & 1, kWaitNs)) {
+                if (lane == 0)
+                    failed = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
-            const int ksteps = min(BK / 16, (K - kb * BK + 15) / 16);
-            for (int kk = 0; kk < ksteps; kk++)
-                umma_bf16(tmem, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32), idesc,
-                          (kb > 0 || kk > 0) ? 1 : 0);
-            umma_commit(&empty[s]);
+            const int m0 = (t / tilesN) * BM, n0 = (t % tilesN) * BN;
+            const uint32_t tl = tmem + (uint32_t)(b * BN) + ((uint32_t)(quarter * 32) << 16);
+            epilogue_rows<BN, EPI>(tl, m0 + quarter * 32 + lane, M, N, n0, Z, bias, Act);
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&tempty[b])) : "memory");
         }
-        umma_commit(&accum);
     }
-    __syncwarp();
-    // epilogue: every warp waits for the accumulator
-    const bool ok = mbar_wait_bounded(&accum, 0, kWaitNs);
-    __syncthreads();   // the producer's and issuer's failure flag
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (ok && !failed) {
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            if (n0 + c0 >= N)
-                break;   // uniform over the warp
-            uint32_t r[16];
-            tmem_ld16(tl + c0, r);
-            if (row < M) {
-                const int col0 = n0 + c0;
-                float v[16];
-#pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    v[j] = __uint_as_float(r[j]);
-                    if (EPI != EPI_STORE && col0 + j < N)
-                        v[j] += bias[col0 + j];
-                }
-                if (col0 + 16 <= N && (N & 7) == 0) {
-                    // whole 16-column chunk: 16-byte stores (rows start on
-                    // 16-byte boundaries when N is a multiple of 8)
-                    if (Z) {
-                        float4 *z = reinterpret_cast<float4 *>(Z + (size_t)row * N + col0);
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            z[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                    }
-                    if (Act) {
-                        __align__(16) __nv_bfloat16 b[16];
-#pragma unroll
-                        for (int j = 0; j < 16; j++)
-                            b[j] = __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
-                        uint4 *a = reinterpret_cast<uint4 *>(Act + (size_t)row * N + col0);
-                        a[0] = reinterpret_cast<const uint4 *>(b)[0];
-                        a[1] = reinterpret_cast<const uint4 *>(b)[1];
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        const int col = col0 + j;
-                        if (col < N) {
-                            if (Z)
-                                Z[(size_t)row * N + col] = v[j];
-                            if (Act)
-                                Act[(size_t)row * N + col] =
-                                    __float2bfloat16(EPI == EPI_BIAS_GELU ? gelu_f(v[j]) : v[j]);
-                        }
-                    }
-                }
-            }
-        }
-    } else if (tid == 0 && err) {
-        atomicExch(err, CL_ERR_TIMEOUT);
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
+    if (failed && tid == 0 && err)
+        atomicExch(err, CL_ERR_TIMEOUT);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * BN) : "memory");
 }
-
-// Dynamic shared memory of a BN instance: the stage ring and 1 KB for the
-// alignment of its start (97 KB at BN = 128).
-constexpr int smem_bytes(int bn) { return kStages * (BM * BK * 2 + bn * BK * 2) + 1024; }
 
 }  // namespace tc
 }  // namespace clb
