@@ -221,14 +221,15 @@ def run_oracle_cb_sample(deck, w, opt_type, budget_s):
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "closures_ref")
 
 
-def run_reference_build(w, side, steps, threads, moment=False):
+def run_reference_build(w, side, steps, threads, moment=False, skip=0):
     """The reference's own program (oracle/_ref/closures_ref: its main.cpp,
     solvers and OpenMP loops, compiled from its sources) on a centred
     side x side sub-grid of the workload's deck -- the same cell size, time
     step, closure and initial pulse -- timed as the difference of two runs
-    that stop at T_FINAL = 0.5 dt and (steps + 0.5) dt, so that start-up,
-    set-up and output cancel.  Returns (seconds for `steps` RK2 steps,
-    cells with ghosts)."""
+    that stop at T_FINAL = (skip + 0.5) dt and (skip + steps + 0.5) dt, so
+    that start-up, set-up, the `skip` steps before the window and output
+    cancel.  Returns (seconds for RK2 steps skip+1 .. skip+steps, cells with
+    ghosts)."""
     nx = w["num_cells_x"]
     dx = (w.get("b_x", 1.5) - w.get("a_x", -1.5)) / nx
     cx = 0.5 * (w.get("b_x", 1.5) + w.get("a_x", -1.5))
@@ -243,7 +244,7 @@ def run_reference_build(w, side, steps, threads, moment=False):
         dt = decks.max_dt(sub)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
     secs = []
-    for k in (0.5, steps + 0.5):
+    for k in (skip + 0.5, skip + steps + 0.5):
         with tempfile.TemporaryDirectory() as d:
             kw = dict(sub, t_final=k * dt)
             text = decks.moment_deck_text(**kw) if moment else decks.deck_text(**kw)
@@ -297,9 +298,11 @@ def reference_build_arm(args, world, w):
     threads_all = cpu_threads()
     side = REF_SAMPLE_SIDE.get(args.workload, 64)
     steps = 1
+    # the native arm's headline window: --t-start, then W warm-up steps
+    skip = (int(round(args.t_start / decks.max_dt(w))) if args.t_start > 0 else 0) + args.warmup
     tried = {}
     for th in sorted({1, threads_all}):
-        secs_th, C = run_reference_build(w, side, steps, th)
+        secs_th, C = run_reference_build(w, side, steps, th, skip=skip)
         tried[th] = secs_th
     # the faster of one thread and all threads: the reference's per-cell
     # dynamic schedule can make all threads slower than one
@@ -308,19 +311,20 @@ def reference_build_arm(args, world, w):
     value = 2 * C * steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-solves/s",
-        "n_gpus": world, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * secs / steps,
+        "n_gpus": world, "steps": steps, "warmup": skip, "ms_per_step": 1e3 * secs / steps,
         "steps_per_s": steps / secs, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [w["num_cells_x"], w["num_cells_y"]],
                    "moment_order": w["moment_order"], "quad_order": w["quad_order"],
-                   "use_gaunt": w["use_gaunt"], "tol": w["tol"], "t_start": 0.0,
+                   "use_gaunt": w["use_gaunt"], "tol": w["tol"], "t_start": skip * decks.max_dt(w),
                    "sample_grid": [side, side]},
         "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads, "kind": "reference",
                          "sample": "the reference's own program (its sources compiled -O3 -fopenmp "
                                    "-DUSE_OPENMP with a GSL shim and OpenBLAS) on the centred %dx%d "
                                    "sub-grid of the deck (same cell size, time step and pulse), "
-                                   "RK2 step 1 from t=0, %d OpenMP thread(s): the faster of 1 and all %d"
-                                   % (side, side, threads, threads_all),
+                                   "RK2 step %d (the native arm's headline window starts there), %d OpenMP "
+                                   "thread(s): the faster of 1 and all %d"
+                                   % (side, side, skip + 1, threads, threads_all),
                          "by_threads": {str(k): 2 * C * steps / v for k, v in tried.items()}},
         "e2e": {"value": value, "unit": "cell-solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},

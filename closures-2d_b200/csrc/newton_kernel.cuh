@@ -1795,7 +1795,7 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
     static_assert(NW == 8 || NTF > 0, "the 4-warp shape runs the fused contractions only");
     constexpr int kThreads = NW * 32, kWarps = NW;
     extern __shared__ __align__(16) double sm[];
-    __shared__ int ctl[4];   // [0] problem, [1] done, [2] exhausted
+    __shared__ int ctl[4];   // [0] problem, [1] done, [2] exhausted, [3] next slot of phase B
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
     const int T = a.T, MT = a.T / 16, kq = a.kq, ldv = a.ldv, ldE = a.ldE, ldG = a.ldG;
@@ -1888,6 +1888,7 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
             ctl[0] = p;
             ctl[2] = exhausted ? 1 : 0;
             ctl[1] = (nActive == 0) ? 1 : 0;
+            ctl[3] = 0;
         }
         __syncthreads();
         if (ctl[1])
@@ -2062,8 +2063,18 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
         __syncthreads();
         }
 
-        // ---- phase B: per-slot Newton logic, one warp per slot
-        for (int s = warp; s < T; s += kWarps) {
+        // ---- phase B: per-slot Newton logic, one warp per slot.  Warps take
+        // the slots from a shared counter, so a warp that drew a cell needing
+        // the full Newton step (factorisation, inverse, condition estimate)
+        // does not also hold back cells that converged at this evaluation;
+        // a slot's logic touches only its own state and its helpers'.
+        for (;;) {
+            int s = 0;
+            if (lane == 0)
+                s = atomicAdd(&ctl[3], 1);
+            s = __shfl_sync(0xffffffffu, s, 0);
+            if (s >= T)
+                break;
             int st = L.ints[s * SI_N + SI_STATE];
             if (st == S_NEWTON || st == S_TRIAL) {
                 if (a.optType != 0)
