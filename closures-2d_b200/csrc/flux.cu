@@ -151,15 +151,11 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
     const int NTf = nb / 8;
     const int ntiles1 = kAnsatzTiles * (kq / 8);
 
-    load_chunk(0, 0);
-    for (int c = 0; c < nchunks; c++) {
-        const int buf = c & 1;
-        cp_async_wait<0>();
-        __syncthreads();   // chunk c visible; every warp is done with chunk c - 1
-        if (c + 1 < nchunks)
-            load_chunk(c + 1, buf ^ 1);   // into the buffer chunk c - 1 used
-        const double *Pb = sP + buf * kq * ldPf;
-        const double *Qb = sQ + buf * 4 * kq;
+    // Per chunk: the stencil, then in one barrier interval the projection of
+    // this chunk and the ansatz of the next (they use disjoint buffers), so a
+    // chunk takes two CTA barriers and the projection's MMAs interleave with
+    // the next ansatz's exponentials across warps.
+    auto ansatz = [&](const double *Pb) {
         // 1. ansatz on the halo tile
         if (PAIR) {
             const int nbe = f.nbe;
@@ -210,7 +206,8 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 sA[q * ldA + cell] = v[h];
             }
         }
-        __syncthreads();
+    };
+    auto stencil = [&](const double *Qb) {
         // 2. limited upwind stencil.  Thread (q = warp, column j = lane % 16)
         //    sweeps interior rows ib..ib+7 (ib = 8 * (lane / 16)) down its
         //    column: each slopefit of a cell is formed once and serves the
@@ -285,7 +282,8 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 out[r * TY] = fx[r] + fy * cyd;
             }
         }
-        __syncthreads();
+    };
+    auto projection = [&](const double *Pb) {
         // 3. projection on the basis: flux[ic][k] += F[ic][q] p[q][k]
         if (PAIR) {
             // k = the chunk's 8 pairs; rows t4, t4 + 4 of sF and their
@@ -319,6 +317,23 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
                 }
             }
         }
+    };
+    load_chunk(0, 0);
+    cp_async_wait<0>();
+    __syncthreads();
+    ansatz(sP);   // chunk 0, buffer 0
+    __syncthreads();
+    for (int c = 0; c < nchunks; c++) {
+        const int buf = c & 1;
+        if (c + 1 < nchunks)
+            load_chunk(c + 1, buf ^ 1);   // the buffer of chunk c - 1, free since the last barrier
+        stencil(sQ + buf * 4 * kq);
+        cp_async_wait<0>();
+        __syncthreads();   // the stencil flux of chunk c complete; chunk c + 1 staged
+        projection(sP + buf * kq * ldPf);
+        if (c + 1 < nchunks)
+            ansatz(sP + (buf ^ 1) * kq * ldPf);
+        __syncthreads();   // the ansatz of chunk c + 1 complete; chunk c's buffers free
     }
 
     // epilogue: Euler + collision + source (+ Heun average)
