@@ -125,6 +125,7 @@ def lib():
             "cl_tune": (C.c_int, [vp, C.c_int, C.POINTER(cl_tuning)]),
             "cl_get_tuning": (C.c_int, [vp, C.POINTER(cl_tuning)]),
             "cl_set_launch_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+            "cl_set_range_test": (C.c_int, [vp, C.c_int]),
             "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
@@ -441,6 +442,11 @@ class Context:
     def set_launch_shape(self, newton_warps=8, newton_contraction=0, flux_contraction=0):
         _check(lib().cl_set_launch_shape(self._ctx, newton_warps, newton_contraction, flux_contraction),
                self._err)
+
+    def set_range_test(self, enable=True):
+        """K1's exponent-range convergence test on or off (cl_set_range_test);
+        results are the same either way."""
+        _check(lib().cl_set_range_test(self._ctx, 1 if enable else 0), self._err)
 
     def stream(self):
         """The context's CUDA stream as a torch.cuda.ExternalStream (for

@@ -67,6 +67,14 @@ struct DeviceBasis {
     double *ellVal = nullptr;
     int *ellOff = nullptr;
     int ellChunks = 0, ellRows = 0;
+    // row 0 of the Gaunt contraction (CSR rows (0, j), layout columns) and
+    // the eigenvalue bounds of the quadrature Gram matrix of the moment basis
+    int *r0off = nullptr;
+    unsigned short *r0idx = nullptr;
+    double *r0val = nullptr;
+    double *rangeC = nullptr;   // max_q |p_k(q)|, then max_q of each degree's norm
+    double gramLo = 0, gramHi = 0;
+    int maxDeg = 0;
 
     void release()
     {
@@ -88,6 +96,10 @@ struct DeviceBasis {
         cudaFree(binv);
         cudaFree(pcol);
         cudaFree(fbinv);
+        cudaFree(r0off);
+        cudaFree(r0idx);
+        cudaFree(r0val);
+        cudaFree(rangeC);
         *this = DeviceBasis();
     }
 };
@@ -226,7 +238,52 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         }
     }
     std::vector<unsigned short> &pairs = prod;
+    // Gram matrix M = sum_q w_q p(q) p(q)^T of the moment basis: Gershgorin
+    // bounds of its eigenvalues, widened by 1e-12 of the largest diagonal
+    // entry for the rounding of the sums (gramLo = 0 when not positive)
+    {
+        std::vector<double> M((size_t)n * n, 0.0);
+        for (int q = 0; q < nq; q++) {
+            const double *pq = p + (size_t)q * n2;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++)
+                    M[(size_t)i * n + j] += w[q] * pq[i] * pq[j];
+        }
+        double lo = 0.0, hi = 0.0, dmax = 0.0;
+        for (int i = 0; i < n; i++) {
+            double r = 0.0;
+            for (int j = 0; j < n; j++)
+                if (j != i)
+                    r += std::fabs(M[(size_t)i * n + j]);
+            const double d = M[(size_t)i * n + i];
+            lo = (i == 0) ? d - r : std::min(lo, d - r);
+            hi = std::max(hi, d + r);
+            dmax = std::max(dmax, std::fabs(d));
+        }
+        lo -= 1e-12 * dmax;
+        hi += 1e-12 * dmax;
+        B.gramLo = lo > 0.0 ? lo : 0.0;
+        B.gramHi = hi;
+    }
+    // bounds of |alpha . p(q) - alpha_0 p_0| from the coefficients: the
+    // largest |p_k(q)| and the largest norm of each degree's values over q,
+    // rounded up by 1e-12
+    B.maxDeg = degB[n - 1];
+    std::vector<double> rangeC(n + B.maxDeg + 1, 0.0);
+    for (int q = 0; q < nq; q++) {
+        const double *pq = p + (size_t)q * n2;
+        std::vector<double> sq(B.maxDeg + 1, 0.0);
+        for (int k = 0; k < n; k++) {
+            rangeC[k] = std::max(rangeC[k], std::fabs(pq[k]));
+            sq[degB[k]] += pq[k] * pq[k];
+        }
+        for (int l = 0; l <= B.maxDeg; l++)
+            rangeC[n + l] = std::max(rangeC[n + l], std::sqrt(sq[l]));
+    }
+    for (auto &x : rangeC)
+        x *= 1.0 + 1e-12;
     cudaError_t e;
+    if ((e = upload(&B.rangeC, rangeC)) != cudaSuccess) return e;
     if ((e = upload(&B.P, P)) != cudaSuccess) return e;
     if ((e = upload(&B.w, W)) != cudaSuccess) return e;
     if ((e = upload(&B.Pf, Pf)) != cudaSuccess) return e;
@@ -271,6 +328,19 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
             x = (unsigned short)colH[x];
         B.ellChunks = chunks;
         B.ellRows = rows2;
+        // pairs (0, j) are the Gaunt table's rows j = 0 .. n-1 (row i n + j, i <= j)
+        std::vector<int> r0off(n + 1);
+        std::vector<unsigned short> r0idx;
+        std::vector<double> r0val;
+        for (int j = 0; j <= n; j++)
+            r0off[j] = goff[j] - goff[0];
+        for (int k = goff[0]; k < goff[n]; k++) {
+            r0idx.push_back((unsigned short)colH[gidx[k]]);
+            r0val.push_back(gval[k]);
+        }
+        if ((e = upload(&B.r0off, r0off)) != cudaSuccess) return e;
+        if ((e = upload(&B.r0idx, r0idx)) != cudaSuccess) return e;
+        if ((e = upload(&B.r0val, r0val)) != cudaSuccess) return e;
         if ((e = upload(&B.ellPair, epair)) != cudaSuccess) return e;
         if ((e = upload(&B.ellIdx, eidx)) != cudaSuccess) return e;
         if ((e = upload(&B.ellVal, eval)) != cudaSuccess) return e;
@@ -318,6 +388,13 @@ NewtonProblem make_problem(const DeviceBasis &B)
     pb.ellChunks = B.ellChunks;
     pb.ellRows = B.ellRows;
     pb.p0 = B.p0;
+    pb.row0Off = B.r0off;
+    pb.row0Idx = B.r0idx;
+    pb.row0Val = B.r0val;
+    pb.rangeC = B.rangeC;
+    pb.maxDeg = B.maxDeg;
+    pb.gramLo = (B.useGaunt && !B.r0off) ? 0.0 : B.gramLo;
+    pb.gramHi = B.gramHi;
     pb.n = B.n;
     pb.nb = B.nb;
     pb.K2p = B.K2p;
@@ -431,6 +508,7 @@ struct cl_ctx {
     // host angular data it is built from; which basis each kernel reads
     DeviceBasis B2;
     int newtonB2 = 0, fluxB2 = 0;
+    int rangeTest = 1;   // K1's exponent-range test (cl_set_range_test)
     int angN = 0, angN2 = 0, angNq = 0, angGaunt = 0, angNnz = 0;
     std::vector<double> aw, axi, aeta, ap, agval;
     std::vector<int> agoff, agidx;
@@ -1266,6 +1344,8 @@ static bool newton_shape(const cl_ctx *ctx, const DeviceBasis &B, int nw, Newton
     a.prob[0] = make_problem(B);
     a.prob[0].P2M = keep.P2M;
     a.prob[0].alphaP = keep.alphaP;
+    if (!ctx->rangeTest)
+        a.prob[0].gramLo = 0.0;
     a.nw = nw;
     if (plan_newton(a) != 0 || a.ntf == 0 || (B.paired && a.ntExact == 0))
         return false;
@@ -1477,6 +1557,17 @@ int cl_get_tuning(cl_ctx *ctx, cl_tuning *out)
     if (!ctx || !out)
         return CL_ERR_ARG;
     *out = ctx->tuning;
+    return CL_OK;
+}
+
+int cl_set_range_test(cl_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->rangeTest = enable ? 1 : 0;
+    ctx->nargs.prob[0].gramLo = enable ? make_problem(ctx->newtonB2 ? ctx->B2 : ctx->B).gramLo : 0.0;
+    invalidate_graph(ctx);
     return CL_OK;
 }
 

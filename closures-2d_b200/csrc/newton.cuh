@@ -37,6 +37,18 @@ struct NewtonProblem {
     const int *ellOff;
     int ellChunks, ellRows;
     double p0;                  // p[0] = Y_00 (fobj.cpp:305 divides by it)
+    // Converged-evaluation test without the Hessian (Mn, FP64): row 0 of the
+    // Gaunt contraction (CSR rows (0, j), j < n, G columns in the layout's
+    // order; null without Gaunt), bounds gramLo <= lambda <= gramHi of the
+    // quadrature Gram matrix sum_q w_q p(q) p(q)^T of the moment basis
+    // (gramLo = 0: the test is off), rangeC[k] = max_q |p_k(q)| (k < n) and
+    // rangeC[n + l] = max_q ||(p_k(q))_{deg k = l}|| (l <= maxDeg)
+    const int *row0Off;
+    const unsigned short *row0Idx;
+    const double *row0Val;
+    const double *rangeC;
+    double gramLo, gramHi;
+    int maxDeg;
     int n, nb, K2p, nqp, ldP;
     // direction pairs: the basis stores one direction of each (phi, phi + pi)
     // pair with its columns grouped by degree parity (nbe even basis columns,

@@ -545,9 +545,52 @@ __device__ __forceinline__ void release_helpers(Layout &L, int T, int s, int lan
     __syncwarp();
 }
 
-// Newton logic for one slot after its evaluation (warp-wide).
+// Sufficient condition, at a Mn evaluation, for the reference's condition
+// test (opt.cpp:244-261: dpotrf succeeds and anorm / rcond from dpocon is at
+// most MOMOPT_COND_H_MAX) to pass.  With the exponents s_q = alpha . p(q) in
+// [lo, hi] over the quadrature, x^T H x = sum_q w_q e^{s_q} (p(q) . x)^2 lies
+// between e^lo and e^hi times x^T M x, M = sum_q w_q p(q) p(q)^T with
+// gramLo <= lambda(M) <= gramHi, so cond_2(H) <= e^(hi - lo) gramHi / gramLo,
+// and the 1-norm condition number whose estimate (a lower bound) dpocon
+// returns is at most n cond_2(H).  p_0 is constant, so
+// |s_q - alpha_0 p_0| <= min(sum_k>=1 |alpha_k| c_k,
+// sum_l>=1 ||alpha of degree l|| d_l) (c_k = max_q |p_k(q)|, d_l the largest
+// norm over q of the degree-l basis values; Cauchy-Schwarz per degree),
+// which bounds hi - lo by twice that.  The rounding of the computed H
+// (quadrature and Gaunt sums: about 1e-10 e^hi in the 2-norm) is covered by
+// the 1e-9 e^hi gramHi taken off the smallest eigenvalue, and a factor 4
+// covers the estimate's own rounding.  Such an H is far from Cholesky
+// breakdown (n eps cond_2(H) << 1).  `ai`: lane k's alpha_k.
+__device__ __forceinline__ bool exponent_range_bound(const NewtonArgs &a, const NewtonProblem &pb, double ai,
+                                                     int lane)
+{
+    const int n = pb.n, maxDeg = pb.maxDeg;
+    const double b1 = warp_sum((lane >= 1 && lane < n) ? fabs(ai) * pb.rangeC[lane] : 0.0);
+    // lane l (1 <= l <= maxDeg) sums alpha_k^2 over degree l's moments
+    // k = l (l + 1) / 2 .. l (l + 1) / 2 + l
+    const double sq = (lane < n) ? ai * ai : 0.0;
+    const int base = lane * (lane + 1) / 2;
+    double gl = 0.0;
+    for (int j = 0; j <= maxDeg; j++) {
+        const double v = __shfl_sync(0xffffffffu, sq, min(base + j, 31));
+        if (j <= lane && base + j < n)
+            gl += v;
+    }
+    const double b2 = warp_sum((lane >= 1 && lane <= maxDeg) ? sqrt(gl) * pb.rangeC[n + lane] : 0.0);
+    const double span = 2.0 * fmin(b1, b2) * (1.0 + 1e-12);
+    if (!(span <= 40.0))
+        return false;
+    const double ratio = exp(span);
+    const double lmin = pb.gramLo - 1e-9 * ratio * pb.gramHi;
+    if (!(lmin > 0.0))
+        return false;
+    return (double)n * ratio * pb.gramHi * (1.0 + 1e-9) <= 0.25 * a.condHMax * lmin;
+}
+
+// Newton logic for one slot after its evaluation (warp-wide).  `range`: the
+// evaluation is Mn in FP64 (the exponent-range test applies).
 __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
-                           int warp)
+                           int warp, bool range)
 {
     const int n = pb.n;
     const int ldv = a.ldv, ldG = a.ldG, ldh = a.ldh;
@@ -558,23 +601,13 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     double *vec = L.vec + warp * 64;
     const double *Gs = L.G + s * ldG;
 
-    // H from the contraction results
-    hessian_from_contractions(a, pb, L, Gs, Hs, lane);
-    __syncwarp();
-
     const double ui = act ? L.u[s * ldv + lane] : 0.0;
     const double ai = act ? L.alpha[s * ldv + lane] : 0.0;
-    double gi;
-    if (a.momentType == 0)
-        gi = act ? Hs[lane] / pb.p0 - ui : 0.0;     // fobj.cpp:303-306
-    else
-        gi = act ? Gs[pb.K2p + lane] - ui : 0.0;    // fobj.cpp:427-431 / :445-452
     const double au = warp_sum(ai * ui);
     double fpart = 0.0;
     for (int k = 0; k < a.ntq; k++)
         fpart += L.fpart[s * a.ntq + k];
     const double fsum = fpart - au;                  // no-Hessian f (linesearch's fobj)
-    const double fH = (a.momentType == 0) ? Hs[0] / (pb.p0 * pb.p0) - au : fsum;
 
     int state = si[SI_STATE];
     if (state == S_TRIAL) {
@@ -642,6 +675,43 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         si[SI_ITER] = iter;
         si[SI_TOTAL] += 1;
     }
+    // the stopping test applies (no gamma test, iterations left, the last
+    // line search moved)
+    const bool stopTest = !(a.tolGamma > 0.0) && iter < si[SI_MAXITER] && sc[SC_T] != 0.0;
+    if (range && a.momentType == 0 && pb.gramLo > 0.0 && stopTest) {
+        // Converged with the condition test passing by the exponent range:
+        // the gradient needs row 0 of H only (the same sums, in the same
+        // order, as the full contraction), and the reference's outcome is
+        // convergence at this iteration.  A finite gradient implies finite
+        // G (G_0 is a sum of positive terms), so the full contraction's
+        // zero-padded entries would add exact zeros.
+        double h0 = 0.0;
+        if (act) {
+            if (a.useGaunt) {
+                const int e1 = pb.row0Off[lane + 1];
+                for (int e = pb.row0Off[lane]; e < e1; e++)
+                    h0 = fma(pb.row0Val[e], Gs[pb.row0Idx[e]], h0);
+            } else {
+                h0 = Gs[pb.pcol ? pb.pcol[lane] : lane];
+            }
+        }
+        const double g0 = act ? h0 / pb.p0 - ui : 0.0;
+        if (sqrt(warp_sum(g0 * g0)) <= sc[SC_RTOL] && exponent_range_bound(a, pb, ai, lane)) {
+            converge(a, pb, L, s, ui, ai, g0, lane);
+            return;
+        }
+    }
+
+    // H from the contraction results
+    hessian_from_contractions(a, pb, L, Gs, Hs, lane);
+    __syncwarp();
+    double gi;
+    if (a.momentType == 0)
+        gi = act ? Hs[lane] / pb.p0 - ui : 0.0;     // fobj.cpp:303-306
+    else
+        gi = act ? Gs[pb.K2p + lane] - ui : 0.0;    // fobj.cpp:427-431 / :445-452
+    const double fH = (a.momentType == 0) ? Hs[0] / (pb.p0 * pb.p0) - au : fsum;
+
     // row `lane` of H in registers; utils_norm1 = max absolute row sum
     double h[kMaxN], v[kMaxN];
     double rowsum = 0.0;
@@ -663,7 +733,7 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     //          cannot break down, so the factorisation is not needed either;
     //  tier 1: after the factorisation, the comparison-matrix bound.
     const double err = sqrt(warp_sum(gi * gi));
-    const bool convTest = err <= sc[SC_RTOL] && !(a.tolGamma > 0.0) && iter < si[SI_MAXITER] && sc[SC_T] != 0.0;
+    const bool convTest = err <= sc[SC_RTOL] && stopTest;
     if (convTest) {
         const double dom = act ? 2.0 * Hs[lane * ldh + lane] - rowsum : DBL_MAX;
         const double delta = -warp_max(-dom);
@@ -2080,7 +2150,7 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
                 if (a.optType != 0)
                     slot_logic_cb(a, pb, L, s, lane, warp);
                 else
-                    slot_logic(a, pb, L, s, lane, warp);
+                    slot_logic(a, pb, L, s, lane, warp, PPN == 0 && MIX == 0);
             }
         }
         if constexpr (NTF > 0)

@@ -242,6 +242,13 @@ int cl_get_tuning(cl_ctx *ctx, cl_tuning *out);
 /* Forces the shapes (CL_ERR_ARG where the configuration has no such
  * instance): newton_warps 8 or 4, contractions CL_CONTRACT_PAIRS/_SINGLE. */
 int cl_set_launch_shape(cl_ctx *ctx, int newton_warps, int newton_contraction, int flux_contraction);
+/* The exponent-range test of K1 (on by default; Mn in FP64): an evaluation
+ * whose gradient meets the tolerance converges without forming the Hessian
+ * when the range of alpha . p over the quadrature bounds the Hessian's
+ * condition number below MOMOPT_COND_H_MAX / 4 -- the reference's outcome
+ * (opt.cpp:244-306) at that evaluation.  Results are bit-identical with the
+ * test on or off; off runs every evaluation through the Hessian. */
+int cl_set_range_test(cl_ctx *ctx, int enable);
 
 /* Batched per-vector operator: the GPU equivalent of calling
  * opt(n, n2, nq, u, alpha, options, w, p, &outs) (opt.cpp:82-148) on `count`

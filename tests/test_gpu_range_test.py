@@ -1,0 +1,93 @@
+"""K1's exponent-range convergence test (cl_set_range_test).
+
+At a Mn evaluation whose gradient meets the tolerance, the reference
+(opt.cpp:244-306) factors H, estimates its condition number and converges
+when the estimate is at most MOMOPT_COND_H_MAX.  K1 decides that outcome
+without forming H when the range of alpha . p over the quadrature (bounded
+from the multipliers) bounds cond(H) below MOMOPT_COND_H_MAX / 4.  The test
+only skips work, so every result must be bit-identical with it off, where
+each evaluation goes through the Hessian, its factorisation and the
+condition bounds.
+"""
+import numpy as np
+import pytest
+
+import closures_b200 as cb
+import decks
+
+pytestmark = pytest.mark.gpu
+
+M6 = dict(num_cells_x=60, num_cells_y=60, gaussian_sigma=0.08, floor=1e-8, moment_order=6, quad_order=40,
+          tol=1e-8, use_gaunt=1)
+M2_PRODUCTS = dict(num_cells_x=40, num_cells_y=40, gaussian_sigma=0.1, floor=1e-6, moment_order=2,
+                   quad_order=20, tol=1e-8, use_gaunt=0)
+M4_LATTICE = dict(num_cells_x=40, num_cells_y=40, a_x=-3.5, b_x=3.5, a_y=-3.5, b_y=3.5, init_cond="lattice",
+                  floor=1e-10, moment_order=4, quad_order=30, tol=1e-8, use_gaunt=1)
+
+CASES = {
+    "m6_gaunt_pairs": (M6, None),
+    "m6_gaunt_single": (M6, (8, cb.CL_CONTRACT_SINGLE, cb.CL_CONTRACT_PAIRS)),
+    "m6_gaunt_4warp": (M6, (4, cb.CL_CONTRACT_PAIRS, cb.CL_CONTRACT_PAIRS)),
+    "m2_products": (M2_PRODUCTS, None),
+    "m4_lattice": (M4_LATTICE, None),
+}
+
+
+def _grid_run(tmp_path, kw, shape, on, steps):
+    deck = str(tmp_path / ("input_%d.deck" % on))
+    decks.write_deck(deck, decks.deck_text(**kw, extra={"MOMOPT_GPU_TUNE": "0"}))
+    s = cb.Solver(deck, str(tmp_path))
+    ctx = s.context()
+    if shape is not None:
+        ctx.set_launch_shape(*shape)
+    ctx.set_range_test(on)
+    for _ in range(steps):
+        s.update(s.max_dt)
+    m, a = ctx.get_state()
+    it = s.last_iterations()
+    st = s.stats()
+    s.close()
+    return m, a, it, st
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_grid_bit_identical_with_and_without(tmp_path, case):
+    kw, shape = CASES[case]
+    on = _grid_run(tmp_path, kw, shape, 1, 4)
+    off = _grid_run(tmp_path, kw, shape, 0, 4)
+    assert np.array_equal(on[0], off[0]) and np.array_equal(on[1], off[1])
+    assert np.array_equal(on[2], off[2])
+    for key in ("total_iter", "total_trials", "hist_reg"):
+        assert on[3][key] == off[3][key], key
+
+
+def _batch(ctx, u, alpha):
+    uu, aa = u.copy(), alpha.copy()
+    it, reg, st = ctx.solve_batch(uu, aa, check=False)
+    return uu, aa, it, reg, st
+
+
+@pytest.mark.parametrize("order,Q,gaunt", [(6, 40, 1), (3, 30, 0), (4, 30, 1)])
+def test_batch_bit_identical_with_and_without(order, Q, gaunt):
+    """Cold starts (isotropic), the converged multipliers as starts (every
+    vector converges at its first evaluation) and perturbed starts."""
+    a = cb.Angular(order, Q, gaunt)
+    u, alpha_exact = cb.sample_moment_vectors(a, 4096, seed=31, s_range=(0.1, 20.0))
+    ctxs = {}
+    for on in (1, 0):
+        ctxs[on] = cb.Context.for_batches(a, cb.make_options(tol=1e-8))
+        ctxs[on].set_range_test(on)
+    cold = {on: _batch(ctxs[on], u, cb.isotropic_alpha(a.n, u.shape[0])) for on in (1, 0)}
+    for x, y in zip(cold[1], cold[0]):
+        assert np.array_equal(x, y)
+    assert np.all(cold[1][4] == 0)
+    conv = cold[1][1]
+    again = {on: _batch(ctxs[on], u, conv) for on in (1, 0)}
+    for x, y in zip(again[1], again[0]):
+        assert np.array_equal(x, y)
+    warm = conv + 1e-4 * np.random.default_rng(5).standard_normal(conv.shape)
+    pert = {on: _batch(ctxs[on], u, warm) for on in (1, 0)}
+    for x, y in zip(pert[1], pert[0]):
+        assert np.array_equal(x, y)
+    for c in ctxs.values():
+        c.close()
