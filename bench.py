@@ -66,6 +66,24 @@ def flops_per_trial(n, nq):
     return nq * (2 * n + 2)
 
 
+def flops_per_screen(n, nq):
+    """One evaluation of K1's screening pass: alpha.m and the gradient sums
+    over the quadrature (no Hessian columns)."""
+    return nq * 4 * n
+
+
+def newton_flops(s0, s1, per_iter, n, nq):
+    """Algorithmic FLOPs of K1 between two stats snapshots: full Newton
+    iterations, line-search trials, and the screening pass's evaluations (the
+    solves it settled count one iteration in total_iter but did not form the
+    Hessian)."""
+    iters = s1["total_iter"] - s0["total_iter"]
+    trials = s1["total_trials"] - s0["total_trials"]
+    screened = s1.get("screened", 0) - s0.get("screened", 0)
+    evals = s1.get("screen_evals", 0) - s0.get("screen_evals", 0)
+    return (iters - screened) * per_iter + trials * flops_per_trial(n, nq) + evals * flops_per_screen(n, nq)
+
+
 def flops_flux_stage(C, C_int, n, nq):
     """solveFlux per stage: ansatz alpha.m on all cells, stencil + projection
     on interior cells (momopt_update.cpp:96-202)."""
@@ -447,7 +465,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         newton_ms = float(km[0] + km[2])
         flux_ms = float(km[1] + km[3])
         device_ms = float(km.sum())
-        f_newton = iters * per_iter + trials * flops_per_trial(n, ang.nq)
+        f_newton = newton_flops(s0, s1, per_iter, n, ang.nq)
         f_flux = 2 * k * flops_flux_stage(C, C_int, n, ang.nq)
         return {
             "t_start": t_start, "steps": k,
@@ -456,6 +474,8 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
             "ms_per_step": device_ms / k, "steps_per_s": 1e3 * k / device_ms,
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
             "fallback_restarts": s1["fallbacks"] - s0["fallbacks"],
+            "screened_per_solve": (s1["screened"] - s0["screened"]) / solves,
+            "screen_evals_per_solve": (s1["screen_evals"] - s0["screen_evals"]) / solves,
             "kernel_ms": {"newton": newton_ms, "flux": flux_ms},
             "newton_tflops": f_newton / (newton_ms * 1e-3) / 1e12,
             "flux_tflops": f_flux / (flux_ms * 1e-3) / 1e12,
@@ -848,8 +868,7 @@ def native_arm(args, world, rank, local):
         # the change of basis adds the two triangular solves of
         # H_P = T^-1 H_M T^-T and the basis update T <- T L (n^3 each)
         per_iter += 3.0 * n ** 3
-    f_newton = iters * per_iter + \
-        trials * flops_per_trial(n, ang.nq)
+    f_newton = newton_flops(st0, st1, per_iter, n, ang.nq)
     f_flux = 2 * args.steps * flops_flux_stage(C, C_int, n, ang.nq)
     ach_newton = f_newton / (newton_ms * 1e-3) / 1e12
     ach_flux = f_flux / (flux_ms * 1e-3) / 1e12

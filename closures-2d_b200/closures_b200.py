@@ -65,14 +65,15 @@ class cl_node(C.Structure):
 class cl_stats(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
                 ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64),
-                ("total_trials", C.c_int64), ("fallbacks", C.c_int64)]
+                ("total_trials", C.c_int64), ("fallbacks", C.c_int64), ("screened", C.c_int64),
+                ("screen_evals", C.c_int64)]
 
 
 class cl_tuning(C.Structure):
     _fields_ = [("newton_warps", C.c_int), ("newton_ctas", C.c_int), ("newton_contraction", C.c_int),
                 ("flux_contraction", C.c_int), ("from_cache", C.c_int), ("ncand", C.c_int),
                 ("cand_kernel", C.c_int * 8), ("cand_warps", C.c_int * 8),
-                ("cand_contraction", C.c_int * 8), ("cand_ms", C.c_float * 8)]
+                ("cand_contraction", C.c_int * 8), ("cand_ms", C.c_float * 8), ("screen_ctas", C.c_int)]
 
 
 _CONTRACTION_NAMES = {0: "pairs", 1: "single"}
@@ -89,7 +90,7 @@ def _tuning_dict(t):
             "newton_ctas": t.newton_ctas,
             "newton_contraction": _CONTRACTION_NAMES.get(t.newton_contraction),
             "flux_contraction": _CONTRACTION_NAMES.get(t.flux_contraction),
-            "from_cache": bool(t.from_cache), "candidates": cands}
+            "from_cache": bool(t.from_cache), "candidates": cands, "screen_ctas": t.screen_ctas}
 
 
 _lib = None
@@ -381,7 +382,8 @@ class Context:
         _check(lib().cl_get_stats(self._ctx, C.byref(s)), self._err)
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
-                "total_trials": s.total_trials, "fallbacks": s.fallbacks}
+                "total_trials": s.total_trials, "fallbacks": s.fallbacks,
+                "screened": s.screened, "screen_evals": s.screen_evals}
 
     def solve_batch(self, u, alpha, check=True):
         """opt() on every row of u/alpha (in place).  Returns iters, reg, status."""
@@ -585,7 +587,8 @@ class Solver:
         _check(lib().cl_get_stats(ctx, C.byref(s)), lambda: lib().cl_last_error(ctx))
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
-                "total_trials": s.total_trials, "fallbacks": s.fallbacks}
+                "total_trials": s.total_trials, "fallbacks": s.fallbacks,
+                "screened": s.screened, "screen_evals": s.screen_evals}
 
     def close(self):
         if self._s:

@@ -75,6 +75,13 @@ struct DeviceBasis {
     double *rangeC = nullptr;   // max_q |p_k(q)|, then max_q of each degree's norm
     double gramLo = 0, gramHi = 0;
     int maxDeg = 0;
+    // screening layout (paired): the basis columns and the gradient columns
+    // of G only (the first n Gaunt or product columns in the parity groups)
+    double *Ps = nullptr;
+    int ldPs = 0, K2ps = 0, K2es = 0;
+    unsigned short *r0idxS = nullptr;   // row-0 Gaunt entries in the screening columns
+    int *pcolS = nullptr;               // products (k, 0) in the screening columns
+    int screenOk = 0;
 
     void release()
     {
@@ -100,6 +107,9 @@ struct DeviceBasis {
         cudaFree(r0idx);
         cudaFree(r0val);
         cudaFree(rangeC);
+        cudaFree(Ps);
+        cudaFree(r0idxS);
+        cudaFree(pcolS);
         *this = DeviceBasis();
     }
 };
@@ -346,6 +356,51 @@ cudaError_t build_device_basis(DeviceBasis &B, int n, int n2, int nq, int useGau
         if ((e = upload(&B.ellVal, eval)) != cudaSuccess) return e;
         if ((e = upload(&B.ellOff, eoff)) != cudaSuccess) return e;
     }
+    if (paired) {
+        // Screening layout: the gradient needs G columns k < n (Gaunt) or the
+        // products (k, 0) (both of degree deg k).  In the full layout they are
+        // the first entries of their parity group, so here they keep their
+        // positions within the group (and within their 8-column tile), the
+        // odd group starting at K2es.
+        int ne = 0;
+        for (int k = 0; k < n; k++)
+            ne += (degB[k] % 2 == 0);
+        B.K2es = round_up(ne, 8);
+        B.K2ps = B.K2es + round_up(n - ne, 8);
+        std::vector<int> colS(n);
+        bool ok = true;
+        for (int k = 0; k < n; k++) {
+            colS[k] = (degB[k] % 2 == 0) ? colH[k] : colH[k] - B.K2e + B.K2es;
+            ok = ok && (degH[k] == degB[k]) && colS[k] >= 0 && colS[k] < B.K2ps;
+        }
+        int ldPs = B.nb + B.K2ps;
+        while (ldPs % 16 != 4)
+            ldPs++;
+        B.ldPs = ldPs;
+        std::vector<double> Ps((size_t)B.nqp * ldPs + B.nqp, 0.0);
+        for (int r = 0; r < rows; r++) {
+            const int q = (r / Q) * 2 * Q + r % Q;
+            const double *pq = p + (size_t)q * n2;
+            double *row = &Ps[(size_t)basis_row(r, ldPs)];
+            for (int k = 0; k < n; k++)
+                row[colB[k]] = pq[k];
+            for (int k = 0; k < n; k++)
+                row[B.nb + colS[k]] = useGaunt ? pq[k] : pq[prod[k] >> 8] * pq[prod[k] & 255];
+            Ps[(size_t)basis_wgap(r, ldPs)] = w[q];
+        }
+        if ((e = upload(&B.Ps, Ps)) != cudaSuccess) return e;
+        if (useGaunt) {
+            std::vector<unsigned short> r0s;
+            for (int k = goff[0]; k < goff[n]; k++) {
+                ok = ok && gidx[k] < n;
+                r0s.push_back((unsigned short)(gidx[k] < n ? colS[gidx[k]] : 0));
+            }
+            if ((e = upload(&B.r0idxS, r0s)) != cudaSuccess) return e;
+        } else {
+            if ((e = upload(&B.pcolS, colS)) != cudaSuccess) return e;
+        }
+        B.screenOk = ok ? 1 : 0;
+    }
     return cudaSuccess;
 }
 
@@ -405,6 +460,23 @@ NewtonProblem make_problem(const DeviceBasis &B)
     pb.K2e = B.K2e;
     pb.binv = B.binv;
     pb.pcol = B.pcol;
+    return pb;
+}
+
+// The screening pass's view of the basis: the gradient-column layout.
+static NewtonProblem make_screen_problem(const DeviceBasis &B)
+{
+    NewtonProblem pb = make_problem(B);
+    pb.P = B.Ps;
+    pb.ldP = B.ldPs;
+    pb.K2p = B.K2ps;
+    pb.K2e = B.K2es;
+    pb.row0Idx = B.r0idxS;
+    pb.pcol = B.pcolS;
+    pb.ellPair = pb.ellIdx = nullptr;
+    pb.ellVal = nullptr;
+    pb.ellOff = nullptr;
+    pb.ellChunks = pb.ellRows = 0;
     return pb;
 }
 
@@ -509,6 +581,13 @@ struct cl_ctx {
     DeviceBasis B2;
     int newtonB2 = 0, fluxB2 = 0;
     int rangeTest = 1;   // K1's exponent-range test (cl_set_range_test)
+    // screening pass before K1 in grid stages (Mn, FP64, direction pairs):
+    // its arguments, CTAs, the list of cells left for K1 and, per stage or
+    // band, the list length and the screening work counter
+    NewtonArgs sargs;
+    int screen = 0, nCtasScreen = 0;
+    int *dPend = nullptr, *dPendCount = nullptr, *dGate = nullptr;
+    unsigned int *dScreenQ = nullptr;
     int angN = 0, angN2 = 0, angNq = 0, angGaunt = 0, angNnz = 0;
     std::vector<double> aw, axi, aeta, ap, agval;
     std::vector<int> agoff, agidx;
@@ -517,6 +596,8 @@ struct cl_ctx {
 };
 
 extern "C" {
+
+static void update_screen(cl_ctx *ctx);
 
 const char *cl_global_error(void) { return g_global_err.c_str(); }
 
@@ -684,7 +765,11 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         cudaMalloc(&ctx->dSigS, C * 8) != cudaSuccess || cudaMalloc(&ctx->dQueue, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&ctx->dStats, sizeof(DevStats)) != cudaSuccess || cudaMalloc(&ctx->dErr, 2 * sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&ctx->dIters, C * sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&ctx->dIters, C * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dPend, C * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dPendCount, (4 + kHostBands) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dScreenQ, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&ctx->dGate, (4 + kHostBands) * sizeof(int)) != cudaSuccess) {
         ctx->err = "device allocation failed";
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
@@ -799,6 +884,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         ctx->err = std::string("set-up: ") + cudaGetErrorString(cudaGetLastError());
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
+    update_screen(ctx);
     ctx->tuning.newton_warps = a.nw;
     ctx->tuning.newton_ctas = ctx->nCtas;
     ctx->tuning.newton_contraction = ctx->B.paired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
@@ -822,6 +908,10 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->dMom);
     cudaFree(ctx->dAlpha);
     cudaFree(ctx->dOld);
+    cudaFree(ctx->dPend);
+    cudaFree(ctx->dPendCount);
+    cudaFree(ctx->dScreenQ);
+    cudaFree(ctx->dGate);
     cudaFree(ctx->dSigT);
     cudaFree(ctx->dSigS);
     cudaFree(ctx->dQueue);
@@ -870,6 +960,80 @@ static int enqueue_prediction(cl_ctx *ctx, cudaStream_t st)
     return 2 + 4 * chunks;
 }
 
+// Screening before K1 where it applies: Mn, FP64, plain Newton, K1 on the
+// direction-pair layout with the exponent-range test on.
+static void update_screen(cl_ctx *ctx)
+{
+    ctx->screen = 0;
+    ctx->tuning.screen_ctas = 0;
+    const DeviceBasis &B = ctx->newtonB2 ? ctx->B2 : ctx->B;
+    const NewtonArgs &k = ctx->nargs;
+    if (!ctx->rangeTest || !ctx->dPend || !B.paired || !B.screenOk || k.nprob != 1 || k.momentType != 0 ||
+        k.mixed || k.optType != 0 || !(k.prob[0].gramLo > 0.0))
+        return;
+    NewtonArgs s = k;
+    s.prob[0] = make_screen_problem(B);
+    if (plan_screen(s) != 0 || prepare_screen(s) != cudaSuccess)
+        return;
+    ctx->sargs = s;
+    ctx->nCtasScreen = sm_count() * screen_ctas_per_sm(s);
+    ctx->screen = 1;
+    ctx->tuning.screen_ctas = ctx->nCtasScreen;
+}
+
+// Fraction of a launch's cells whose previous solve took one iteration, at
+// or above which the screening pass runs: then it settles most cells, and
+// K1's time over the rest is not set by long Newton chains the easy cells
+// would have run beside.
+constexpr double kScreenGate = 0.85;
+
+// K1 of a grid stage or band (`a` complete; `slot` selects the counters):
+// with screening, the gate count, the screening pass over the same cells,
+// then K1 over the cells it left (or over all of them when the gate stays
+// shut).
+static cudaError_t launch_stage_newton(cl_ctx *ctx, NewtonArgs &a, int slot, cudaStream_t st, int *nk)
+{
+    cudaError_t e;
+    if (ctx->screen && a.prob[0].iters) {
+        NewtonArgs s = ctx->sargs;
+        NewtonProblem &sp = s.prob[0];
+        const NewtonProblem &kp = a.prob[0];
+        sp.count = kp.count;
+        sp.first = kp.first;
+        sp.u = kp.u;
+        sp.alpha = kp.alpha;
+        sp.iters = kp.iters;
+        sp.regs = kp.regs;
+        sp.status = kp.status;
+        sp.alphaStart = kp.alphaStart;
+        sp.queue = ctx->dScreenQ + slot;
+        sp.pendList = ctx->dPend + kp.first;
+        sp.pendCount = ctx->dPendCount + slot;
+        sp.gateCount = ctx->dGate + slot;
+        sp.gateMin = (int)std::ceil(kScreenGate * kp.count);
+        s.momentsOld = a.momentsOld;
+        if ((e = cudaMemsetAsync(ctx->dScreenQ + slot, 0, sizeof(unsigned), st)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(ctx->dPendCount + slot, 0, sizeof(int), st)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(ctx->dGate + slot, 0, sizeof(int), st)) != cudaSuccess)
+            return e;
+        if ((e = launch_screen_gate(kp.iters, kp.first, kp.count, ctx->dGate + slot, st)) != cudaSuccess)
+            return e;
+        if ((e = launch_screen(s, ctx->nCtasScreen, st)) != cudaSuccess)
+            return e;
+        *nk += 2;
+        a.prob[0].cellList = ctx->dPend + kp.first;
+        a.prob[0].countDev = ctx->dPendCount + slot;
+        a.prob[0].gateCount = sp.gateCount;
+        a.prob[0].gateMin = sp.gateMin;
+    }
+    if ((e = launch_newton(a, ctx->nCtas, st)) != cudaSuccess)
+        return e;
+    *nk += 1;
+    return cudaSuccess;
+}
+
 // Enqueues RK stage `stage` (0 or 1) on the context's stream: [periodic
 // ghost copy], [warm-start prediction], K1, K2+K3 (stage 1 also the Heun
 // average).  The stage's work counter must be zero when K1 starts.
@@ -898,9 +1062,8 @@ static cudaError_t enqueue_stage(cl_ctx *ctx, int stage, double dt, double dx, d
     a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
     if (beforeK1 && (e = cudaEventRecord(beforeK1, ctx->stream)) != cudaSuccess)
         return e;
-    if ((e = launch_newton(a, ctx->nCtas, ctx->stream)) != cudaSuccess)
+    if ((e = launch_stage_newton(ctx, a, stage, ctx->stream, nk)) != cudaSuccess)
         return e;
-    *nk += 1;
     if (afterK1 && (e = cudaEventRecord(afterK1, ctx->stream)) != cudaSuccess)
         return e;
     FluxArgs f = ctx->fargs;
@@ -1017,8 +1180,7 @@ int cl_step_timed(cl_ctx *ctx, double dt, double dx, double dy, float *ms)
         a.prob[0].alphaStart = ctx->warm ? ctx->dAlphaPred : nullptr;
         a.momentsOld = (stage == 0) ? ctx->dOld : nullptr;
         if (e == cudaSuccess)
-            e = launch_newton(a, ctx->nCtas, ctx->stream);
-        nk++;
+            e = launch_stage_newton(ctx, a, stage, ctx->stream, &nk);
         cudaEventRecord(ev[3 * stage + 1], ctx->stream);
         FluxArgs f = ctx->fargs;
         f.dt = dt;
@@ -1238,9 +1400,10 @@ int cl_step_host(cl_ctx *ctx, double dt, double dx, double dy, double *moments, 
             a.prob[0].first = (stage == 0) ? (int)band0[b] : 0;
             a.prob[0].count = (stage == 0) ? (int)(band0[b + 1] - band0[b]) : (int)C;
             a.prob[0].queue = ctx->dQueue + ((stage == 0 && bands > 1) ? 4 + b : stage);
-            if (e == cudaSuccess)
-                run(launch_newton(a, ctx->nCtas, S));
-            nk++;
+            if (e == cudaSuccess) {
+                NewtonArgs ab = a;   // the band's own list and counters
+                run(launch_stage_newton(ctx, ab, (stage == 0 && bands > 1) ? 4 + b : stage, S, &nk));
+            }
         }
         FluxArgs f = ctx->fargs;
         f.dt = dt;
@@ -1394,9 +1557,10 @@ struct TuneScratch {
     }
 };
 
-// Median K1 time (ms) of `a` over the context's state (copies); < 0 if a
-// launch failed or reported an error.
-static float time_newton(cl_ctx *ctx, NewtonArgs a, TuneScratch &S)
+// Median K1 time (ms) of `a` (basis B) over the context's state (copies),
+// the screening pass included where it applies to B; < 0 if a launch failed
+// or reported an error.
+static float time_newton(cl_ctx *ctx, NewtonArgs a, const DeviceBasis &B, TuneScratch &S)
 {
     const size_t C = (size_t)ctx->C, n = (size_t)ctx->n;
     a.prob[0].count = (int)C;
@@ -1412,15 +1576,46 @@ static float time_newton(cl_ctx *ctx, NewtonArgs a, TuneScratch &S)
     a.stats = S.st;
     a.err = S.err;
     const int grid = sm_count() * newton_ctas_per_sm(a);
+    NewtonArgs sa;
+    int sgrid = 0;
+    if (ctx->rangeTest && ctx->dPend && B.paired && B.screenOk && a.nprob == 1 && a.momentType == 0 &&
+        !a.mixed && a.optType == 0 && a.prob[0].gramLo > 0.0) {
+        sa = a;
+        sa.prob[0] = make_screen_problem(B);
+        if (plan_screen(sa) == 0 && prepare_screen(sa) == cudaSuccess) {
+            NewtonProblem &sp = sa.prob[0];
+            sp.count = (int)C;
+            sp.u = S.u;
+            sp.alpha = S.a;
+            sp.iters = S.it;
+            sp.queue = S.q + 1;
+            sp.pendList = ctx->dPend;
+            sp.pendCount = (int *)(S.q + 2);
+            sp.gateCount = (const int *)(S.q + 3);
+            sp.gateMin = (int)std::ceil(kScreenGate * (double)C);
+            sgrid = sm_count() * screen_ctas_per_sm(sa);
+            a.prob[0].cellList = ctx->dPend;
+            a.prob[0].countDev = (const int *)(S.q + 2);
+            a.prob[0].gateCount = sp.gateCount;
+            a.prob[0].gateMin = sp.gateMin;
+        }
+    }
     float ms[3] = {0, 0, 0};
     cudaStream_t st = ctx->stream;
     for (int r = 0; r < 4; r++) {
         if (cudaMemcpyAsync(S.u, ctx->dMom, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
             cudaMemcpyAsync(S.a, ctx->dAlpha, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-            cudaMemsetAsync(S.q, 0, sizeof(unsigned), st) != cudaSuccess ||
+            cudaMemcpyAsync(S.it, ctx->dIters, C * sizeof(int), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemsetAsync(S.q, 0, 4 * sizeof(unsigned), st) != cudaSuccess ||
             cudaMemsetAsync(S.err, 0, 2 * sizeof(int), st) != cudaSuccess)
             return -1.0f;
         cudaEventRecord(S.e0, st);
+        if (sgrid > 0) {
+            if (launch_screen_gate(S.it, 0, (int)C, (int *)(S.q + 3), st) != cudaSuccess ||
+                launch_screen(sa, sgrid, st) != cudaSuccess)
+                return -1.0f;
+            g_launches += 2;
+        }
         if (launch_newton(a, grid, st) != cudaSuccess)
             return -1.0f;
         g_launches++;
@@ -1498,6 +1693,7 @@ static int apply_shape(cl_ctx *ctx, int nw, int ncontr, int fcontr)
     ctx->fluxB2 = (bf == &ctx->B2);
     if (!ctx->newtonB2 && !ctx->fluxB2)
         ctx->B2.release();
+    update_screen(ctx);
     invalidate_graph(ctx);
     ctx->tuning.newton_warps = nw;
     ctx->tuning.newton_ctas = ctx->nCtas;
@@ -1567,6 +1763,7 @@ int cl_set_range_test(cl_ctx *ctx, int enable)
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->rangeTest = enable ? 1 : 0;
     ctx->nargs.prob[0].gramLo = enable ? make_problem(ctx->newtonB2 ? ctx->B2 : ctx->B).gramLo : 0.0;
+    update_screen(ctx);
     invalidate_graph(ctx);
     return CL_OK;
 }
@@ -1617,7 +1814,7 @@ int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out)
     TuneScratch S;
     if (cudaMalloc(&S.u, C * n * 8) != cudaSuccess || cudaMalloc(&S.a, C * n * 8) != cudaSuccess ||
         cudaMalloc(&S.it, C * sizeof(int)) != cudaSuccess || cudaMalloc(&S.err, 2 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&S.q, sizeof(unsigned)) != cudaSuccess || cudaMalloc(&S.st, sizeof(DevStats)) != cudaSuccess ||
+        cudaMalloc(&S.q, 4 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&S.st, sizeof(DevStats)) != cudaSuccess ||
         cudaEventCreate(&S.e0) != cudaSuccess || cudaEventCreate(&S.e1) != cudaSuccess) {
         ctx->err = "tuner scratch";
         return CL_ERR_CUDA;
@@ -1635,7 +1832,7 @@ int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out)
             NewtonArgs a;
             if (!newton_shape(ctx, *B, nw, a))
                 continue;
-            const float ms = time_newton(ctx, a, S);
+            const float ms = time_newton(ctx, a, *B, S);
             if (ms < 0 || T.ncand >= CL_TUNE_MAX)
                 continue;
             const int contr = B->paired ? CL_CONTRACT_PAIRS : CL_CONTRACT_SINGLE;
@@ -1678,6 +1875,7 @@ int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out)
         return rc;
     T.newton_warps = ctx->tuning.newton_warps;
     T.newton_ctas = ctx->tuning.newton_ctas;
+    T.screen_ctas = ctx->tuning.screen_ctas;
     T.newton_contraction = bestNc;
     T.flux_contraction = bestFc;
     ctx->tuning = T;
@@ -1760,6 +1958,8 @@ int cl_get_stats(cl_ctx *ctx, cl_stats *s)
     s->iter_mean = d.numSolves ? (double)d.totalIter / (double)d.numSolves : 0.0;
     s->total_trials = (int64_t)d.trials;
     s->fallbacks = (int64_t)d.fallbacks;
+    s->screened = (int64_t)d.screened;
+    s->screen_evals = (int64_t)d.screenEvals;
     return CL_OK;
 }
 

@@ -160,9 +160,11 @@ struct DevStats {
     unsigned long long numSolves;
     unsigned long long trials;          // line-search evaluations
     unsigned long long fallbacks;       // predicted starts abandoned for the fallback start
+    unsigned long long screened;        // solves settled by the screening pass
+    unsigned long long screenEvals;     // evaluations of the screening pass
     int maxIter;
     int pad;
 };
-constexpr int kStatU64 = kNumReg + 4;
+constexpr int kStatU64 = kNumReg + 6;
 
 }  // namespace clb

@@ -71,7 +71,23 @@ struct NewtonProblem {
     unsigned int *queue;        // work counter, zero before the launch
     int first;                  // index of the first work item: the launch solves
                                 // items first .. first + count - 1 (a band of cells)
+    // K1 after a screening pass: the cells to solve are cellList[0 .. *countDev)
+    // (both null otherwise); the screening pass appends them at
+    // pendList[atomicAdd(pendCount, 1)].  The pass runs only when *gateCount
+    // (cells of the launch whose previous solve took at most one iteration,
+    // from `iters`) is at least gateMin, and evaluates only such cells;
+    // otherwise K1 solves cells first .. first + count - 1 directly.
+    const int *cellList;
+    const int *countDev;
+    int *pendList;
+    int *pendCount;
+    const int *gateCount;
+    int gateMin;
 };
+
+// Cells of [first, first + count) whose previous solve took at most one
+// iteration (iters[c] <= 1), added to *out (zero before the launch).
+cudaError_t launch_screen_gate(const int *iters, int first, int count, int *out, cudaStream_t stream);
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
 // S_HELP: an idle slot lent, for one round, to a slot whose line search is
@@ -130,6 +146,14 @@ cudaError_t prepare_newton(const NewtonArgs &a);
 bool newton_pair_supported(int nt, int nbk);
 // ... and in the 4-warp launch shape.
 bool newton_pair4_supported(int nt, int nbk);
+// Screening pass (Mn, FP64, direction pairs; a.prob[0] the gradient-column
+// layout of the problem): layout, instance check, shared-memory attribute,
+// launch and resident CTAs per SM.
+int plan_screen(NewtonArgs &a);
+bool screen_supported(int nt, int nbk);
+cudaError_t prepare_screen(const NewtonArgs &a);
+cudaError_t launch_screen(const NewtonArgs &a, int grid, cudaStream_t stream);
+int screen_ctas_per_sm(const NewtonArgs &a);
 // Launches the persistent kernel on `stream` over `grid` CTAs.
 cudaError_t launch_newton(const NewtonArgs &a, int grid, cudaStream_t stream);
 int newton_ctas_per_sm(const NewtonArgs &a);

@@ -587,6 +587,23 @@ __device__ __forceinline__ bool exponent_range_bound(const NewtonArgs &a, const 
     return (double)n * ratio * pb.gramHi * (1.0 + 1e-9) <= 0.25 * a.condHMax * lmin;
 }
 
+// H_0,lane (lane < n) from the contraction results: the row-0 entries of the
+// Gaunt table in its order (the sums of the full contraction without its zero
+// padding), or the product column (lane, 0).
+__device__ __forceinline__ double hessian_row0(const NewtonArgs &a, const NewtonProblem &pb, const double *Gs,
+                                               int lane)
+{
+    double h0 = 0.0;
+    if (a.useGaunt) {
+        const int e1 = pb.row0Off[lane + 1];
+        for (int e = pb.row0Off[lane]; e < e1; e++)
+            h0 = fma(pb.row0Val[e], Gs[pb.row0Idx[e]], h0);
+    } else {
+        h0 = Gs[pb.pcol ? pb.pcol[lane] : lane];
+    }
+    return h0;
+}
+
 // Newton logic for one slot after its evaluation (warp-wide).  `range`: the
 // evaluation is Mn in FP64 (the exponent-range test applies).
 __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane,
@@ -685,17 +702,7 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
         // convergence at this iteration.  A finite gradient implies finite
         // G (G_0 is a sum of positive terms), so the full contraction's
         // zero-padded entries would add exact zeros.
-        double h0 = 0.0;
-        if (act) {
-            if (a.useGaunt) {
-                const int e1 = pb.row0Off[lane + 1];
-                for (int e = pb.row0Off[lane]; e < e1; e++)
-                    h0 = fma(pb.row0Val[e], Gs[pb.row0Idx[e]], h0);
-            } else {
-                h0 = Gs[pb.pcol ? pb.pcol[lane] : lane];
-            }
-        }
-        const double g0 = act ? h0 / pb.p0 - ui : 0.0;
+        const double g0 = act ? hessian_row0(a, pb, Gs, lane) / pb.p0 - ui : 0.0;
         if (sqrt(warp_sum(g0 * g0)) <= sc[SC_RTOL] && exponent_range_bound(a, pb, ai, lane)) {
             converge(a, pb, L, s, ui, ai, g0, lane);
             return;
@@ -1919,16 +1926,18 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
                     break;
                 }
                 const NewtonProblem &pb = a.prob[p];
+                const bool list = pb.cellList && (!pb.gateCount || *pb.gateCount >= pb.gateMin);
+                const int count = list ? *pb.countDev : pb.count;
                 unsigned base = atomicAdd(pb.queue, (unsigned)nIdle);
-                if (base >= (unsigned)pb.count) {
+                if (base >= (unsigned)count) {
                     exhausted = true;
                     continue;
                 }
-                int take = min(nIdle, pb.count - (int)base);
+                int take = min(nIdle, count - (int)base);
                 int c = 0;
                 for (int s = 0; s < T && c < take; s++) {
                     if (L.ints[s * SI_N + SI_STATE] == S_IDLE) {
-                        L.ints[s * SI_N + SI_CELL] = pb.first + (int)base + c;
+                        L.ints[s * SI_N + SI_CELL] = list ? pb.cellList[(int)base + c] : pb.first + (int)base + c;
                         L.ints[s * SI_N + SI_STATE] = S_NEW;
                         c++;
                     }
@@ -2166,6 +2175,164 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
     } else if (tid == kStatU64) {
         atomicMax(&a.stats->maxIter, *(int *)&L.stat[kStatU64]);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Screening pass (Mn, FP64, direction pairs): the first evaluation of every
+// cell of a launch, with the gradient columns of G only (the first n Gaunt or
+// product columns, laid out as in the full layout's parity groups, so each
+// sum is the full evaluation's bit for bit).  A cell whose first Newton
+// iteration converges with the condition test decided by the exponent-range
+// bound (the outcome of opt.cpp:244-306 at that evaluation) is finished here
+// as K1 would finish it; every other cell is appended to pb.pendList, and K1
+// solves those from their starts (the screening evaluation is not counted).
+// Without the Hessian columns, the Newton state and the Gaunt table, a CTA
+// of 8 warps fits twice per SM.
+__device__ void screen_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout &L, int s, int lane)
+{
+    const int n = pb.n, ldv = a.ldv;
+    const bool act = lane < n;
+    int *si = L.ints + s * SI_N;
+    const double *sc = L.scal + s * SC_N;
+    const double ui = act ? L.u[s * ldv + lane] : 0.0;
+    const double ai = act ? L.alpha[s * ldv + lane] : 0.0;
+    bool conv = false;
+    if (lane == 0)
+        atomicAdd(&L.stat[kNumReg + 5], 1ull);
+    // slot_logic's stopping-test conditions at iteration 1 (t = 1)
+    if (!(a.tolGamma > 0.0) && 1 < si[SI_MAXITER]) {
+        const double g0 = act ? hessian_row0(a, pb, L.G + s * a.ldG, lane) / pb.p0 - ui : 0.0;
+        conv = sqrt(warp_sum(g0 * g0)) <= sc[SC_RTOL] && exponent_range_bound(a, pb, ai, lane);
+        if (conv) {
+            __syncwarp();
+            if (lane == 0) {
+                si[SI_ITER] = 1;
+                si[SI_TOTAL] = 1;
+            }
+            __syncwarp();
+            converge(a, pb, L, s, ui, ai, g0, lane);
+            if (lane == 0)
+                atomicAdd(&L.stat[kNumReg + 4], 1ull);
+        }
+    }
+    if (!conv && lane == 0) {
+        pb.pendList[atomicAdd(pb.pendCount, 1)] = si[SI_CELL];
+        si[SI_STATE] = S_IDLE;
+    }
+}
+
+template <int NT, int NBK>
+__global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ NewtonArgs a)
+{
+    constexpr int kThreads = 256, kWarps = 8;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int ctl[2];   // [0] done, [1] next slot of the test
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int T = a.T, ldv = a.ldv;
+    const NewtonProblem &pb = a.prob[0];
+    Layout L = make_layout(sm, a);
+    for (int i = tid; i < 4 * T * ldv; i += kThreads)
+        L.alpha[i] = 0.0;
+    for (int i = tid; i < T * SI_N; i += kThreads)
+        L.ints[i] = (i % SI_N == SI_STATE) ? S_IDLE : 0;
+    for (int i = tid; i <= kStatU64; i += kThreads)
+        L.stat[i] = 0ull;
+    for (int i = tid; i < 64; i += kThreads)
+        L.exptab[i] = a.ex.tab[i];
+    for (int i = tid; i < T * SC_N; i += kThreads)
+        L.scal[i] = 0.0;
+    if (tid == 0) {
+        for (int b = 0; b < 3; b++)
+            mbar_init(&L.bar[b], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    unsigned mbPhase = 0;
+    if (pb.gateCount && *pb.gateCount < pb.gateMin)
+        return;   // most cells iterate: K1 solves them all, in one pass
+    for (;;) {
+        if (tid == 0) {
+            // fill the slots with cells whose previous solve took at most one
+            // iteration; the others go straight to K1's list
+            int filled = 0;
+            bool exhausted = false;
+            while (filled < T && !exhausted) {
+                const unsigned base = atomicAdd(pb.queue, (unsigned)(T - filled));
+                const int take = (base < (unsigned)pb.count) ? min(T - filled, pb.count - (int)base) : 0;
+                exhausted = take < T - filled;
+                for (int k = 0; k < take; k++) {
+                    const int cell = pb.first + (int)base + k;
+                    if (pb.iters && pb.iters[cell] > 1) {
+                        pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
+                    } else {
+                        L.ints[filled * SI_N + SI_CELL] = cell;
+                        L.ints[filled * SI_N + SI_STATE] = S_NEW;
+                        filled++;
+                    }
+                }
+            }
+            for (int s = filled; s < T; s++)
+                L.ints[s * SI_N + SI_STATE] = S_IDLE;
+            ctl[0] = (filled == 0);
+            ctl[1] = 0;
+        }
+        __syncthreads();
+        if (ctl[0])
+            break;
+        for (int s = warp; s < T; s += kWarps)
+            if (L.ints[s * SI_N + SI_STATE] == S_NEW)
+                init_slot(a, pb, L, s, lane, ldv);
+        __syncthreads();
+        if (!phase_a_fused<8, 0, NT, NBK, 0, 1, 8>(a, pb, L, tid, lane, warp, mbPhase))
+            return;   // a staged chunk never arrived (error recorded)
+        for (;;) {
+            int s = 0;
+            if (lane == 0)
+                s = atomicAdd(&ctl[1], 1);
+            s = __shfl_sync(0xffffffffu, s, 0);
+            if (s >= T)
+                break;
+            if (L.ints[s * SI_N + SI_STATE] == S_NEWTON)
+                screen_logic(a, pb, L, s, lane);
+        }
+        fence_proxy_async_smem();   // this round's shared-memory writes before the next bulk copies
+        __syncthreads();
+    }
+    if (tid < kStatU64) {
+        unsigned long long v = L.stat[tid];
+        if (v)
+            atomicAdd(&a.stats->hist[0] + tid, v);
+    } else if (tid == kStatU64) {
+        atomicMax(&a.stats->maxIter, *(int *)&L.stat[kStatU64]);
+    }
+}
+
+__global__ void screen_gate_kernel(const int *iters, int first, int count, int *out)
+{
+    int v = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        v += (iters[first + i] <= 1) ? 1 : 0;
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, m);
+    if ((threadIdx.x & 31) == 0 && v)
+        atomicAdd(out, v);
+}
+
+template <int NT, int NBK>
+cudaError_t screen_run(const NewtonArgs &a, int grid, cudaStream_t stream, int mode, int *occ)
+{
+    auto *k = screen_kernel<NT, NBK>;
+    if (mode == 1)
+        return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, a.smemBytes);
+    if (mode == 2) {
+        int b = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, 256, a.smemBytes);
+        *occ = b < 1 ? 1 : b;
+        return e;
+    }
+    k<<<grid, 256, a.smemBytes, stream>>>(a);
+    return cudaGetLastError();
 }
 
 // One kernel instance: mode 0 launches it, 1 sets its shared-memory limit,

@@ -122,6 +122,11 @@ typedef struct {
     int64_t total_iter;             /* sum of iterations (device counter) */
     int64_t total_trials;           /* line-search function evaluations */
     int64_t fallbacks;              /* predicted starts replaced by the fallback start */
+    int64_t screened;               /* solves settled by K1's screening pass at their first
+                                       evaluation (counted in the fields above as well) */
+    int64_t screen_evals;           /* evaluations run by the screening pass (gradient
+                                       columns only; those of unsettled cells are not
+                                       counted in total_iter) */
 } cl_stats;
 
 typedef struct cl_ctx cl_ctx;
@@ -235,6 +240,7 @@ typedef struct {
     int cand_warps[CL_TUNE_MAX];
     int cand_contraction[CL_TUNE_MAX];
     float cand_ms[CL_TUNE_MAX];          /* median launch time */
+    int screen_ctas;          /* CTAs of K1's screening pass (0: no screening pass) */
 } cl_tuning;
 int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out);   /* use_cache 0: always time */
 /* The shapes in use (after cl_tune, cl_set_launch_shape or the defaults). */

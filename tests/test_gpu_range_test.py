@@ -1,13 +1,16 @@
-"""K1's exponent-range convergence test (cl_set_range_test).
+"""K1's exponent-range convergence test (cl_set_range_test) and the
+screening pass that uses it.
 
 At a Mn evaluation whose gradient meets the tolerance, the reference
 (opt.cpp:244-306) factors H, estimates its condition number and converges
 when the estimate is at most MOMOPT_COND_H_MAX.  K1 decides that outcome
 without forming H when the range of alpha . p over the quadrature (bounded
-from the multipliers) bounds cond(H) below MOMOPT_COND_H_MAX / 4.  The test
-only skips work, so every result must be bit-identical with it off, where
-each evaluation goes through the Hessian, its factorisation and the
-condition bounds.
+from the multipliers) bounds cond(H) below MOMOPT_COND_H_MAX / 4.  With the
+direction-pair layout, a screening pass evaluates every cell first with the
+gradient columns only and settles the cells that converge there; K1 solves
+the rest from their starts.  Both only skip work, so every result must be
+bit-identical with the test off, where each evaluation goes through K1's
+Hessian, its factorisation and the condition bounds.
 """
 import numpy as np
 import pytest
@@ -91,3 +94,35 @@ def test_batch_bit_identical_with_and_without(order, Q, gaunt):
         assert np.array_equal(x, y)
     for c in ctxs.values():
         c.close()
+
+
+def test_host_step_bit_identical_with_and_without(tmp_path):
+    """The banded host-state step (screening per band, each band with its
+    own list of cells left for K1) against the device step with the test
+    off."""
+    import torch
+    kw = dict(num_cells_x=320, num_cells_y=330, gaussian_sigma=0.2, floor=1e-6, moment_order=4,
+              quad_order=30, tol=1e-8, use_gaunt=1)
+    deck = str(tmp_path / "input.deck")
+    decks.write_deck(deck, decks.deck_text(**kw, extra={"MOMOPT_GPU_TUNE": "0"}))
+    a = cb.Solver(deck, str(tmp_path))
+    b = cb.Solver(deck, str(tmp_path))
+    ca, cbx = a.context(), b.context()
+    cbx.set_range_test(False)
+    shape = (ca.NX * ca.NY, ca.n)
+    hm = torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    ha = torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    m0, a0 = ca.get_state()
+    hm[:] = m0.reshape(shape)
+    ha[:] = a0.reshape(shape)
+    for _ in range(3):
+        ca.step_host(a.max_dt, a.dx, a.dy, hm, ha)
+        cbx.step(a.max_dt, a.dx, a.dy)
+    mr, ar = cbx.get_state()
+    np.testing.assert_array_equal(hm, mr.reshape(shape))
+    np.testing.assert_array_equal(ha, ar.reshape(shape))
+    sa, sb = ca.stats(), cbx.stats()
+    assert sa["num_solves"] == sb["num_solves"] and sa["total_iter"] == sb["total_iter"]
+    assert sa["hist_reg"] == sb["hist_reg"]
+    a.close()
+    b.close()
