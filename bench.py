@@ -72,6 +72,23 @@ def flops_per_screen(n, nq):
     return nq * 4 * n
 
 
+def uniform_tile_fraction(alpha):
+    """Fraction of K2+K3's 16x16 tiles whose tile-plus-halo alpha is one
+    value, bit for bit (those tiles apply zero flux without the chunk loop);
+    alpha [NX][NY][n] with the ghost cells."""
+    NX, NY, _ = alpha.shape
+    bits = np.ascontiguousarray(alpha).view(np.int64)
+    eq = np.all(bits == bits[2, 2], axis=2)
+    tx, ty = (NX - 4 + 15) // 16, (NY - 4 + 15) // 16
+    hit = 0
+    for bx in range(tx):
+        for by in range(ty):
+            i0, j0 = 2 + 16 * bx, 2 + 16 * by
+            if i0 + 18 <= NX and j0 + 18 <= NY and eq[i0 - 2:i0 + 18, j0 - 2:j0 + 18].all():
+                hit += 1
+    return hit / (tx * ty)
+
+
 def newton_flops(s0, s1, per_iter, n, nq):
     """Algorithmic FLOPs of K1 between two stats snapshots: full Newton
     iterations, line-search trials, and the screening pass's evaluations (the
@@ -453,6 +470,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
 
     def window(k, t_start):
         """k steps kernel by kernel (CUDA events around every kernel)."""
+        uniform = uniform_tile_fraction(ctx.get_state()[1])
         s0 = solver.stats()
         km = np.zeros(4)
         for _ in range(k):
@@ -474,6 +492,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
             "ms_per_step": device_ms / k, "steps_per_s": 1e3 * k / device_ms,
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
             "fallback_restarts": s1["fallbacks"] - s0["fallbacks"],
+            "flux_uniform_tiles": uniform,
             "screened_per_solve": (s1["screened"] - s0["screened"]) / solves,
             "screen_evals_per_solve": (s1["screen_evals"] - s0["screen_evals"]) / solves,
             "kernel_ms": {"newton": newton_ms, "flux": flux_ms},

@@ -40,12 +40,13 @@ int plan_screen(NewtonArgs &a)
     a.offEllVal = a.offEllIdx = a.offEllPair = a.offEllOff = off;
     a.offExp = take(64);
     a.offBar = take(4);
+    a.offEg = take(4 * a.ldv);   // the representative start and results
+    a.offE = 0;
     exp_consts_init(a.ex);
     const int unionBase = off;
     const int endG = unionBase + ((T * a.ldG + 1) & ~1);
     const int endA = unionBase + 3 * (a.kq * pb.ldP + a.kq);   // three staged chunks
     a.offP = unionBase;
-    a.offE = a.offEg = 0;
     a.offG = unionBase;
     a.offH = a.offVec = endG;
     a.doubleBuffer = 1;

@@ -2226,11 +2226,22 @@ __global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ 
 {
     constexpr int kThreads = 256, kWarps = 8;
     extern __shared__ __align__(16) double sm[];
-    __shared__ int ctl[2];   // [0] done, [1] next slot of the test
+    __shared__ int ctl[4];   // [0] done, [1] next slot of the test, [2] slots claimed, [3] counter exhausted
+    __shared__ int repValid, repHits;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int T = a.T, ldv = a.ldv;
     const NewtonProblem &pb = a.prob[0];
+    const int n = pb.n;
     Layout L = make_layout(sm, a);
+    // The representative: the start (u, alpha) of a cell this CTA settled,
+    // as loaded, and the results written for it.  A later cell whose start
+    // is the same, bit for bit, takes those results without an evaluation
+    // (the first evaluation is a function of the start alone; not with
+    // predicted starts, which enter it too).  Floor cells that no
+    // perturbation has reached share one start.
+    double *repIn = L.Eg, *repOut = L.Eg + 2 * ldv;   // [2][ldv] each: u, alpha
+    double *rawU = L.aold, *rawA = L.d;               // per slot: the start as loaded
+    const bool dedup = pb.alphaStart == nullptr;
     for (int i = tid; i < 4 * T * ldv; i += kThreads)
         L.alpha[i] = 0.0;
     for (int i = tid; i < T * SI_N; i += kThreads)
@@ -2245,6 +2256,7 @@ __global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ 
         for (int b = 0; b < 3; b++)
             mbar_init(&L.bar[b], 1);
         mbar_init_fence();
+        repValid = 0;
     }
     __syncthreads();
     unsigned mbPhase = 0;
@@ -2252,25 +2264,85 @@ __global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ 
         return;   // most cells iterate: K1 solves them all, in one pass
     for (;;) {
         if (tid == 0) {
-            // fill the slots with cells whose previous solve took at most one
-            // iteration; the others go straight to K1's list
-            int filled = 0;
-            bool exhausted = false;
-            while (filled < T && !exhausted) {
-                const unsigned base = atomicAdd(pb.queue, (unsigned)(T - filled));
-                const int take = (base < (unsigned)pb.count) ? min(T - filled, pb.count - (int)base) : 0;
-                exhausted = take < T - filled;
-                for (int k = 0; k < take; k++) {
-                    const int cell = pb.first + (int)base + k;
-                    if (pb.iters && pb.iters[cell] > 1) {
-                        pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
-                    } else {
-                        L.ints[filled * SI_N + SI_CELL] = cell;
-                        L.ints[filled * SI_N + SI_STATE] = S_NEW;
-                        filled++;
+            ctl[2] = 0;
+            ctl[3] = 0;
+            repHits = 0;
+        }
+        __syncthreads();
+        // Refill, one candidate per warp at a time: cells whose previous
+        // solve took more than one iteration go straight to K1's list,
+        // copies of the representative are finished here, the rest take
+        // slots (a cell drawn after the slots ran out goes to the list).
+        for (;;) {
+            int cell = -1;
+            if (lane == 0 && *(volatile int *)&ctl[2] < T && !*(volatile int *)&ctl[3]) {
+                const unsigned item = atomicAdd(pb.queue, 1u);
+                if (item < (unsigned)pb.count)
+                    cell = pb.first + (int)item;
+                else
+                    ctl[3] = 1;
+            }
+            cell = __shfl_sync(0xffffffffu, cell, 0);
+            if (cell < 0)
+                break;
+            if (pb.iters && pb.iters[cell] > 1) {
+                if (lane == 0)
+                    pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
+                continue;
+            }
+            const double uk = (lane < n) ? pb.u[(size_t)cell * n + lane] : 0.0;
+            const double ak = (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0;
+            if (dedup && *(volatile int *)&repValid) {
+                const bool same = lane >= n || (__double_as_longlong(uk) == __double_as_longlong(repIn[lane]) &&
+                                                __double_as_longlong(ak) == __double_as_longlong(repIn[ldv + lane]));
+                if (__all_sync(0xffffffffu, same)) {
+                    if (lane < n) {
+                        pb.u[(size_t)cell * n + lane] = repOut[lane];
+                        pb.alpha[(size_t)cell * n + lane] = repOut[ldv + lane];
+                        if (a.momentsOld != nullptr) {
+                            const int i = cell / a.NY, j = cell % a.NY;
+                            if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
+                                a.momentsOld[(size_t)cell * n + lane] = uk;
+                        }
                     }
+                    if (lane == 0) {
+                        // finish_slot's records of a first-iteration convergence
+                        if (pb.iters)
+                            pb.iters[cell] = 1;
+                        if (pb.regs)
+                            pb.regs[cell] = kRegularizations[0];
+                        if (pb.status)
+                            pb.status[cell] = 0;
+                        atomicAdd(&L.stat[0], 1ull);
+                        atomicAdd(&L.stat[kNumReg], 1ull);
+                        atomicAdd(&L.stat[kNumReg + 1], 1ull);
+                        atomicMax((int *)&L.stat[kStatU64], 1);
+                        atomicAdd(&L.stat[kNumReg + 4], 1ull);
+                        atomicAdd(&repHits, 1);
+                    }
+                    continue;
                 }
             }
+            int s = 0;
+            if (lane == 0)
+                s = atomicAdd(&ctl[2], 1);
+            s = __shfl_sync(0xffffffffu, s, 0);
+            if (s < T) {
+                if (lane < ldv) {
+                    rawU[s * ldv + lane] = uk;
+                    rawA[s * ldv + lane] = ak;
+                }
+                if (lane == 0) {
+                    L.ints[s * SI_N + SI_CELL] = cell;
+                    L.ints[s * SI_N + SI_STATE] = S_NEW;
+                }
+            } else if (lane == 0) {
+                pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
+            }
+        }
+        __syncthreads();
+        const int filled = min(ctl[2], T);
+        if (tid == 0) {
             for (int s = filled; s < T; s++)
                 L.ints[s * SI_N + SI_STATE] = S_IDLE;
             ctl[0] = (filled == 0);
@@ -2297,6 +2369,23 @@ __global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ 
         }
         fence_proxy_async_smem();   // this round's shared-memory writes before the next bulk copies
         __syncthreads();
+        // a new representative when the current one found no copy this
+        // round: the first slot settled here (SI_ITER = 1)
+        if (dedup && warp == 0 && repHits == 0) {
+            const unsigned m = __ballot_sync(0xffffffffu, lane < filled && L.ints[lane * SI_N + SI_ITER] == 1);
+            if (m) {
+                const int s = __ffs(m) - 1, cell = L.ints[s * SI_N + SI_CELL];
+                if (lane < ldv) {
+                    repIn[lane] = rawU[s * ldv + lane];
+                    repIn[ldv + lane] = rawA[s * ldv + lane];
+                    repOut[lane] = (lane < n) ? pb.u[(size_t)cell * n + lane] : 0.0;
+                    repOut[ldv + lane] = (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0;
+                }
+                __syncwarp();
+                if (lane == 0)
+                    repValid = 1;
+            }
+        }
     }
     if (tid < kStatU64) {
         unsigned long long v = L.stat[tid];
