@@ -124,7 +124,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -484,7 +484,11 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         flux_ms = float(km[1] + km[3])
         device_ms = float(km.sum())
         f_newton = newton_flops(s0, s1, per_iter, n, ang.nq)
-        f_flux = 2 * k * flops_flux_stage(C, C_int, n, ang.nq)
+        # the flux work of the tiles that ran it (a tile with one alpha over
+        # tile and halo applies zero flux without the kinetic flux loop)
+        tiles = ((solver.NX - 4 + 15) // 16) * ((solver.NY - 4 + 15) // 16)
+        run_frac = (s1["flux_tiles"] - s0["flux_tiles"]) / float(2 * k * tiles)
+        f_flux = 2 * k * flops_flux_stage(C, C_int, n, ang.nq) * run_frac
         return {
             "t_start": t_start, "steps": k,
             "value": solves / (device_ms * 1e-3),
@@ -493,6 +497,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
             "iter_mean": iters / solves, "trials_per_solve": trials / solves,
             "fallback_restarts": s1["fallbacks"] - s0["fallbacks"],
             "flux_uniform_tiles": uniform,
+            "flux_tiles_run": run_frac,
             "screened_per_solve": (s1["screened"] - s0["screened"]) / solves,
             "screen_evals_per_solve": (s1["screen_evals"] - s0["screen_evals"]) / solves,
             "kernel_ms": {"newton": newton_ms, "flux": flux_ms},
@@ -888,7 +893,9 @@ def native_arm(args, world, rank, local):
         # H_P = T^-1 H_M T^-T and the basis update T <- T L (n^3 each)
         per_iter += 3.0 * n ** 3
     f_newton = newton_flops(st0, st1, per_iter, n, ang.nq)
-    f_flux = 2 * args.steps * flops_flux_stage(C, C_int, n, ang.nq)
+    tiles = ((solver.NX - 4 + 15) // 16) * ((solver.NY - 4 + 15) // 16)
+    run_frac = (st1["flux_tiles"] - st0["flux_tiles"]) / float(2 * args.steps * tiles)
+    f_flux = 2 * args.steps * flops_flux_stage(C, C_int, n, ang.nq) * run_frac
     ach_newton = f_newton / (newton_ms * 1e-3) / 1e12
     ach_flux = f_flux / (flux_ms * 1e-3) / 1e12
     dominant = "newton" if newton_ms >= flux_ms else "flux"

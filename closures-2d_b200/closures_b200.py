@@ -66,7 +66,7 @@ class cl_stats(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("iter_mean", C.c_double), ("num_solves", C.c_int64),
                 ("hist_reg", C.c_int64 * 5), ("total_iter", C.c_int64),
                 ("total_trials", C.c_int64), ("fallbacks", C.c_int64), ("screened", C.c_int64),
-                ("screen_evals", C.c_int64)]
+                ("screen_evals", C.c_int64), ("flux_tiles", C.c_int64)]
 
 
 class cl_tuning(C.Structure):
@@ -383,7 +383,8 @@ class Context:
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
                 "total_trials": s.total_trials, "fallbacks": s.fallbacks,
-                "screened": s.screened, "screen_evals": s.screen_evals}
+                "screened": s.screened, "screen_evals": s.screen_evals,
+                "flux_tiles": s.flux_tiles}
 
     def solve_batch(self, u, alpha, check=True):
         """opt() on every row of u/alpha (in place).  Returns iters, reg, status."""
@@ -588,7 +589,8 @@ class Solver:
         return {"max_iter": s.max_iter, "iter_mean": s.iter_mean, "num_solves": s.num_solves,
                 "hist_reg": list(s.hist_reg), "total_iter": s.total_iter,
                 "total_trials": s.total_trials, "fallbacks": s.fallbacks,
-                "screened": s.screened, "screen_evals": s.screen_evals}
+                "screened": s.screened, "screen_evals": s.screen_evals,
+                "flux_tiles": s.flux_tiles}
 
     def close(self):
         if self._s:

@@ -586,7 +586,7 @@ struct cl_ctx {
     // band, the list length and the screening work counter
     NewtonArgs sargs;
     int screen = 0, nCtasScreen = 0;
-    int *dPend = nullptr, *dPendCount = nullptr, *dGate = nullptr;
+    int *dPend = nullptr, *dPend2 = nullptr, *dPendCount = nullptr, *dGate = nullptr;
     unsigned int *dScreenQ = nullptr;
     int angN = 0, angN2 = 0, angNq = 0, angGaunt = 0, angNnz = 0;
     std::vector<double> aw, axi, aeta, ap, agval;
@@ -767,6 +767,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         cudaMallocHost(&ctx->hErr, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dIters, C * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dPend, C * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dPend2, C * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dPendCount, (4 + kHostBands) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dScreenQ, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&ctx->dGate, (4 + kHostBands) * sizeof(int)) != cudaSuccess) {
@@ -848,6 +849,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
 
     FluxArgs &f = ctx->fargs;
     memset(&f, 0, sizeof(f));
+    f.tilesRun = &ctx->dStats->fluxTiles;
     f.alpha = ctx->dAlpha;
     f.moments = ctx->dMom;
     f.sigmaT = ctx->dSigT;
@@ -909,6 +911,7 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->dAlpha);
     cudaFree(ctx->dOld);
     cudaFree(ctx->dPend);
+    cudaFree(ctx->dPend2);
     cudaFree(ctx->dPendCount);
     cudaFree(ctx->dScreenQ);
     cudaFree(ctx->dGate);
@@ -1022,8 +1025,11 @@ static cudaError_t launch_stage_newton(cl_ctx *ctx, NewtonArgs &a, int slot, cud
             return e;
         if ((e = launch_screen(s, ctx->nCtasScreen, st)) != cudaSuccess)
             return e;
-        *nk += 2;
-        a.prob[0].cellList = ctx->dPend + kp.first;
+        if ((e = launch_order_list(ctx->dPend + kp.first, ctx->dPendCount + slot, kp.iters, ctx->dPend2 + kp.first,
+                                   st)) != cudaSuccess)
+            return e;
+        *nk += 3;
+        a.prob[0].cellList = ctx->dPend2 + kp.first;
         a.prob[0].countDev = ctx->dPendCount + slot;
         a.prob[0].gateCount = sp.gateCount;
         a.prob[0].gateMin = sp.gateMin;
@@ -1594,7 +1600,7 @@ static float time_newton(cl_ctx *ctx, NewtonArgs a, const DeviceBasis &B, TuneSc
             sp.gateCount = (const int *)(S.q + 3);
             sp.gateMin = (int)std::ceil(kScreenGate * (double)C);
             sgrid = sm_count() * screen_ctas_per_sm(sa);
-            a.prob[0].cellList = ctx->dPend;
+            a.prob[0].cellList = ctx->dPend2;
             a.prob[0].countDev = (const int *)(S.q + 2);
             a.prob[0].gateCount = sp.gateCount;
             a.prob[0].gateMin = sp.gateMin;
@@ -1612,9 +1618,10 @@ static float time_newton(cl_ctx *ctx, NewtonArgs a, const DeviceBasis &B, TuneSc
         cudaEventRecord(S.e0, st);
         if (sgrid > 0) {
             if (launch_screen_gate(S.it, 0, (int)C, (int *)(S.q + 3), st) != cudaSuccess ||
-                launch_screen(sa, sgrid, st) != cudaSuccess)
+                launch_screen(sa, sgrid, st) != cudaSuccess ||
+                launch_order_list(ctx->dPend, (const int *)(S.q + 2), S.it, ctx->dPend2, st) != cudaSuccess)
                 return -1.0f;
-            g_launches += 2;
+            g_launches += 3;
         }
         if (launch_newton(a, grid, st) != cudaSuccess)
             return -1.0f;
@@ -1638,6 +1645,7 @@ static float time_flux(cl_ctx *ctx, FluxArgs f, TuneScratch &S)
     f.moments = S.u;
     f.alpha = ctx->dAlpha;
     f.momentsOld = nullptr;
+    f.tilesRun = nullptr;
     f.dt = 1e-6;
     f.dx = f.dy = 1.0;
     if (plan_flux(f) != 0 || prepare_flux(f) != cudaSuccess)
@@ -1960,6 +1968,7 @@ int cl_get_stats(cl_ctx *ctx, cl_stats *s)
     s->fallbacks = (int64_t)d.fallbacks;
     s->screened = (int64_t)d.screened;
     s->screen_evals = (int64_t)d.screenEvals;
+    s->flux_tiles = (int64_t)d.fluxTiles;
     return CL_OK;
 }
 

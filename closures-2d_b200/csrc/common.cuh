@@ -164,6 +164,7 @@ struct DevStats {
     unsigned long long screenEvals;     // evaluations of the screening pass
     int maxIter;
     int pad;
+    unsigned long long fluxTiles;       // K2+K3 tiles that ran the chunk loop
 };
 constexpr int kStatU64 = kNumReg + 6;
 

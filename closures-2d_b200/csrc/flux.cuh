@@ -32,6 +32,7 @@ struct FluxArgs {
     int smemBytes;
     int tilesX, tilesY;
     int tileBase;               // first tile of the launch (row-major over tilesX x tilesY)
+    unsigned long long *tilesRun;   // nullable: tiles that ran the chunk loop (non-uniform)
 };
 
 int plan_flux(FluxArgs &f);

@@ -88,6 +88,10 @@ struct NewtonProblem {
 // Cells of [first, first + count) whose previous solve took at most one
 // iteration (iters[c] <= 1), added to *out (zero before the launch).
 cudaError_t launch_screen_gate(const int *iters, int first, int count, int *out, cudaStream_t stream);
+// The *count cells of `list` into `out`, most previous iterations first
+// (iters[c], counting sort), so that K1 starts the longest Newton chains
+// first and the short ones fill in behind them.
+cudaError_t launch_order_list(const int *list, const int *count, const int *iters, int *out, cudaStream_t stream);
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
 // S_HELP: an idle slot lent, for one round, to a slot whose line search is

@@ -89,6 +89,39 @@ cudaError_t launch_screen_gate(const int *iters, int first, int count, int *out,
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void __launch_bounds__(1024) order_list_kernel(const int *list, const int *countPtr, const int *iters,
+                                                          int *out)
+{
+    __shared__ int hist[32], start[32];
+    const int cnt = *countPtr;
+    if (threadIdx.x < 32)
+        hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x)
+        atomicAdd(&hist[31 - min(iters[list[i]], 31)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int b = 0; b < 32; b++) {
+            start[b] = acc;
+            acc += hist[b];
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+        const int c = list[i];
+        out[atomicAdd(&start[31 - min(iters[c], 31)], 1)] = c;
+    }
+}
+}  // namespace
+
+cudaError_t launch_order_list(const int *list, const int *count, const int *iters, int *out, cudaStream_t stream)
+{
+    order_list_kernel<<<1, 1024, 0, stream>>>(list, count, iters, out);
+    return cudaGetLastError();
+}
+
 int screen_ctas_per_sm(const NewtonArgs &a)
 {
     int occ = 1;

@@ -2269,75 +2269,92 @@ __global__ void __launch_bounds__(256, 2) screen_kernel(const __grid_constant__ 
             repHits = 0;
         }
         __syncthreads();
-        // Refill, one candidate per warp at a time: cells whose previous
-        // solve took more than one iteration go straight to K1's list,
-        // copies of the representative are finished here, the rest take
-        // slots (a cell drawn after the slots ran out goes to the list).
+        // Refill, kBatch candidates per warp at a time (their loads in
+        // flight together): cells whose previous solve took more than one
+        // iteration go straight to K1's list, copies of the representative
+        // are finished here, the rest take slots (a cell drawn after the
+        // slots ran out goes to the list).
+        constexpr int kBatch = 4;
         for (;;) {
-            int cell = -1;
+            int base = -1;
             if (lane == 0 && *(volatile int *)&ctl[2] < T && !*(volatile int *)&ctl[3]) {
-                const unsigned item = atomicAdd(pb.queue, 1u);
+                const unsigned item = atomicAdd(pb.queue, (unsigned)kBatch);
                 if (item < (unsigned)pb.count)
-                    cell = pb.first + (int)item;
+                    base = (int)item;
                 else
                     ctl[3] = 1;
             }
-            cell = __shfl_sync(0xffffffffu, cell, 0);
-            if (cell < 0)
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base < 0)
                 break;
-            if (pb.iters && pb.iters[cell] > 1) {
-                if (lane == 0)
-                    pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
-                continue;
+            const int cnt = min(kBatch, pb.count - base);
+            double ub[kBatch], ab[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                const size_t at = (size_t)(pb.first + base + b) * n + lane;
+                ub[b] = (b < cnt && lane < n) ? pb.u[at] : 0.0;
+                ab[b] = (b < cnt && lane < n) ? pb.alpha[at] : 0.0;
             }
-            const double uk = (lane < n) ? pb.u[(size_t)cell * n + lane] : 0.0;
-            const double ak = (lane < n) ? pb.alpha[(size_t)cell * n + lane] : 0.0;
-            if (dedup && *(volatile int *)&repValid) {
-                const bool same = lane >= n || (__double_as_longlong(uk) == __double_as_longlong(repIn[lane]) &&
-                                                __double_as_longlong(ak) == __double_as_longlong(repIn[ldv + lane]));
-                if (__all_sync(0xffffffffu, same)) {
-                    if (lane < n) {
-                        pb.u[(size_t)cell * n + lane] = repOut[lane];
-                        pb.alpha[(size_t)cell * n + lane] = repOut[ldv + lane];
-                        if (a.momentsOld != nullptr) {
-                            const int i = cell / a.NY, j = cell % a.NY;
-                            if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
-                                a.momentsOld[(size_t)cell * n + lane] = uk;
-                        }
-                    }
-                    if (lane == 0) {
-                        // finish_slot's records of a first-iteration convergence
-                        if (pb.iters)
-                            pb.iters[cell] = 1;
-                        if (pb.regs)
-                            pb.regs[cell] = kRegularizations[0];
-                        if (pb.status)
-                            pb.status[cell] = 0;
-                        atomicAdd(&L.stat[0], 1ull);
-                        atomicAdd(&L.stat[kNumReg], 1ull);
-                        atomicAdd(&L.stat[kNumReg + 1], 1ull);
-                        atomicMax((int *)&L.stat[kStatU64], 1);
-                        atomicAdd(&L.stat[kNumReg + 4], 1ull);
-                        atomicAdd(&repHits, 1);
-                    }
+            const int itb = (lane < cnt && pb.iters) ? pb.iters[pb.first + base + lane] : 0;
+#pragma unroll
+            for (int b = 0; b < kBatch; b++) {
+                if (b >= cnt)
+                    break;
+                const int cell = pb.first + base + b;
+                const double uk = ub[b], ak = ab[b];
+                if (__shfl_sync(0xffffffffu, itb, b) > 1) {
+                    if (lane == 0)
+                        pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
                     continue;
                 }
-            }
-            int s = 0;
-            if (lane == 0)
-                s = atomicAdd(&ctl[2], 1);
-            s = __shfl_sync(0xffffffffu, s, 0);
-            if (s < T) {
-                if (lane < ldv) {
-                    rawU[s * ldv + lane] = uk;
-                    rawA[s * ldv + lane] = ak;
+                if (dedup && *(volatile int *)&repValid) {
+                    const bool same = lane >= n ||
+                                      (__double_as_longlong(uk) == __double_as_longlong(repIn[lane]) &&
+                                       __double_as_longlong(ak) == __double_as_longlong(repIn[ldv + lane]));
+                    if (__all_sync(0xffffffffu, same)) {
+                        if (lane < n) {
+                            pb.u[(size_t)cell * n + lane] = repOut[lane];
+                            pb.alpha[(size_t)cell * n + lane] = repOut[ldv + lane];
+                            if (a.momentsOld != nullptr) {
+                                const int i = cell / a.NY, j = cell % a.NY;
+                                if (i >= 2 && i < a.NX - 2 && j >= 2 && j < a.NY - 2)
+                                    a.momentsOld[(size_t)cell * n + lane] = uk;
+                            }
+                        }
+                        if (lane == 0) {
+                            // finish_slot's records of a first-iteration convergence
+                            if (pb.iters)
+                                pb.iters[cell] = 1;
+                            if (pb.regs)
+                                pb.regs[cell] = kRegularizations[0];
+                            if (pb.status)
+                                pb.status[cell] = 0;
+                            atomicAdd(&L.stat[0], 1ull);
+                            atomicAdd(&L.stat[kNumReg], 1ull);
+                            atomicAdd(&L.stat[kNumReg + 1], 1ull);
+                            atomicMax((int *)&L.stat[kStatU64], 1);
+                            atomicAdd(&L.stat[kNumReg + 4], 1ull);
+                            atomicAdd(&repHits, 1);
+                        }
+                        continue;
+                    }
                 }
-                if (lane == 0) {
-                    L.ints[s * SI_N + SI_CELL] = cell;
-                    L.ints[s * SI_N + SI_STATE] = S_NEW;
+                int s = 0;
+                if (lane == 0)
+                    s = atomicAdd(&ctl[2], 1);
+                s = __shfl_sync(0xffffffffu, s, 0);
+                if (s < T) {
+                    if (lane < ldv) {
+                        rawU[s * ldv + lane] = uk;
+                        rawA[s * ldv + lane] = ak;
+                    }
+                    if (lane == 0) {
+                        L.ints[s * SI_N + SI_CELL] = cell;
+                        L.ints[s * SI_N + SI_STATE] = S_NEW;
+                    }
+                } else if (lane == 0) {
+                    pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
                 }
-            } else if (lane == 0) {
-                pb.pendList[atomicAdd(pb.pendCount, 1)] = cell;
             }
         }
         __syncthreads();

@@ -127,6 +127,8 @@ typedef struct {
     int64_t screen_evals;           /* evaluations run by the screening pass (gradient
                                        columns only; those of unsettled cells are not
                                        counted in total_iter) */
+    int64_t flux_tiles;             /* K2+K3 16x16 tiles that ran the kinetic flux (the
+                                       others had one alpha over tile and halo: zero flux) */
 } cl_stats;
 
 typedef struct cl_ctx cl_ctx;
