@@ -376,12 +376,14 @@ REF_SAMPLE_SIDE = {"m6_800": 96, "pp6_800": 96, "m4_lattice_200": 96, "m2_50": 5
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture of the workload: newton on m6_800 (profiles/newton_kernel_m6_800.md;
-# algorithmic state traffic of that launch 290 MB read + 433 MB written) and
-# a stage-1 pn_stage launch on pn6_800 (profiles/pn_tile_kernel_pn6_800.md;
-# algorithmic 2n doubles + 16 bytes per cell = 297 MB, part of the read
-# served by L2 from the stage before).
-NCU_TRAFFIC = {("m6_800", "newton"): 670.6e6, ("pn6_800", "pn_stage"): 255.6e6}
+# capture each: on m6_800 the K1 group of a stage at t = 3 dt, the screening
+# pass (662.8 MB, profiles/screen_kernel_m6_800.md; algorithmic state traffic
+# 290 MB read, 290 MB written and 145 MB of saved moments) and K1 over the
+# cells it left (8.6 MB, profiles/newton_kernel_m6_800.md); a stage-1
+# pn_stage launch on pn6_800 (profiles/pn_tile_kernel_pn6_800.md; algorithmic
+# 2n doubles + 16 bytes per cell = 297 MB, part of the read served by L2 from
+# the stage before).
+NCU_TRAFFIC = {("m6_800", "newton"): 671.4e6, ("pn6_800", "pn_stage"): 255.6e6}
 
 
 def train_grid_mlp(cb, torch, w, n, harvest, args):
