@@ -508,7 +508,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
             "newton_frac": f_newton / (newton_ms * 1e-3) / 1e12 / peak,
             "iter_hist_last_stage": np.bincount(np.minimum(it.ravel(), 20), minlength=21).tolist(),
             "iter_hist_last_stage_interior": np.bincount(np.minimum(it[interior], 20), minlength=21).tolist(),
-            "_device_ms": device_ms,
+            "_device_ms": device_ms, "_iters": iters, "_trials": trials,
         }
 
     step = 0
@@ -521,7 +521,8 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
     step += args.warmup
     # launch shapes: the autotuner times its candidates on this state
     tuning = {"headline": ctx.tune() if not args.no_tune else ctx.tuning()}
-    head_state = ctx.get_state() if not args.no_cpu_baseline else None
+    head_state = ctx.get_state()
+    head_iters = ctx.last_iterations()
 
     sampler = ClockSampler(local)
     torch.cuda.synchronize()
@@ -534,6 +535,28 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
     clocks = sampler.stop()
     full_ms += head["_device_ms"]
     step += args.steps
+
+    # the same window again from the same state with every exact shortcut
+    # off (K1's exponent-range test, and with it the screening pass and its
+    # copies of repeated starts; K2+K3's uniform tiles): the work of the
+    # reference's algorithm, and a check that the shortcuts change no result
+    end_state, end_iters = ctx.get_state(), ctx.last_iterations()
+    ctx.set_state(*head_state)
+    ctx.set_last_iterations(head_iters)
+    ctx.set_range_test(False)
+    ctx.set_uniform_flux_skip(False)
+    full_work = window(args.steps, head["t_start"])
+    fw_state = ctx.get_state()
+    fw_iters = full_work["_iters"]
+    fw_trials = full_work["_trials"]
+    full_work["same_state_as_headline"] = bool(np.array_equal(fw_state[0], end_state[0]) and
+                                               np.array_equal(fw_state[1], end_state[1]))
+    for key in ("_device_ms", "_iters", "_trials"):
+        full_work.pop(key)
+    ctx.set_range_test(True)
+    ctx.set_uniform_flux_skip(True)
+    ctx.set_state(*end_state)
+    ctx.set_last_iterations(end_iters)
 
     # end to end through the C ABI with host buffers: every step uploads the
     # state from pinned host memory, runs the RK2 step and reads it back;
@@ -598,8 +621,9 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         full = {"steps": nfull, "t_final": solver.t_final, "last_dt": last_dt,
                 "device_s": full_ms * 1e-3, "steps_per_s": nfull / (full_ms * 1e-3),
                 "value": solves / (full_ms * 1e-3), "value_interior": 2 * C_int * nfull / (full_ms * 1e-3),
-                "iter_mean": (s_full1["total_iter"] - s_begin["total_iter"] - e2e_iters) / solves,
-                "trials_per_solve": (s_full1["total_trials"] - s_begin["total_trials"] - e2e_trials) / solves,
+                "iter_mean": (s_full1["total_iter"] - s_begin["total_iter"] - e2e_iters - fw_iters) / solves,
+                "trials_per_solve": (s_full1["total_trials"] - s_begin["total_trials"] - e2e_trials - fw_trials)
+                / solves,
                 "max_iter": s_full1["max_iter"],
                 "timing": "graph steps timed by CUDA events on the library stream, the two windows "
                           "kernel by kernel; the e2e steps after the headline window are not part of "
@@ -622,7 +646,8 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
     achieved = head["newton_tflops"] if dominant == "newton" else head["flux_tflops"]
     for win in (head, late):
         if win is not None:
-            win.pop("_device_ms")
+            for key in ("_device_ms", "_iters", "_trials"):
+                win.pop(key)
     line = {
         "metric": METRIC, "value": head["value"], "unit": "cell-solves/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup,
@@ -643,7 +668,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         "iter_mean": head["iter_mean"], "trials_per_solve": head["trials_per_solve"],
         "fallback_restarts": head["fallback_restarts"],
         "kernel_ms": head["kernel_ms"],
-        "windows": {"headline": head, "late": late},
+        "windows": {"headline": head, "headline_full_work": full_work, "late": late},
         "full_run": full,
         "nn": nn,
         "tuning": tuning,

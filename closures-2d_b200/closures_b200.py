@@ -127,6 +127,7 @@ def lib():
             "cl_get_tuning": (C.c_int, [vp, C.POINTER(cl_tuning)]),
             "cl_set_launch_shape": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
             "cl_set_range_test": (C.c_int, [vp, C.c_int]),
+            "cl_set_uniform_flux_skip": (C.c_int, [vp, C.c_int]),
             "cl_get_last_iterations": (C.c_int, [vp, ip]),
             "cl_solve_batch": (C.c_int, [vp, C.c_int, dp, dp, ip, dp, ip]),
             "cl_solve_batch_device": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, vp]),
@@ -450,6 +451,11 @@ class Context:
         """K1's exponent-range convergence test on or off (cl_set_range_test);
         results are the same either way."""
         _check(lib().cl_set_range_test(self._ctx, 1 if enable else 0), self._err)
+
+    def set_uniform_flux_skip(self, enable=True):
+        """K2+K3's uniform-tile shortcut on or off (cl_set_uniform_flux_skip);
+        results are the same either way, up to the sign of zero."""
+        _check(lib().cl_set_uniform_flux_skip(self._ctx, 1 if enable else 0), self._err)
 
     def stream(self):
         """The context's CUDA stream as a torch.cuda.ExternalStream (for

@@ -850,6 +850,7 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
     FluxArgs &f = ctx->fargs;
     memset(&f, 0, sizeof(f));
     f.tilesRun = &ctx->dStats->fluxTiles;
+    f.skipUniform = 1;
     f.alpha = ctx->dAlpha;
     f.moments = ctx->dMom;
     f.sigmaT = ctx->dSigT;
@@ -1761,6 +1762,16 @@ int cl_get_tuning(cl_ctx *ctx, cl_tuning *out)
     if (!ctx || !out)
         return CL_ERR_ARG;
     *out = ctx->tuning;
+    return CL_OK;
+}
+
+int cl_set_uniform_flux_skip(cl_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return CL_ERR_ARG;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->fargs.skipUniform = enable ? 1 : 0;
+    invalidate_graph(ctx);
     return CL_OK;
 }
 

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kFluxThreads, 1) flux_kernel(const __grid_cons
         const int h = idx / nb, c = idx % nb;
         differs |= __double_as_longlong(sAl[h * ldAl + c]) != __double_as_longlong(sAl[c]);
     }
-    const int nloop = __syncthreads_or(differs) ? nchunks : 0;
+    const int nloop = (__syncthreads_or(differs) || !f.skipUniform) ? nchunks : 0;
     if (tid == 0 && nloop > 0 && f.tilesRun != nullptr)
         atomicAdd(f.tilesRun, 1ull);
     if (nloop > 0)

@@ -33,6 +33,7 @@ struct FluxArgs {
     int tilesX, tilesY;
     int tileBase;               // first tile of the launch (row-major over tilesX x tilesY)
     unsigned long long *tilesRun;   // nullable: tiles that ran the chunk loop (non-uniform)
+    int skipUniform;                // 1: uniform tiles apply zero flux without the chunk loop
 };
 
 int plan_flux(FluxArgs &f);

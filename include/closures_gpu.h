@@ -257,6 +257,12 @@ int cl_set_launch_shape(cl_ctx *ctx, int newton_warps, int newton_contraction, i
  * (opt.cpp:244-306) at that evaluation.  Results are bit-identical with the
  * test on or off; off runs every evaluation through the Hessian. */
 int cl_set_range_test(cl_ctx *ctx, int enable);
+/* K2+K3's uniform-tile shortcut (on by default): a 16x16 tile whose alpha,
+ * halo included, is one value bit for bit has zero flux (every slope and
+ * upwind difference of momopt_update.cpp:96-202 is an exact zero) and skips
+ * the kinetic flux loop.  Results are the same with it off, up to the sign
+ * of zero; off, every tile runs the loop. */
+int cl_set_uniform_flux_skip(cl_ctx *ctx, int enable);
 
 /* Batched per-vector operator: the GPU equivalent of calling
  * opt(n, n2, nq, u, alpha, options, w, p, &outs) (opt.cpp:82-148) on `count`

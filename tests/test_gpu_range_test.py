@@ -10,7 +10,8 @@ direction-pair layout, a screening pass evaluates every cell first with the
 gradient columns only and settles the cells that converge there; K1 solves
 the rest from their starts.  Both only skip work, so every result must be
 bit-identical with the test off, where each evaluation goes through K1's
-Hessian, its factorisation and the condition bounds.
+Hessian, its factorisation and the condition bounds.  K2+K3's uniform-tile
+shortcut likewise: the same states with every tile running the flux loop.
 """
 import numpy as np
 import pytest
@@ -126,3 +127,30 @@ def test_host_step_bit_identical_with_and_without(tmp_path):
     assert sa["hist_reg"] == sb["hist_reg"]
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("case", ["m6_gaunt_pairs", "m4_lattice"])
+def test_uniform_flux_tiles_same_result(tmp_path, case):
+    """K2+K3 with the uniform-tile shortcut (a tile whose alpha, halo
+    included, is one value applies zero flux) against every tile running
+    the flux loop: the same states (np.array_equal: up to the sign of zero),
+    and the shortcut did skip tiles."""
+    kw, _ = CASES[case]
+    runs = {}
+    for on in (1, 0):
+        deck = str(tmp_path / ("flux_%d.deck" % on))
+        decks.write_deck(deck, decks.deck_text(**kw, extra={"MOMOPT_GPU_TUNE": "0"}))
+        s = cb.Solver(deck, str(tmp_path))
+        ctx = s.context()
+        ctx.set_uniform_flux_skip(bool(on))
+        for _ in range(4):
+            s.update(s.max_dt)
+        m, a = ctx.get_state()
+        runs[on] = (m, a, s.stats()["flux_tiles"])
+        tiles = ((kw["num_cells_x"] + 15) // 16) * ((kw["num_cells_y"] + 15) // 16)
+        s.close()
+    assert np.array_equal(runs[1][0], runs[0][0]) and np.array_equal(runs[1][1], runs[0][1])
+    assert runs[0][2] == 8 * tiles            # 4 steps, 2 stages, every tile
+    assert runs[1][2] <= runs[0][2]
+    if case == "m6_gaunt_pairs":
+        assert runs[1][2] < runs[0][2]        # the pulse has not reached the corners
