@@ -76,10 +76,10 @@ def test_mixed_rejected_where_not_provided():
 
 
 def test_mixed_cfg2_lattice_against_fp64_and_oracle(tmp_path):
-    """The M4 lattice at 200 x 200, Q = 30 (the mixed-precision configuration
-    of the north star) for three RK2 steps, cell by cell: mixed against the
-    FP64 GPU path and against the FP64 oracle, to the north star's 1e-6
-    relative for the mixed path.  The comparison with the oracle is made on
+    """The M4 lattice at 200 x 200, Q = 30 (the deck mixed precision is meant
+    for) for three RK2 steps, cell by cell: mixed against the FP64 GPU path and
+    against the FP64 oracle, to 1e-6 relative (the accuracy asked of the mixed
+    path).  The comparison with the oracle is made on
     the cells whose result rounding does not decide (the two oracle builds and
     the FP64 GPU path agree to 1e-10), which must be nearly all of them."""
     import pyoracle
