@@ -559,8 +559,8 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
         full_work["same_state_as_headline"] = None
     for key in ("_device_ms", "_iters", "_trials"):
         full_work.pop(key)
-    ctx.set_range_test(True)
-    ctx.set_uniform_flux_skip(True)
+    ctx.set_range_test(not args.no_shortcuts)
+    ctx.set_uniform_flux_skip(not args.no_shortcuts)
     ctx.set_state(*end_state)
     ctx.set_last_iterations(end_iters)
 
@@ -668,6 +668,7 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
                    "moment_type": w.get("moment_type", "mn"),
                    "newton": args.newton, "precision": args.precision, "opt_type": args.opt_type,
                    "contraction": args.contraction, "t_start": head["t_start"],
+                   "shortcuts": not args.no_shortcuts,
                    "l2": "state 2x%d MB > L2, no flush" % (C * n * 8 // 2 ** 20),
                    "parallelism": "single"},
         "value_interior": head["value_interior"],
@@ -844,6 +845,9 @@ def native_arm(args, world, rank, local):
     else:
         solver = cb.Solver(deck, tmp)
     ctx = solver.context()
+    if args.no_shortcuts:
+        ctx.set_range_test(False)
+        ctx.set_uniform_flux_skip(False)
     dt, dx, dy = solver.max_dt, solver.dx, solver.dy
     C = solver.NX * solver.NY
     C_int = solver.nx * solver.ny
@@ -1385,6 +1389,9 @@ def main():
                     help="single-GPU grid workloads: skip the learned-start comparison on the late window")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no autotuner)")
+    ap.add_argument("--no-shortcuts", action="store_true",
+                    help="grid workloads: every exact shortcut off for the whole run (K1's "
+                         "exponent-range test with the screening pass, K2+K3's uniform tiles)")
     ap.add_argument("--opt-type", type=int, default=0, choices=[0, 1, 2],
                     help="grid workloads: MOMOPT_OPTIMIZATION_TYPE (1: change-of-basis Newton, "
                          "2: BFGS sub-iterations in the change of basis)")

@@ -768,9 +768,10 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
             colsum += fabs(v[i]);
         }
         __syncwarp();
-        double rs = 0.0;
-        if (act)
-            for (int c = 0; c <= lane; c++)
+        double rs = 0.0;   // unrolled: the loads issue together, the sum keeps its order
+#pragma unroll
+        for (int c = 0; c < kMaxN; c++)
+            if (act && c <= lane)
                 rs += fabs(Hs[lane * ldh + c]);
         // ||A^-1||_1 <= ||L^-1||_1 ||L^-1||_inf, and the Higham estimate never
         // exceeds ||A^-1||_1: when the bound already shows cond <= COND_H_MAX
@@ -792,8 +793,9 @@ __device__ void slot_logic(const NewtonArgs &a, const NewtonProblem &pb, Layout 
     vec[lane] = gi;
     __syncwarp();
     double y = 0.0;
-    if (act)
-        for (int c = 0; c <= lane; c++)
+#pragma unroll
+    for (int c = 0; c < kMaxN; c++)
+        if (act && c <= lane)
             y = fma(Hs[lane * ldh + c], vec[c], y);
     __syncwarp();
     vec[32 + lane] = y;
