@@ -586,7 +586,7 @@ struct cl_ctx {
     // band, the list length and the screening work counter
     NewtonArgs sargs;
     int screen = 0, nCtasScreen = 0;
-    int *dPend = nullptr, *dPend2 = nullptr, *dPendCount = nullptr, *dGate = nullptr;
+    int *dPend = nullptr, *dPend2 = nullptr, *dPendCount = nullptr, *dGate = nullptr, *dOrderCount = nullptr;
     unsigned int *dScreenQ = nullptr;
     int angN = 0, angN2 = 0, angNq = 0, angGaunt = 0, angNnz = 0;
     std::vector<double> aw, axi, aeta, ap, agval;
@@ -770,7 +770,8 @@ int cl_create(const cl_grid *grid, const cl_options *opts, const cl_angular *ang
         cudaMalloc(&ctx->dPend2, C * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dPendCount, (4 + kHostBands) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->dScreenQ, (4 + kHostBands) * sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&ctx->dGate, (4 + kHostBands) * sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&ctx->dGate, (4 + kHostBands) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->dOrderCount, (4 + kHostBands) * sizeof(int)) != cudaSuccess) {
         ctx->err = "device allocation failed";
         return ctx_fail(ctx, CL_ERR_CUDA);
     }
@@ -916,6 +917,7 @@ void cl_destroy(cl_ctx *ctx)
     cudaFree(ctx->dPendCount);
     cudaFree(ctx->dScreenQ);
     cudaFree(ctx->dGate);
+    cudaFree(ctx->dOrderCount);
     cudaFree(ctx->dSigT);
     cudaFree(ctx->dSigS);
     cudaFree(ctx->dQueue);
@@ -991,49 +993,60 @@ static void update_screen(cl_ctx *ctx)
 // would have run beside.
 constexpr double kScreenGate = 0.85;
 
-// K1 of a grid stage or band (`a` complete; `slot` selects the counters):
-// with screening, the gate count, the screening pass over the same cells,
-// then K1 over the cells it left (or over all of them when the gate stays
-// shut).
+// Whole stages of at most this many cells are ordered for K1 too (gate
+// shut, or no screening): one CTA sorts them in a small fraction of the
+// stage.  Larger stages keep cell order: sorting 646,416 cells in one CTA
+// took about a millisecond per stage and measured 4-6 % slower at t = 0.9 of
+// the M6 pulse.
+constexpr int kOrderWholeMax = 131072;
+
+// K1 of a grid stage or band (`a` complete; `slot` selects the counters).
+// With screening: the gate count and the screening pass over the same
+// cells.  Then the order of K1's cells, longest previous Newton chain first
+// (the cells the screening left; or the whole range when it is small), and
+// K1 over that list.
 static cudaError_t launch_stage_newton(cl_ctx *ctx, NewtonArgs &a, int slot, cudaStream_t st, int *nk)
 {
     cudaError_t e;
-    if (ctx->screen && a.prob[0].iters) {
-        NewtonArgs s = ctx->sargs;
-        NewtonProblem &sp = s.prob[0];
-        const NewtonProblem &kp = a.prob[0];
-        sp.count = kp.count;
-        sp.first = kp.first;
-        sp.u = kp.u;
-        sp.alpha = kp.alpha;
-        sp.iters = kp.iters;
-        sp.regs = kp.regs;
-        sp.status = kp.status;
-        sp.alphaStart = kp.alphaStart;
-        sp.queue = ctx->dScreenQ + slot;
-        sp.pendList = ctx->dPend + kp.first;
-        sp.pendCount = ctx->dPendCount + slot;
-        sp.gateCount = ctx->dGate + slot;
-        sp.gateMin = (int)std::ceil(kScreenGate * kp.count);
-        s.momentsOld = a.momentsOld;
-        if ((e = cudaMemsetAsync(ctx->dScreenQ + slot, 0, sizeof(unsigned), st)) != cudaSuccess)
+    const NewtonProblem kp = a.prob[0];
+    if (kp.iters && ctx->dPend && (ctx->screen || kp.count <= kOrderWholeMax)) {
+        int gateMin = 0;
+        if (ctx->screen) {
+            NewtonArgs s = ctx->sargs;
+            NewtonProblem &sp = s.prob[0];
+            sp.count = kp.count;
+            sp.first = kp.first;
+            sp.u = kp.u;
+            sp.alpha = kp.alpha;
+            sp.iters = kp.iters;
+            sp.regs = kp.regs;
+            sp.status = kp.status;
+            sp.alphaStart = kp.alphaStart;
+            sp.queue = ctx->dScreenQ + slot;
+            sp.pendList = ctx->dPend + kp.first;
+            sp.pendCount = ctx->dPendCount + slot;
+            sp.gateCount = ctx->dGate + slot;
+            sp.gateMin = gateMin = (int)std::ceil(kScreenGate * kp.count);
+            s.momentsOld = a.momentsOld;
+            if ((e = cudaMemsetAsync(ctx->dScreenQ + slot, 0, sizeof(unsigned), st)) != cudaSuccess)
+                return e;
+            if ((e = cudaMemsetAsync(ctx->dPendCount + slot, 0, sizeof(int), st)) != cudaSuccess)
+                return e;
+            if ((e = cudaMemsetAsync(ctx->dGate + slot, 0, sizeof(int), st)) != cudaSuccess)
+                return e;
+            if ((e = launch_screen_gate(kp.iters, kp.first, kp.count, ctx->dGate + slot, st)) != cudaSuccess)
+                return e;
+            if ((e = launch_screen(s, ctx->nCtasScreen, st)) != cudaSuccess)
+                return e;
+            *nk += 2;
+        }
+        if ((e = launch_order_cells(ctx->screen ? ctx->dPend + kp.first : nullptr, ctx->dPendCount + slot, kp.first,
+                                    kp.count, ctx->screen ? ctx->dGate + slot : nullptr, gateMin, kOrderWholeMax,
+                                    kp.iters, ctx->dPend2 + kp.first, ctx->dOrderCount + slot, st)) != cudaSuccess)
             return e;
-        if ((e = cudaMemsetAsync(ctx->dPendCount + slot, 0, sizeof(int), st)) != cudaSuccess)
-            return e;
-        if ((e = cudaMemsetAsync(ctx->dGate + slot, 0, sizeof(int), st)) != cudaSuccess)
-            return e;
-        if ((e = launch_screen_gate(kp.iters, kp.first, kp.count, ctx->dGate + slot, st)) != cudaSuccess)
-            return e;
-        if ((e = launch_screen(s, ctx->nCtasScreen, st)) != cudaSuccess)
-            return e;
-        if ((e = launch_order_list(ctx->dPend + kp.first, ctx->dPendCount + slot, kp.iters, ctx->dPend2 + kp.first,
-                                   st)) != cudaSuccess)
-            return e;
-        *nk += 3;
+        *nk += 1;
         a.prob[0].cellList = ctx->dPend2 + kp.first;
-        a.prob[0].countDev = ctx->dPendCount + slot;
-        a.prob[0].gateCount = sp.gateCount;
-        a.prob[0].gateMin = sp.gateMin;
+        a.prob[0].countDev = ctx->dOrderCount + slot;
     }
     if ((e = launch_newton(a, ctx->nCtas, st)) != cudaSuccess)
         return e;
@@ -1602,9 +1615,7 @@ static float time_newton(cl_ctx *ctx, NewtonArgs a, const DeviceBasis &B, TuneSc
             sp.gateMin = (int)std::ceil(kScreenGate * (double)C);
             sgrid = sm_count() * screen_ctas_per_sm(sa);
             a.prob[0].cellList = ctx->dPend2;
-            a.prob[0].countDev = (const int *)(S.q + 2);
-            a.prob[0].gateCount = sp.gateCount;
-            a.prob[0].gateMin = sp.gateMin;
+            a.prob[0].countDev = (const int *)(S.q + 4);
         }
     }
     float ms[3] = {0, 0, 0};
@@ -1613,14 +1624,16 @@ static float time_newton(cl_ctx *ctx, NewtonArgs a, const DeviceBasis &B, TuneSc
         if (cudaMemcpyAsync(S.u, ctx->dMom, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
             cudaMemcpyAsync(S.a, ctx->dAlpha, C * n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
             cudaMemcpyAsync(S.it, ctx->dIters, C * sizeof(int), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-            cudaMemsetAsync(S.q, 0, 4 * sizeof(unsigned), st) != cudaSuccess ||
+            cudaMemsetAsync(S.q, 0, 5 * sizeof(unsigned), st) != cudaSuccess ||
             cudaMemsetAsync(S.err, 0, 2 * sizeof(int), st) != cudaSuccess)
             return -1.0f;
         cudaEventRecord(S.e0, st);
         if (sgrid > 0) {
             if (launch_screen_gate(S.it, 0, (int)C, (int *)(S.q + 3), st) != cudaSuccess ||
                 launch_screen(sa, sgrid, st) != cudaSuccess ||
-                launch_order_list(ctx->dPend, (const int *)(S.q + 2), S.it, ctx->dPend2, st) != cudaSuccess)
+                launch_order_cells(ctx->dPend, (const int *)(S.q + 2), 0, (int)C, (const int *)(S.q + 3),
+                                   sa.prob[0].gateMin, kOrderWholeMax, S.it, ctx->dPend2, (int *)(S.q + 4),
+                                   st) != cudaSuccess)
                 return -1.0f;
             g_launches += 3;
         }
@@ -1833,7 +1846,7 @@ int cl_tune(cl_ctx *ctx, int use_cache, cl_tuning *out)
     TuneScratch S;
     if (cudaMalloc(&S.u, C * n * 8) != cudaSuccess || cudaMalloc(&S.a, C * n * 8) != cudaSuccess ||
         cudaMalloc(&S.it, C * sizeof(int)) != cudaSuccess || cudaMalloc(&S.err, 2 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&S.q, 4 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&S.st, sizeof(DevStats)) != cudaSuccess ||
+        cudaMalloc(&S.q, 5 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&S.st, sizeof(DevStats)) != cudaSuccess ||
         cudaEventCreate(&S.e0) != cudaSuccess || cudaEventCreate(&S.e1) != cudaSuccess) {
         ctx->err = "tuner scratch";
         return CL_ERR_CUDA;

@@ -71,12 +71,12 @@ struct NewtonProblem {
     unsigned int *queue;        // work counter, zero before the launch
     int first;                  // index of the first work item: the launch solves
                                 // items first .. first + count - 1 (a band of cells)
-    // K1 after a screening pass: the cells to solve are cellList[0 .. *countDev)
-    // (both null otherwise); the screening pass appends them at
-    // pendList[atomicAdd(pendCount, 1)].  The pass runs only when *gateCount
-    // (cells of the launch whose previous solve took at most one iteration,
-    // from `iters`) is at least gateMin, and evaluates only such cells;
-    // otherwise K1 solves cells first .. first + count - 1 directly.
+    // K1 over a list: the cells to solve are cellList[0 .. *countDev), or
+    // cells first .. first + count - 1 when cellList is null or *countDev is
+    // negative.  The screening pass appends the cells it leaves at
+    // pendList[atomicAdd(pendCount, 1)]; it runs only when *gateCount (cells
+    // of the launch whose previous solve took at most one iteration, from
+    // `iters`) is at least gateMin, and evaluates only such cells.
     const int *cellList;
     const int *countDev;
     int *pendList;
@@ -88,10 +88,15 @@ struct NewtonProblem {
 // Cells of [first, first + count) whose previous solve took at most one
 // iteration (iters[c] <= 1), added to *out (zero before the launch).
 cudaError_t launch_screen_gate(const int *iters, int first, int count, int *out, cudaStream_t stream);
-// The *count cells of `list` into `out`, most previous iterations first
-// (iters[c], counting sort), so that K1 starts the longest Newton chains
-// first and the short ones fill in behind them.
-cudaError_t launch_order_list(const int *list, const int *count, const int *iters, int *out, cudaStream_t stream);
+// K1's list, most previous iterations first (iters[c], a counting sort in
+// one CTA), so that K1 starts the longest Newton chains first and the short
+// ones fill in behind them: the *listCount cells of `list` when the
+// screening gate is open (list non-null and *gateCount >= gateMin); else the
+// cells first .. first + count - 1 when count <= wholeMax, or *outCount = -1
+// (K1 takes the range in cell order); written to out[0 .. *outCount).
+cudaError_t launch_order_cells(const int *list, const int *listCount, int first, int count, const int *gateCount,
+                               int gateMin, int wholeMax, const int *iters, int *out, int *outCount,
+                               cudaStream_t stream);
 
 // Per-slot state in shared memory: slot states, doubles (SC_*) and ints (SI_*).
 // S_HELP: an idle slot lent, for one round, to a slot whose line search is

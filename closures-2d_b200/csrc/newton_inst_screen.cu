@@ -90,35 +90,63 @@ cudaError_t launch_screen_gate(const int *iters, int first, int count, int *out,
 }
 
 namespace {
-__global__ void __launch_bounds__(1024) order_list_kernel(const int *list, const int *countPtr, const int *iters,
-                                                          int *out)
+__global__ void __launch_bounds__(1024) order_cells_kernel(const int *list, const int *listCount, int first, int count,
+                                                           const int *gateCount, int gateMin, int wholeMax,
+                                                           const int *iters, int *out, int *outCount)
 {
     __shared__ int hist[32], start[32];
-    const int cnt = *countPtr;
+    const bool useList = list != nullptr && (gateCount == nullptr || *gateCount >= gateMin);
+    if (!useList && count > wholeMax) {
+        if (threadIdx.x == 0)
+            *outCount = -1;   // K1 takes the range in cell order
+        return;
+    }
+    const int cnt = useList ? *listCount : count;
+    const unsigned lane = threadIdx.x & 31u;
     if (threadIdx.x < 32)
         hist[threadIdx.x] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x)
-        atomicAdd(&hist[31 - min(iters[list[i]], 31)], 1);
+    // one shared atomic per bucket per warp (lanes with equal buckets grouped)
+    for (int base = 0; base < cnt; base += blockDim.x) {
+        const int i = base + (int)threadIdx.x;
+        const int c = (i < cnt) ? (useList ? list[i] : first + i) : 0;
+        const int b = (i < cnt) ? 31 - min(iters[c], 31) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && lane == (unsigned)(__ffs(peers) - 1))
+            atomicAdd(&hist[b], __popc(peers));
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         int acc = 0;
-        for (int b = 0; b < 32; b++) {
-            start[b] = acc;
-            acc += hist[b];
+        for (int k = 0; k < 32; k++) {
+            start[k] = acc;
+            acc += hist[k];
         }
+        *outCount = cnt;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-        const int c = list[i];
-        out[atomicAdd(&start[31 - min(iters[c], 31)], 1)] = c;
+    for (int base = 0; base < cnt; base += blockDim.x) {
+        const int i = base + (int)threadIdx.x;
+        const int c = (i < cnt) ? (useList ? list[i] : first + i) : 0;
+        const int b = (i < cnt) ? 31 - min(iters[c], 31) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(peers) - 1;
+        int pos = 0;
+        if (b >= 0 && lane == (unsigned)leader)
+            pos = atomicAdd(&start[b], __popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader);
+        if (b >= 0)
+            out[pos + __popc(peers & ((1u << lane) - 1u))] = c;
     }
 }
 }  // namespace
 
-cudaError_t launch_order_list(const int *list, const int *count, const int *iters, int *out, cudaStream_t stream)
+cudaError_t launch_order_cells(const int *list, const int *listCount, int first, int count, const int *gateCount,
+                               int gateMin, int wholeMax, const int *iters, int *out, int *outCount,
+                               cudaStream_t stream)
 {
-    order_list_kernel<<<1, 1024, 0, stream>>>(list, count, iters, out);
+    order_cells_kernel<<<1, 1024, 0, stream>>>(list, listCount, first, count, gateCount, gateMin, wholeMax, iters, out,
+                                               outCount);
     return cudaGetLastError();
 }
 

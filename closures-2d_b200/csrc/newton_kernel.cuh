@@ -1928,7 +1928,7 @@ __global__ void __launch_bounds__(NW * 32, NW == 8 ? 1 : 2) newton_kernel(const 
                     break;
                 }
                 const NewtonProblem &pb = a.prob[p];
-                const bool list = pb.cellList && (!pb.gateCount || *pb.gateCount >= pb.gateMin);
+                const bool list = pb.cellList && *pb.countDev >= 0;
                 const int count = list ? *pb.countDev : pb.count;
                 unsigned base = atomicAdd(pb.queue, (unsigned)nIdle);
                 if (base >= (unsigned)count) {
