@@ -683,7 +683,11 @@ def single_grid_run(args, cb, torch, solver, deck, w, ang, nnz, local):
             "bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": NCU_TRAFFIC.get((args.workload, dominant)),
             "peak_source": "FP64 DMMA m16n8k8 throughput measured live (cl_fp64_peak)",
-            "other": {"newton_tflops": head["newton_tflops"], "flux_tflops": head["flux_tflops"]},
+            "other": {"newton_tflops": head["newton_tflops"], "flux_tflops": head["flux_tflops"],
+                      # the same window with every exact shortcut off: K1 and
+                      # K2+K3 doing the reference algorithm's work on every cell
+                      "full_work_newton_frac": full_work["newton_frac"],
+                      "full_work_flux_frac": full_work["flux_tflops"] / peak},
         },
         "cpu_baseline": cpu,
         "e2e": {"value": 2 * C * e2e_steps / e2e_s, "unit": "cell-solves/s",
