@@ -988,10 +988,11 @@ static void update_screen(cl_ctx *ctx)
 }
 
 // Fraction of a launch's cells whose previous solve took one iteration, at
-// or above which the screening pass runs: then it settles most cells, and
-// K1's time over the rest is not set by long Newton chains the easy cells
-// would have run beside.
-constexpr double kScreenGate = 0.85;
+// or above which the screening pass runs: then it settles enough cells (most
+// of them copies of repeated starts) that K1's time over the rest is not set
+// by long Newton chains the easy cells would have run beside.  Measured on
+// the M6 pulse's whole run: 0.85 -> 51.6 s, 0.6 -> 46.3 s.
+constexpr double kScreenGate = 0.6;
 
 // Whole stages of at most this many cells are ordered for K1 too (gate
 // shut, or no screening): one CTA sorts them in a small fraction of the
