@@ -991,8 +991,9 @@ static void update_screen(cl_ctx *ctx)
 // or above which the screening pass runs: then it settles enough cells (most
 // of them copies of repeated starts) that K1's time over the rest is not set
 // by long Newton chains the easy cells would have run beside.  Measured on
-// the M6 pulse's whole run: 0.85 -> 51.6 s, 0.6 -> 46.3 s.
-constexpr double kScreenGate = 0.6;
+// the M6 pulse's whole run: 0.85 -> 51.6 s, 0.6 -> 46.3 s, 0.45 -> 45.9 s
+// (and its window at t = 0.9, 56 % one-iteration cells, 6 % faster screened).
+constexpr double kScreenGate = 0.45;
 
 // Whole stages of at most this many cells are ordered for K1 too (gate
 // shut, or no screening): one CTA sorts them in a small fraction of the
